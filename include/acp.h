@@ -1,0 +1,176 @@
+/*
+ * acp.h -- C ABI of the B200 engine for the acPulse_vcLBM hot path.
+ *
+ * The reference runs one process with a C++ object API: Control(file) reads
+ * BoundaryConditions.txt (Control.cpp:8-132), Lattice(Control&) builds the
+ * mesh (Lattice.h:23-57), initialization(Control&) sets the pulse
+ * (Lattice.cpp:1397-1493) and solve(alt) / solve(alt0, alt1) advance one
+ * coarse step (Lattice.cpp:2158-2210).  This header is the thin C layer that a
+ * drop-in Control/Lattice (or a cgo / ctypes / JNI caller) binds: plain
+ * structs, pointers and sizes, no C++ or torch types.  Every function returns
+ * ACP_OK (0) or a negative ACP_ERR_* code; acp_last_error() gives the text.
+ *
+ * Units: the case descriptor is in the reference's SI units (metres, seconds,
+ * kg/m^3).  Populations read back through acp_read_populations are the
+ * reference's FP64 distributions f_i (Node::distr_, Node.h:190) of the array
+ * the next step reads, i.e. post-streaming / pre-collision, for every storage
+ * form.  Array order is structure-of-arrays: index ((q*nz + k)*ny + j)*nx + i.
+ */
+#ifndef ACP_H
+#define ACP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ACP_ABI_VERSION 1
+
+/* status codes */
+#define ACP_OK 0
+#define ACP_ERR_INVALID (-1)     /* bad argument or case description */
+#define ACP_ERR_CUDA (-2)        /* a CUDA runtime call failed */
+#define ACP_ERR_NOMEM (-3)       /* device or host allocation failed */
+#define ACP_ERR_UNSUPPORTED (-4) /* valid but not built (e.g. option combination) */
+#define ACP_ERR_NUMERIC (-5)     /* NaN/Inf or density blow-up detected on the device */
+#define ACP_ERR_TIMEOUT (-6)     /* a bounded device wait gave up */
+#define ACP_ERR_BUDGET (-7)      /* admission refused: HBM budget exhausted */
+#define ACP_ERR_STATE (-8)       /* call out of order (e.g. step before init) */
+
+/* Collision-Model keyword (BoundaryConditions.txt:30-44, Lattice.cpp:2158-2183) */
+enum acp_op { ACP_OP_SRT = 0, ACP_OP_MRT_GS = 1, ACP_OP_MRT_RM = 2, ACP_OP_RR = 3, ACP_OP_HRR = 4 };
+
+/* per-axis boundary: the reference puts LODI boundary nodes on all six faces
+ * (Lattice.cpp:132,142); periodic axes are an extension used by the pulse
+ * configurations (quasi-2D boxes periodic in y and z). */
+enum acp_bc { ACP_BC_LODI = 0, ACP_BC_PERIODIC = 1 };
+
+/* population storage form */
+enum acp_storage {
+    ACP_STORE_F64 = 0,     /* f_i as FP64 (the reference's representation) */
+    ACP_STORE_F32_DEV = 1, /* f_i - w_i*rho0 as FP32, collided in FP32 */
+    ACP_STORE_F16_DEV = 2  /* f_i - w_i*rho0 as FP16 with a power-of-two scale per population */
+};
+
+/* Coupling-Approach keyword (BoundaryConditions.txt:53) */
+enum acp_coupling { ACP_COUPLING_STD = 0, ACP_COUPLING_DC1 = 1, ACP_COUPLING_DC2 = 2 };
+/* F2C-Filter keyword (BoundaryConditions.txt:68) */
+enum acp_f2c_filter { ACP_F2C_NOFI = 0, ACP_F2C_LAG = 1, ACP_F2C_TOU = 2 };
+/* Scaling-Style keyword (BoundaryConditions.txt:89) */
+enum acp_scaling { ACP_SCALING_SRT = 0, ACP_SCALING_MRT = 1 };
+/* Coarse-to-Fine keyword (BoundaryConditions.txt:71-77) */
+enum acp_c2f_replace { ACP_C2F_MF = 0, ACP_C2F_MFP = 1, ACP_C2F_FALL = 2 };
+/* Fine-to-Coarse keyword (BoundaryConditions.txt:79-83) */
+enum acp_f2c_replace { ACP_F2C_MC = 0, ACP_F2C_MCP = 1, ACP_F2C_CALL = 2 };
+
+/* refinement layout */
+enum acp_layout {
+    ACP_LAYOUT_SHELL = 0, /* the reference's: fine shell around a coarse core (Lattice.cpp:17-234) */
+    ACP_LAYOUT_BOX = 1    /* fine box [box_lo, box_hi] (coarse node indices) inside the coarse grid */
+};
+
+/* initial condition */
+enum acp_ic {
+    ACP_IC_REFERENCE = 0, /* Lattice::initialization: Rc = 0.06 m, A = 0.01, centre -8 Rc in x (Lattice.cpp:1415-1433) */
+    ACP_IC_GAUSSIAN = 1   /* rho = rho0 (1 + eps exp(-ln2 r^2 / b^2)), centre and b in coarse cells */
+};
+
+/* readable fields */
+enum acp_field { ACP_FIELD_RHO = 0, ACP_FIELD_UX = 1, ACP_FIELD_UY = 2, ACP_FIELD_UZ = 3, ACP_FIELD_P = 4 };
+
+typedef struct acp_case_desc {
+    /* lattice (Control::getNumberOfNodes*, Control.cpp:43-45) */
+    int nx, ny, nz;
+    double spacing;            /* coarse spacing [m] (Spacing) */
+    double domain_size[3];     /* Domain-Size-X/Y/Z [m]; the reference pulse is centred with them */
+    /* physics (Density, KinematicViscosity, SpeedOfSound, MACH-Number) */
+    double density, kinematic_viscosity, speed_of_sound, mach;
+    /* collision */
+    int op;                    /* enum acp_op */
+    int eq_order;              /* Order-Of-Equilibrium: 2, 3 or 4 */
+    int cubic_mach;            /* Cubic-Mach-Correction yes=1 (RR, HRR) */
+    double hybrid_sigma;       /* Hybrid-Parameter (HRR) */
+    int mrt_writeback;         /* 0: as the reference (collision result discarded, Node.cpp:2603,2833); 1: applied */
+    /* boundaries */
+    int bc[3];                 /* enum acp_bc per axis x, y, z */
+    int transverse;            /* Transverse yes=1 */
+    double k1;                 /* K1-Relaxation */
+    /* refinement */
+    int max_level;             /* MaxLevel: 0 or 1 */
+    int layout;                /* enum acp_layout */
+    int ref_layer_yz, ref_layer_x, overlap; /* RefinementLayerYZ, RefinementLayerX, Overlap (shell layout) */
+    int box_lo[3], box_hi[3];  /* refined box in coarse node indices, inclusive (box layout) */
+    int coupling;              /* enum acp_coupling */
+    int f2c_filter;            /* enum acp_f2c_filter */
+    int scaling_style;         /* enum acp_scaling */
+    int c2f_replace;           /* enum acp_c2f_replace */
+    int f2c_replace;           /* enum acp_f2c_replace */
+    /* initial condition */
+    int ic;                    /* enum acp_ic */
+    double ic_eps, ic_b;       /* amplitude and half-width (coarse cells) for ACP_IC_GAUSSIAN */
+    double ic_center[3];       /* centre in coarse node coordinates for ACP_IC_GAUSSIAN */
+    int ic_dims;               /* 2: r^2 over x,y only (quasi-2D pulse); 3: over x,y,z */
+    /* precision */
+    int storage;               /* enum acp_storage */
+    int reserved[8];
+} acp_case_desc;
+
+typedef struct acp_handle acp_handle;
+
+/* Fill *d with the reference's defaults (BoundaryConditions.txt as shipped,
+ * single level, FP64). */
+void acp_default_case(acp_case_desc* d);
+
+/* Parse a BoundaryConditions.txt file with the reference's keyword rules
+ * (Control::readValue/readString, Control.cpp:135-204): first token matched
+ * exactly, missing mandatory keyword is an error.  Optional keywords added by
+ * this engine (Periodic-X/Y/Z, Pulse-*, Refinement-Box-*, Storage,
+ * MRT-Write-Back, Layout) keep the reference defaults when absent. */
+int acp_parse_case_file(const char* path, acp_case_desc* d, char* err, size_t err_len);
+
+/* Replaces Lattice(Control&) (Lattice.h:23-57): validates the case, builds
+ * the node types and boundary wiring, allocates device state.  device < 0
+ * means the current device. */
+int acp_create(const acp_case_desc* d, int device, acp_handle** out);
+/* Replaces Lattice::initialization (Lattice.cpp:1397-1493). */
+int acp_init(acp_handle* h);
+/* Replaces n calls of Lattice::solve(alt) / solve(alt0, alt1)
+ * (Lattice.cpp:2158-2210): n coarse steps, asynchronous on the handle's
+ * stream. */
+int acp_step(acp_handle* h, int n_coarse_steps);
+/* Wait for the handle's stream; reports a device-side numeric fault. */
+int acp_sync(acp_handle* h);
+/* Node counts of a level's dense box (nodes = dims[0]*dims[1]*dims[2]). */
+int acp_level_dims(acp_handle* h, int level, int dims[3]);
+/* Nodes updated per coarse step, for MLUPS: coarse active + 2 * fine active. */
+int acp_active_updates(acp_handle* h, long long* coarse_nodes, long long* fine_nodes);
+/* Populations of a level as FP64 f_i (see header comment), host buffer of
+ * 19 * nodes doubles; replaces Lattice::getDistribution (Lattice.h:119). */
+int acp_read_populations(acp_handle* h, int level, double* host_out);
+/* Overwrite a level's populations (both ping-pong arrays) from FP64 f_i. */
+int acp_write_populations(acp_handle* h, int level, const double* host_in);
+/* A macroscopic field of a level (SI: kg/m^3, m/s, Pa), host buffer of nodes doubles. */
+int acp_read_field(acp_handle* h, int level, int field, double* host_out);
+/* Pressure probes: n probes at (level, i, j, k) quadruples; sampled after every coarse step into an FP64 device buffer. */
+int acp_set_probes(acp_handle* h, int n, const int* level_ijk);
+/* Copy the probe series: out[sample * n + probe] in Pa; *n_samples set to the count. */
+int acp_read_probes(acp_handle* h, double* out, int max_samples, int* n_samples);
+/* Coarse steps done since acp_init. */
+int acp_steps_done(acp_handle* h, long long* steps);
+/* Bind the handle to a caller-owned cudaStream_t (NULL: the handle's own). */
+int acp_set_stream(acp_handle* h, void* cuda_stream);
+/* Device bytes the handle holds. */
+int acp_device_bytes(acp_handle* h, size_t* bytes);
+/* Device bytes a case would hold, without allocating (admission by HBM footprint). */
+int acp_estimate_bytes(const acp_case_desc* d, size_t* bytes);
+int acp_destroy(acp_handle* h);
+const char* acp_last_error(const acp_handle* h);
+const char* acp_status_string(int status);
+int acp_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ACP_H */

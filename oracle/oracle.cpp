@@ -1,0 +1,546 @@
+// FP64 CPU oracle for the acPulse_vcLBM hot path.
+//
+// TEST INFRASTRUCTURE ONLY.  This is a restatement of the reference's
+// algorithm used as the checker: tests/, __graft_entry__.smoke() and the CPU
+// baseline of bench.py call it; the engine never does.
+//
+// Single level (MaxLevel 0): Lattice::timeStepping{SRT,MRT_GS,MRT_RM,RR,HRR}
+// (Lattice.cpp:1496-2156) with the per-node operators of Node.cpp, restated
+// with the reference's floating-point evaluation order (oracle_ops.h), push
+// streaming (FluidNode.h:22-32, BoundaryNode.h:22-32) and LODI boundary passes
+// in the reference's order: x faces, then z faces, then y faces
+// (Lattice.cpp:1582-1624).  Pinned bit-for-bit against the reference built
+// from its own sources (tests/golden/).
+//
+// Extensions of the reference, used by the pulse configurations: periodic
+// axes (no boundary nodes, wrapped neighbours), the Gaussian pulse initial
+// condition in lattice cells, and the MRT write-back switch.
+#include "oracle_ops.h"
+#include "oracle_topology.h"
+#include "../include/acp.h"
+
+#include <omp.h>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace orc {
+
+enum NodeType : unsigned char { NT_INTERIOR = 0, NT_BOUNDARY = 1 };
+
+struct BNode {
+    long n;           // node index
+    int cls;          // index into kBoundaryClasses
+    long n1, n2;      // normal neighbours
+    long t[4];        // tangent neighbours (-1: none)
+    int corner;
+    int pass;         // 0: x faces, 1: z faces, 2: y faces
+};
+
+struct Level {
+    int nx, ny, nz;
+    long N;
+    std::vector<double> f[2];  // [N][19] per ping-pong array (Node::distr_)
+    std::vector<double> preCol;
+    std::vector<double> psi;   // Node::psi_ (cubic-Mach correction, persistent)
+    std::vector<unsigned char> type;
+    std::vector<BNode> bnodes;
+    std::vector<long> nb;      // [N][18] push targets (-1: none)
+    double dt, omega, spacing;
+    long idx(int i, int j, int k) const { return ((long)k * ny + j) * nx + i; }
+};
+
+struct Mat19 {
+    double a[Q][Q];
+};
+
+static bool invert19(const Mat19& m, Mat19& inv) {
+    double aug[Q][2 * Q];
+    for (int r = 0; r < Q; ++r)
+        for (int c = 0; c < Q; ++c) {
+            aug[r][c] = m.a[r][c];
+            aug[r][Q + c] = r == c ? 1. : 0.;
+        }
+    for (int c = 0; c < Q; ++c) {
+        int p = c;
+        for (int r = c + 1; r < Q; ++r)
+            if (std::fabs(aug[r][c]) > std::fabs(aug[p][c])) p = r;
+        if (std::fabs(aug[p][c]) < 1e-12) return false;
+        if (p != c)
+            for (int k = 0; k < 2 * Q; ++k) std::swap(aug[p][k], aug[c][k]);
+        double piv = aug[c][c];
+        for (int k = 0; k < 2 * Q; ++k) aug[c][k] /= piv;
+        for (int r = 0; r < Q; ++r) {
+            if (r == c) continue;
+            double fct = aug[r][c];
+            if (fct == 0.) continue;
+            for (int k = 0; k < 2 * Q; ++k) aug[r][k] -= fct * aug[c][k];
+        }
+    }
+    for (int r = 0; r < Q; ++r)
+        for (int c = 0; c < Q; ++c) inv.a[r][c] = aug[r][Q + c];
+    return true;
+}
+
+// Gram-Schmidt moment basis of Node::calcAllMoments_GSbasis
+// (Node.cpp:2934-3004), in lattice units (the c^n factors cancel against the
+// back transform of Node.cpp:2870-2931).
+static void gsBasis(Mat19& M) {
+    for (int d = 0; d < Q; ++d) {
+        int ex = EX[d], ey = EY[d], ez = EZ[d];
+        int e2 = ex * ex + ey * ey + ez * ez;
+        bool axis = e2 == 1;
+        double col[Q];
+        col[0] = 1;
+        col[1] = d == 18 ? -1 : (e2 == 2 ? 1 : 0);
+        col[2] = axis ? -2 : 1;
+        col[3] = ex;
+        col[4] = ex * (axis ? -2 : 1);
+        col[5] = ey;
+        col[6] = ey * (axis ? -2 : 1);
+        col[7] = ez;
+        col[8] = ez * (axis ? -2 : 1);
+        col[9] = 3 * ex * ex - e2;
+        col[10] = (3 * ex * ex - e2) * (axis ? -1 : 1);
+        col[11] = ey * ey - ez * ez;
+        col[12] = (ey * ey - ez * ez) * (axis ? -1 : 1);
+        col[13] = ex * ey;
+        col[14] = ey * ez;
+        col[15] = ex * ez;
+        col[16] = ex * (ey * ey - ez * ez);
+        col[17] = ey * (ez * ez - ex * ex);
+        col[18] = ez * (ex * ex - ey * ey);
+        for (int m = 0; m < Q; ++m) M.a[m][d] = col[m];
+    }
+}
+
+// Raw-moment basis of Node::calcAllMoments_RMbasis (Node.cpp:2693-2762),
+// lattice units.
+static void rmBasis(Mat19& M) {
+    for (int d = 0; d < Q; ++d) {
+        int ex = EX[d], ey = EY[d], ez = EZ[d];
+        double col[Q] = {1., (double)ex, (double)ey, (double)ez, (double)(ex * ex + ey * ey + ez * ez),
+                         (double)(ex * ex - ez * ez), (double)(ey * ey - ez * ez), (double)(ex * ey),
+                         (double)(ex * ez), (double)(ey * ez), (double)(ex * ex * ez), (double)(ex * ez * ez),
+                         (double)(ey * ey * ez), (double)(ey * ez * ez), (double)(ex * ex * ey),
+                         (double)(ex * ey * ey), (double)(ex * ex * ez * ez), (double)(ex * ex * ey * ey),
+                         (double)(ey * ey * ez * ez)};
+        for (int m = 0; m < Q; ++m) M.a[m][d] = col[m];
+    }
+}
+
+// Node::calcEquilibrium4_RMbasis (Node.cpp:2607-2647), lattice units.
+static void equilibriumRM(double rho, const double* u, double* eq) {
+    const double w[Q] = {1. / 18, 1. / 18, 1. / 18, 1. / 18, 1. / 18, 1. / 18, 1. / 36, 1. / 36, 1. / 36, 1. / 36,
+                         1. / 36, 1. / 36, 1. / 36, 1. / 36, 1. / 36, 1. / 36, 1. / 36, 1. / 36, 1. / 3};
+    double u2[3] = {u[0] * u[0], u[1] * u[1], u[2] * u[2]};
+    for (int d = 0; d < Q; ++d) {
+        int e[3] = {EX[d], EY[d], EZ[d]};
+        int nz = (e[0] != 0) + (e[1] != 0) + (e[2] != 0);
+        double s;
+        if (nz == 0) {
+            s = 1 - (u2[0] + u2[1] + u2[2]) + 3 * (u2[0] * u2[1] + u2[0] * u2[2] + u2[1] * u2[2]);
+        } else if (nz == 1) {
+            int a = e[0] ? 0 : (e[1] ? 1 : 2);
+            int b = (a + 1) % 3, c = (a + 2) % 3;
+            double sg = e[a];
+            s = 1 + 3 * sg * u[a] + 3 * (u2[a] - u2[b] - u2[c]) - 9 * sg * u[a] * (u2[b] + u2[c]) -
+                9 * u2[a] * (u2[b] + u2[c]);
+        } else {
+            int a = e[0] ? 0 : 1;
+            int b = e[2] ? 2 : 1;
+            double sa = e[a], sb = e[b];
+            s = 1 + 3 * (sa * u[a] + sb * u[b]) + 3 * (u2[a] + u2[b]) + 9 * sa * sb * u[a] * u[b] +
+                9 * (sb * u2[a] * u[b] + sa * u[a] * u2[b]) + 9 * u2[a] * u2[b];
+        }
+        eq[d] = rho * w[d] * s;
+    }
+}
+
+struct Oracle {
+    acp_case_desc desc;
+    Consts k;
+    std::vector<Level> lev;
+    int alt = 1;  // main.cpp:55: alternatingL0 = true; state is in f[alt]
+    long long steps = 0;
+    Mat19 gsM, gsMinv, rmM, rmMinv;
+    std::string err;
+    int threads = 1;
+
+    bool build() {
+        const acp_case_desc& d = desc;
+        if (d.max_level != 0) { err = "oracle: two-level cases are built by the two-level oracle"; return false; }
+        k.setup(d.speed_of_sound, d.spacing, d.kinematic_viscosity, d.density, d.mach, d.k1, d.hybrid_sigma, d.eq_order,
+                d.cubic_mach != 0 && (d.op == ACP_OP_RR || d.op == ACP_OP_HRR), d.transverse != 0);
+        gsBasis(gsM);
+        rmBasis(rmM);
+        if (!invert19(gsM, gsMinv) || !invert19(rmM, rmMinv)) { err = "moment basis not invertible"; return false; }
+        lev.resize(1);
+        Level& L = lev[0];
+        L.nx = d.nx; L.ny = d.ny; L.nz = d.nz;
+        L.N = (long)L.nx * L.ny * L.nz;
+        for (int a = 0; a < 2; ++a) L.f[a].assign(L.N * Q, 0.);
+        L.preCol.assign(L.N * Q, 0.);
+        L.psi.assign(L.N * Q, 0.);
+        L.type.assign(L.N, NT_INTERIOR);
+        L.nb.assign(L.N * 18, -1);
+        L.dt = k.dt(0);
+        L.omega = k.omega(0);
+        L.spacing = k.spacing;
+        const int dims[3] = {L.nx, L.ny, L.nz};
+        for (int a = 0; a < 3; ++a) {
+            if (d.bc[a] == ACP_BC_LODI && dims[a] < 4) { err = "LODI axes need at least 4 nodes"; return false; }
+            if (d.bc[a] == ACP_BC_PERIODIC && dims[a] < 1) { err = "empty axis"; return false; }
+        }
+        auto wrapped = [&](int i, int j, int kk, long& out) {
+            int c[3] = {i, j, kk};
+            for (int a = 0; a < 3; ++a) {
+                if (c[a] < 0 || c[a] >= dims[a]) {
+                    if (d.bc[a] != ACP_BC_PERIODIC) return false;
+                    c[a] = (c[a] % dims[a] + dims[a]) % dims[a];
+                }
+            }
+            out = L.idx(c[0], c[1], c[2]);
+            return true;
+        };
+        for (int kk = 0; kk < L.nz; ++kk)
+            for (int j = 0; j < L.ny; ++j)
+                for (int i = 0; i < L.nx; ++i) {
+                    int c[3] = {i, j, kk};
+                    int fc[3];
+                    for (int a = 0; a < 3; ++a)
+                        fc[a] = d.bc[a] == ACP_BC_LODI ? (c[a] == 0 ? -1 : (c[a] == dims[a] - 1 ? 1 : 0)) : 0;
+                    long n = L.idx(i, j, kk);
+                    if (fc[0] == 0 && fc[1] == 0 && fc[2] == 0) {
+                        for (int q = 0; q < 18; ++q) {
+                            long t;
+                            if (!wrapped(i + EX[q], j + EY[q], kk + EZ[q], t)) { err = "interior neighbour missing"; return false; }
+                            L.nb[n * 18 + q] = t;
+                        }
+                        continue;
+                    }
+                    L.type[n] = NT_BOUNDARY;
+                    const BClass* bc = boundaryClass(fc[0], fc[1], fc[2]);
+                    BNode b;
+                    b.n = n;
+                    b.cls = (int)(bc - kBoundaryClasses);
+                    b.corner = bc->corner;
+                    if (!wrapped(i + bc->n1[0], j + bc->n1[1], kk + bc->n1[2], b.n1) ||
+                        !wrapped(i + bc->n2[0], j + bc->n2[1], kk + bc->n2[2], b.n2)) {
+                        err = "normal neighbour missing"; return false;
+                    }
+                    for (int m = 0; m < 4; ++m) b.t[m] = -1;
+                    int nface = (fc[0] != 0) + (fc[1] != 0) + (fc[2] != 0);
+                    if (nface == 1) {
+                        int t[4][3];
+                        faceTangents(fc[0], fc[1], fc[2], t);
+                        for (int m = 0; m < 4; ++m)
+                            if (!wrapped(i + t[m][0], j + t[m][1], kk + t[m][2], b.t[m])) { err = "tangent missing"; return false; }
+                    }
+                    for (int m = 0; m < 5 && bc->push[m] >= 0; ++m) {
+                        int q = bc->push[m];
+                        long t;
+                        if (!wrapped(i + EX[q], j + EY[q], kk + EZ[q], t)) { err = "push target missing"; return false; }
+                        L.nb[n * 18 + q] = t;
+                    }
+                    b.pass = fc[0] != 0 ? 0 : (fc[2] != 0 ? 1 : 2);
+                    L.bnodes.push_back(b);
+                }
+        return true;
+    }
+
+    // Lattice::initialization (Lattice.cpp:1397-1493) and the Gaussian pulse
+    // of the pulse configurations.
+    void init() {
+        for (size_t l = 0; l < lev.size(); ++l) {
+            Level& L = lev[l];
+            double sp = k.spacing / std::pow(2., (double)l);
+            for (int kk = 0; kk < L.nz; ++kk)
+                for (int j = 0; j < L.ny; ++j)
+                    for (int i = 0; i < L.nx; ++i) {
+                        double rho;
+                        if (desc.ic == ACP_IC_REFERENCE) {
+                            double Rc = 0.06, A = 0.01, xCenter = -8. * Rc;
+                            double xNode = i * sp - desc.domain_size[0] / 2.;
+                            double yNode = j * sp - desc.domain_size[1] / 2.;
+                            double xRel = xNode - xCenter;
+                            rho = desc.density * (1 + A * std::exp(-(xRel * xRel + yNode * yNode) / (2 * Rc * Rc)));
+                        } else {
+                            double s = 1. / std::pow(2., (double)l);
+                            double dx = i * s - desc.ic_center[0], dy = j * s - desc.ic_center[1];
+                            double dz = desc.ic_dims == 3 ? kk * s - desc.ic_center[2] : 0.;
+                            double r2 = dx * dx + dy * dy + dz * dz;
+                            rho = desc.density * (1 + desc.ic_eps * std::exp(-std::log(2.) * r2 / (desc.ic_b * desc.ic_b)));
+                        }
+                        double u[3] = {0., 0., 0.}, eq[Q];
+                        equilibrium(k, k.order, rho, u, eq);
+                        long n = L.idx(i, j, kk);
+                        for (int q = 0; q < Q; ++q) {
+                            L.f[0][n * Q + q] = eq[q];
+                            L.f[1][n * Q + q] = eq[q];
+                            L.preCol[n * Q + q] = eq[q];
+                            L.psi[n * Q + q] = 0.;
+                        }
+                    }
+        }
+        alt = 1;
+        steps = 0;
+    }
+
+    // Node::collide* on one node, in place (Node.cpp:511-736, 2565-2605, 2798-2835).
+    void collideNode(Level& L, long n, double* f) {
+        int op = desc.op;
+        double dt = L.dt;
+        double* psi = &L.psi[n * Q];
+        if (op == ACP_OP_MRT_GS || op == ACP_OP_MRT_RM) {
+            if (!desc.mrt_writeback) return;  // the reference discards the back transform (Node.cpp:2603,2833)
+            double rho = 0, j[3] = {0, 0, 0};
+            for (int q = 0; q < Q; ++q) {
+                rho += f[q];
+                j[0] += EX[q] * f[q]; j[1] += EY[q] * f[q]; j[2] += EZ[q] * f[q];
+            }
+            if (op == ACP_OP_MRT_GS) {
+                double m[Q], meq[Q] = {0}, s[Q];
+                for (int a = 0; a < Q; ++a) {
+                    m[a] = 0;
+                    for (int q = 0; q < Q; ++q) m[a] += gsM.a[a][q] * f[q];
+                }
+                double jj = j[0] * j[0] + j[1] * j[1] + j[2] * j[2];
+                meq[0] = rho; meq[3] = j[0]; meq[5] = j[1]; meq[7] = j[2];
+                meq[1] = jj / rho;
+                meq[9] = (2 * j[0] * j[0] - j[1] * j[1] - j[2] * j[2]) / rho;
+                meq[11] = (j[1] * j[1] - j[2] * j[2]) / rho;
+                meq[13] = j[0] * j[1] / rho;
+                meq[14] = j[1] * j[2] / rho;
+                meq[15] = j[0] * j[2] / rho;
+                for (int a = 0; a < Q; ++a) s[a] = 1.;
+                s[0] = s[3] = s[5] = s[7] = 0.;
+                s[1] = s[9] = s[11] = s[13] = s[14] = s[15] = L.omega;
+                double dm[Q];
+                for (int a = 0; a < Q; ++a) dm[a] = s[a] * (meq[a] - m[a]);
+                for (int q = 0; q < Q; ++q) {
+                    double acc = 0;
+                    for (int a = 0; a < Q; ++a) acc += gsMinv.a[q][a] * dm[a];
+                    f[q] += acc;
+                }
+            } else {
+                double u[3] = {j[0] / rho, j[1] / rho, j[2] / rho}, eq[Q], m[Q], meq[Q];
+                equilibriumRM(rho, u, eq);
+                for (int a = 0; a < Q; ++a) {
+                    m[a] = 0; meq[a] = 0;
+                    for (int q = 0; q < Q; ++q) { m[a] += rmM.a[a][q] * f[q]; meq[a] += rmM.a[a][q] * eq[q]; }
+                }
+                for (int a = 0; a < Q; ++a) {
+                    double s = (a >= 5 && a <= 9) ? L.omega : 1.;
+                    m[a] += s * (meq[a] - m[a]);
+                }
+                for (int q = 0; q < Q; ++q) {
+                    double acc = 0;
+                    for (int a = 0; a < Q; ++a) acc += rmMinv.a[q][a] * m[a];
+                    f[q] = acc;
+                }
+            }
+            return;
+        }
+        double dens = density(k, f, psi, dt);
+        double u[3];
+        velocity(k, f, psi, dt, dens, u);
+        double eq[Q];
+        equilibrium(k, k.order, dens, u, eq);
+        if (op == ACP_OP_SRT) {
+            for (int q = 0; q < Q; ++q) f[q] += L.omega * (eq[q] - f[q]);
+            return;
+        }
+        bool needStrain = (op == ACP_OP_HRR) || k.cubic;
+        double S[6] = {0, 0, 0, 0, 0, 0};
+        if (needStrain) {
+            // neighbours' pre-collision moments (calcDensityPreCol/VelocityPreCol)
+            double nbRho[6], nbU[6][3], dist[6];
+            const int axisDir[6] = {0, 1, 2, 3, 4, 5};
+            for (int a = 0; a < 6; ++a) {
+                long m = L.nb[n * 18 + axisDir[a]];
+                plainMoments(k, &L.preCol[m * Q], nbRho[a], nbU[a]);
+                dist[a] = L.spacing;
+            }
+            strainAndPsi(k, nbRho, nbU, dist, S, psi);
+        }
+        double P[6];
+        pi1(k, f, eq, psi, dt, P);
+        double neq[Q];
+        if (op == ACP_OP_RR) {
+            recursiveNeq(k, k.order, P, u, neq);
+        } else {
+            double densH = density(k, f, psi, dt);
+            double kinVisc = k.nu;
+            double dynVisc = kinVisc * densH;
+            double invPreFactor = -((dt * k.cs2) / (L.omega * kinVisc));
+            double sg = k.sigma, a[6];
+            for (int c = 0; c < 6; ++c) a[c] = sg * P[c] + (1. - sg) * invPreFactor * (2. * dynVisc * S[c]);
+            recursiveNeq(k, k.order, a, u, neq);
+        }
+        if (k.cubic) {
+            for (int q = 0; q < Q; ++q) f[q] = eq[q] + (1 - L.omega) * neq[q] + 0.5 * dt * psi[q];
+        } else {
+            for (int q = 0; q < Q; ++q) f[q] = eq[q] + (1 - L.omega) * neq[q];
+        }
+    }
+
+    // Node::LODIpressureOutlet (Node.cpp:229-443) writing array `nw`.
+    void lodiNode(Level& L, int level, const BNode& b, int nw) {
+        int od = 1 - nw;
+        const double* fo = L.f[od].data();
+        const double* fn = L.f[nw].data();
+        double dt = L.dt;
+        double localSpacing = k.spacing * std::pow(2., -level);
+        double densB = density(k, &fo[b.n * Q], &L.psi[b.n * Q], dt);
+        double veloB[3];
+        velocity(k, &fo[b.n * Q], &L.psi[b.n * Q], dt, densB, veloB);
+        double dG = 0, vG[3] = {0, 0, 0}, dGT[2] = {0, 0}, vGT[2][3] = {{0, 0, 0}, {0, 0, 0}};
+        {
+            double dN = density(k, &fn[b.n1 * Q], &L.psi[b.n1 * Q], dt);
+            double d2N = density(k, &fn[b.n2 * Q], &L.psi[b.n2 * Q], dt);
+            dG = (4. * dN - d2N - 3. * densB) / (-2. * localSpacing);
+            double vN[3], v2N[3];
+            velocity(k, &fn[b.n1 * Q], &L.psi[b.n1 * Q], dt, dN, vN);
+            velocity(k, &fn[b.n2 * Q], &L.psi[b.n2 * Q], dt, d2N, v2N);
+            for (int c = 0; c < 3; ++c) vG[c] = (4. * vN[c] - v2N[c] - 3. * veloB[c]) / (-2. * localSpacing);
+            if (!b.corner && k.transverse) {
+                double dT[4], vT[4][3];
+                for (int m = 0; m < 4; ++m) {
+                    dT[m] = density(k, &fo[b.t[m] * Q], &L.psi[b.t[m] * Q], dt);
+                    velocity(k, &fo[b.t[m] * Q], &L.psi[b.t[m] * Q], dt, dT[m], vT[m]);
+                }
+                dGT[0] = (dT[0] - dT[1]) / (2. * localSpacing);
+                dGT[1] = (dT[2] - dT[3]) / (2. * localSpacing);
+                for (int c = 0; c < 3; ++c) {
+                    vGT[0][c] = (vT[0][c] - vT[1][c]) / (2. * localSpacing);
+                    vGT[1][c] = (vT[2][c] - vT[3][c]) / (2. * localSpacing);
+                }
+            }
+        }
+        int nd = kBoundaryClasses[b.cls].normalDir;
+        double density = 0., velocity[3] = {0, 0, 0};
+        // axis permutation into the boundary frame (normal first), Node.cpp:305-414
+        int perm[3];
+        bool neg;
+        double L0;
+        if (nd == 0 || nd == 2) { perm[0] = 0; perm[1] = 1; perm[2] = 2; L0 = desc.nx * k.spacing; }
+        else if (nd == 1 || nd == 3) { perm[0] = 1; perm[1] = 0; perm[2] = 2; L0 = desc.ny * k.spacing; }
+        else { perm[0] = 2; perm[1] = 0; perm[2] = 1; L0 = desc.nz * k.spacing; }
+        neg = (nd == 0 || nd == 1 || nd == 4);
+        if (neg) {
+            dG *= -1.;
+            for (int c = 0; c < 3; ++c) vG[c] *= -1.;
+        }
+        double sVG[3], sVB[3], sVGT[2][3];
+        for (int c = 0; c < 3; ++c) {
+            sVG[c] = vG[perm[c]];
+            sVB[c] = veloB[perm[c]];
+            sVGT[0][c] = vGT[0][perm[c]];
+            sVGT[1][c] = vGT[1][perm[c]];
+        }
+        double v[3];
+        lodiIntegrate(k, dt, L0, density, densB, dG, sVG, sVB, v, neg, dGT, sVGT);
+        for (int c = 0; c < 3; ++c) velocity[perm[c]] = v[c];
+        double eq[Q];
+        equilibrium(k, k.order, density, velocity, eq);
+        double* out = &L.f[nw][b.n * Q];
+        for (int q = 0; q < Q; ++q) out[q] = eq[q];
+    }
+
+    void stepSingle() {
+        Level& L = lev[0];
+        int a = alt, nw = 1 - alt;
+        double* A = L.f[a].data();
+        double* B = L.f[nw].data();
+        std::memcpy(L.preCol.data(), A, sizeof(double) * L.N * Q);
+        const long N = L.N;
+#pragma omp parallel for num_threads(threads) schedule(static)
+        for (long n = 0; n < N; ++n) {
+            if (L.type[n] != NT_INTERIOR) continue;
+            double* f = &A[n * Q];
+            collideNode(L, n, f);
+            for (int q = 0; q < 18; ++q) B[L.nb[n * 18 + q] * Q + q] = f[q];
+            B[n * Q + 18] = f[18];
+        }
+        for (const BNode& b : L.bnodes) {
+            for (int q = 0; q < 18; ++q) {
+                long t = L.nb[b.n * 18 + q];
+                if (t >= 0) B[t * Q + q] = A[b.n * Q + q];
+            }
+            B[b.n * Q + 18] = A[b.n * Q + 18];
+        }
+        for (int pass = 0; pass < 3; ++pass) {
+            const long nb = (long)L.bnodes.size();
+#pragma omp parallel for num_threads(threads) schedule(static)
+            for (long m = 0; m < nb; ++m)
+                if (L.bnodes[m].pass == pass) lodiNode(L, 0, L.bnodes[m], nw);
+        }
+        alt = nw;
+        ++steps;
+    }
+};
+
+}  // namespace orc
+
+using orc::Oracle;
+
+extern "C" {
+
+void* orc_create(const acp_case_desc* d, int threads, char* err, int errlen) {
+    Oracle* o = new Oracle();
+    o->desc = *d;
+    o->threads = threads > 0 ? threads : omp_get_max_threads();
+    if (!o->build()) {
+        if (err && errlen > 0) std::snprintf(err, errlen, "%s", o->err.c_str());
+        delete o;
+        return nullptr;
+    }
+    return o;
+}
+
+int orc_init(void* h) {
+    static_cast<Oracle*>(h)->init();
+    return 0;
+}
+
+int orc_step(void* h, int n) {
+    Oracle* o = static_cast<Oracle*>(h);
+    for (int s = 0; s < n; ++s) o->stepSingle();
+    return 0;
+}
+
+int orc_dims(void* h, int level, int* dims) {
+    Oracle* o = static_cast<Oracle*>(h);
+    if (level < 0 || level >= (int)o->lev.size()) return -1;
+    dims[0] = o->lev[level].nx; dims[1] = o->lev[level].ny; dims[2] = o->lev[level].nz;
+    return 0;
+}
+
+// structure-of-arrays output: out[(q*nz + k)*ny + j)*nx + i]
+int orc_read_populations(void* h, int level, double* out) {
+    Oracle* o = static_cast<Oracle*>(h);
+    if (level < 0 || level >= (int)o->lev.size()) return -1;
+    const orc::Level& L = o->lev[level];
+    const double* f = L.f[o->alt].data();
+    for (long n = 0; n < L.N; ++n)
+        for (int q = 0; q < orc::Q; ++q) out[(long)q * L.N + n] = f[n * orc::Q + q];
+    return 0;
+}
+
+int orc_write_populations(void* h, int level, const double* in) {
+    Oracle* o = static_cast<Oracle*>(h);
+    if (level < 0 || level >= (int)o->lev.size()) return -1;
+    orc::Level& L = o->lev[level];
+    for (int a = 0; a < 2; ++a)
+        for (long n = 0; n < L.N; ++n)
+            for (int q = 0; q < orc::Q; ++q) L.f[a][n * orc::Q + q] = in[(long)q * L.N + n];
+    return 0;
+}
+
+long long orc_steps_done(void* h) { return static_cast<Oracle*>(h)->steps; }
+
+void orc_destroy(void* h) { delete static_cast<Oracle*>(h); }
+
+}  // extern "C"
