@@ -1,0 +1,210 @@
+// D3Q19 lattice and the per-node collision operators of the acPulse_vcLBM hot
+// path, written for registers: everything is in lattice units (velocities
+// divided by the molecular velocity c = sqrt(3) cs, time in level steps), and
+// populations are handled as deviations g_i = f_i - w_i * shift, where shift
+// is the reference density for the deviation storage forms and 0 for the
+// plain FP64 form.  Every direction loop is unrolled so the Hermite tensors of
+// each direction become compile-time constants.
+//
+// Reference operators restated here (Node.cpp): calcEquilibrium{2,3,4}_GHbasis
+// 739-1132, calcPi1Tensor 2493-2558, calcRRoffEquilibrium{2,3,4} 1136-1427,
+// calcHRRoffEquilibrium{2,3,4} 1430-1747, the strain-rate / cubic-Mach
+// correction 1750-1889, collideSRT/RR/HRR 511-736, collideMRT_GSbasis
+// 2798-2835 and collideMRT_RMbasis 2565-2605.  The SI formulas of the
+// reference map to lattice units exactly except for the orthogonalisation of
+// the fourth-order Hermite terms, which adds a second-order tensor with the
+// dimensional factor 1/6 (Node.cpp:1087-1089); in lattice units that factor
+// becomes kappa = 1 / (6 c^2), carried as a per-case constant.
+#pragma once
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+
+namespace acp {
+
+constexpr int Q = 19;
+// direction order of Control.cpp:58-116
+__host__ __device__ constexpr int ex(int q) {
+    return q == 0 || q == 6 || q == 7 || q == 15 || q == 16 ? 1 : (q == 2 || q == 10 || q == 11 || q == 14 || q == 17 ? -1 : 0);
+}
+__host__ __device__ constexpr int ey(int q) {
+    return q == 1 || q == 8 || q == 9 || q == 14 || q == 16 ? 1 : (q == 3 || q == 12 || q == 13 || q == 15 || q == 17 ? -1 : 0);
+}
+__host__ __device__ constexpr int ez(int q) {
+    return q == 4 || q == 6 || q == 8 || q == 10 || q == 12 ? 1 : (q == 5 || q == 7 || q == 9 || q == 11 || q == 13 ? -1 : 0);
+}
+__host__ __device__ constexpr double wq(int q) { return q < 6 ? 1.0 / 18.0 : (q < 18 ? 1.0 / 36.0 : 1.0 / 3.0); }
+
+// operator ids (enum acp_op)
+enum { OP_SRT = 0, OP_MRT_GS = 1, OP_MRT_RM = 2, OP_RR = 3, OP_HRR = 4 };
+
+// second-order Hermite tensor components (lattice): e_a e_b - delta_ab / 3
+template <typename R>
+__host__ __device__ constexpr R h2xx(int q) { return R(ex(q) * ex(q)) - R(1) / R(3); }
+template <typename R>
+__host__ __device__ constexpr R h2yy(int q) { return R(ey(q) * ey(q)) - R(1) / R(3); }
+template <typename R>
+__host__ __device__ constexpr R h2zz(int q) { return R(ez(q) * ez(q)) - R(1) / R(3); }
+
+// H2 : A for a symmetric tensor A = {xx, yy, zz, xy, xz, yz}
+template <typename R>
+__device__ __forceinline__ R h2dot(int q, const R* A) {
+    return h2xx<R>(q) * A[0] + h2yy<R>(q) * A[1] + h2zz<R>(q) * A[2] +
+           R(2) * (R(ex(q) * ey(q)) * A[3] + R(ex(q) * ez(q)) * A[4] + R(ey(q) * ez(q)) * A[5]);
+}
+
+// sum of the six orthogonal third-order Hermite terms, weighted as the
+// reference weights them (x3 for the symmetric combinations, x1 for the
+// antisymmetric ones, Node.cpp:942-947):  a = {xxy+yzz, xxz+yyz, xyy+xzz,
+// yzz-xxy, yyz-xxz, xzz-xyy}
+template <typename R>
+__device__ __forceinline__ R h3dot(int q, const R* a) {
+    const R hx = R(ex(q)), hy = R(ey(q)), hz = R(ez(q));
+    const R xxy = h2xx<R>(q) * hy, xyy = h2yy<R>(q) * hx, xxz = h2xx<R>(q) * hz;
+    const R xzz = h2zz<R>(q) * hx, yyz = h2yy<R>(q) * hz, yzz = h2zz<R>(q) * hy;
+    return R(3) * ((xxy + yzz) * a[0] + (xxz + yyz) * a[1] + (xyy + xzz) * a[2]) + (yzz - xxy) * a[3] +
+           (yyz - xxz) * a[4] + (xzz - xyy) * a[5];
+}
+
+// fully orthogonalised fourth-order combination (Node.cpp:1082-1094, 1130):
+// orth(p, s) with p = {xxyy, xxzz, yyzz} products and s = {xx, yy, zz}
+template <typename R>
+__device__ __forceinline__ void orth4(R pxxyy, R pxxzz, R pyyzz, R sxx, R syy, R szz, R kappa, R* fo) {
+    fo[0] = pxxyy + kappa * szz;
+    fo[1] = pxxzz + kappa * syy + R(2.0 / 7.0) * fo[0];
+    fo[2] = pyyzz + kappa * sxx + R(2.0 / 7.0) * fo[0] + R(2.0 / 5.0) * fo[1];
+}
+template <typename R>
+__device__ __forceinline__ R h4dot(int q, const R* a4, R kappa) {
+    R h[3];
+    orth4<R>(h2xx<R>(q) * h2yy<R>(q), h2xx<R>(q) * h2zz<R>(q), h2yy<R>(q) * h2zz<R>(q), h2xx<R>(q), h2yy<R>(q),
+             h2zz<R>(q), kappa, h);
+    return R(8.0 / 7.0) * h[0] * a4[0] + R(56.0 / 45.0) * h[1] * a4[1] + R(40.0 / 27.0) * h[2] * a4[2];
+}
+
+// Velocity coefficients of the Hermite equilibrium up to `ORDER`.
+template <typename R, int ORDER>
+struct EqCoef {
+    R u[3];
+    R uu[6];  // xx yy zz xy xz yz
+    R a3[6];
+    R a4[3];
+    __device__ __forceinline__ void set(const R* v, R kappa) {
+        u[0] = v[0]; u[1] = v[1]; u[2] = v[2];
+        uu[0] = v[0] * v[0]; uu[1] = v[1] * v[1]; uu[2] = v[2] * v[2];
+        uu[3] = v[0] * v[1]; uu[4] = v[0] * v[2]; uu[5] = v[1] * v[2];
+        if (ORDER >= 3) {
+            const R xxy = v[1] * uu[0], xyy = v[0] * uu[1], xxz = v[2] * uu[0];
+            const R xzz = v[0] * uu[2], yyz = v[2] * uu[1], yzz = v[1] * uu[2];
+            a3[0] = xxy + yzz; a3[1] = xxz + yyz; a3[2] = xyy + xzz;
+            a3[3] = yzz - xxy; a3[4] = yyz - xxz; a3[5] = xzz - xyy;
+            if (ORDER == 4) orth4<R>(uu[0] * uu[1], uu[0] * uu[2], uu[1] * uu[2], uu[0], uu[1], uu[2], kappa, a4);
+        }
+    }
+    // feq_q / (rho w_q) - 1
+    __device__ __forceinline__ R poly(int q, R kappa) const {
+        R eu = R(ex(q)) * u[0] + R(ey(q)) * u[1] + R(ez(q)) * u[2];
+        R p = R(3) * eu + R(4.5) * h2dot<R>(q, uu);
+        if (ORDER >= 3) p += R(4.5) * h3dot<R>(q, a3);
+        if (ORDER == 4) p += R(20.25) * h4dot<R>(q, a4, kappa);
+        return p;
+    }
+};
+
+// Recursive off-equilibrium of a second-order coefficient tensor A
+// (RR: A = Pi1; HRR: A = hybrid of Pi1 and the finite-difference strain).
+template <typename R, int ORDER>
+struct NeqCoef {
+    R A[6];
+    R a3[6];
+    R a4[3];
+    __device__ __forceinline__ void set(const R* Ain, const R* u, R kappa) {
+        for (int c = 0; c < 6; ++c) A[c] = Ain[c];
+        if (ORDER >= 3) {
+            const R Pxx = A[0], Pyy = A[1], Pzz = A[2], Pxy = A[3], Pxz = A[4], Pyz = A[5];
+            const R xxy = R(2) * u[0] * Pxy + u[1] * Pxx;
+            const R xyy = R(2) * u[1] * Pxy + u[0] * Pyy;
+            const R xxz = R(2) * u[0] * Pxz + u[2] * Pxx;
+            const R xzz = R(2) * u[2] * Pxz + u[0] * Pzz;
+            const R yyz = R(2) * u[1] * Pyz + u[2] * Pyy;
+            const R yzz = R(2) * u[2] * Pyz + u[1] * Pzz;
+            a3[0] = xxy + yzz; a3[1] = xxz + yyz; a3[2] = xyy + xzz;
+            a3[3] = yzz - xxy; a3[4] = yyz - xxz; a3[5] = xzz - xyy;
+            if (ORDER == 4) {
+                const R xxyy = u[1] * u[1] * Pxx + u[0] * u[0] * Pyy + R(4) * u[0] * u[1] * Pxy;
+                const R xxzz = u[2] * u[2] * Pxx + u[0] * u[0] * Pzz + R(4) * u[0] * u[2] * Pxz;
+                const R yyzz = u[1] * u[1] * Pzz + u[2] * u[2] * Pyy + R(4) * u[1] * u[2] * Pyz;
+                orth4<R>(xxyy, xxzz, yyzz, Pxx, Pyy, Pzz, kappa, a4);
+            }
+        }
+    }
+    // neq_q / w_q
+    __device__ __forceinline__ R poly(int q, R kappa) const {
+        R p = R(4.5) * h2dot<R>(q, A);
+        if (ORDER >= 3) p += R(4.5) * h3dot<R>(q, a3);
+        if (ORDER == 4) p += R(20.25) * h4dot<R>(q, a4, kappa);
+        return p;
+    }
+};
+
+// moment rows (integer coefficients) of the two MRT bases, in lattice units
+// Gram-Schmidt basis (Node.cpp:2934-3004)
+__host__ __device__ constexpr int gsRow(int m, int q) {
+    const int x = ex(q), y = ey(q), z = ez(q), e2 = x * x + y * y + z * z;
+    const bool axis = e2 == 1;
+    switch (m) {
+        case 0: return 1;
+        case 1: return q == 18 ? -1 : (e2 == 2 ? 1 : 0);
+        case 2: return axis ? -2 : 1;
+        case 3: return x;
+        case 4: return x * (axis ? -2 : 1);
+        case 5: return y;
+        case 6: return y * (axis ? -2 : 1);
+        case 7: return z;
+        case 8: return z * (axis ? -2 : 1);
+        case 9: return 3 * x * x - e2;
+        case 10: return (3 * x * x - e2) * (axis ? -1 : 1);
+        case 11: return y * y - z * z;
+        case 12: return (y * y - z * z) * (axis ? -1 : 1);
+        case 13: return x * y;
+        case 14: return y * z;
+        case 15: return x * z;
+        case 16: return x * (y * y - z * z);
+        case 17: return y * (z * z - x * x);
+        default: return z * (x * x - y * y);
+    }
+}
+// raw-moment basis rows 5..9: the deviatoric second-order moments relaxed with
+// omega (Node.cpp:2720-2733, 2580-2584)
+__host__ __device__ constexpr int rmRow2(int m, int q) {
+    const int x = ex(q), y = ey(q), z = ez(q);
+    switch (m) {
+        case 0: return x * x - z * z;
+        case 1: return y * y - z * z;
+        case 2: return x * y;
+        case 3: return x * z;
+        default: return y * z;
+    }
+}
+
+// storage conversion: populations are stored as S and computed as R
+template <typename S>
+struct Store;
+template <>
+struct Store<double> {
+    __device__ __forceinline__ static double load(const double* p, float) { return *p; }
+    __device__ __forceinline__ static void store(double* p, double v, float) { *p = v; }
+};
+template <>
+struct Store<float> {
+    __device__ __forceinline__ static float load(const float* p, float) { return *p; }
+    __device__ __forceinline__ static void store(float* p, float v, float) { *p = v; }
+};
+template <>
+struct Store<__half> {
+    __device__ __forceinline__ static float load(const __half* p, float scale) { return __half2float(*p) * scale; }
+    __device__ __forceinline__ static void store(__half* p, float v, float scale) {
+        *p = __float2half_rn(v * (1.0f / scale));
+    }
+};
+
+}  // namespace acp

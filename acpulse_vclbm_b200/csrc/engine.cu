@@ -1,0 +1,868 @@
+// Host side of the engine: case validation, node classes and boundary wiring,
+// device memory, kernel dispatch, CUDA-graph stepping and the C ABI of
+// include/acp.h.
+#include "../../include/acp.h"
+#include "kernels.cuh"
+#include "topology.h"
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <algorithm>
+#include <mutex>
+#include <string>
+#include <vector>
+
+using namespace acp;
+
+namespace {
+
+struct LevelHost {
+    int nx = 0, ny = 0, nz = 0;
+    long long N = 0;
+    int off[3] = {0, 0, 0};  // box origin in this level's global node index
+    std::vector<uint8_t> code;
+    std::vector<BNodeDev> lodiX, lodiZY;
+    long long active = 0;
+    double omega = 0, dt = 0, spacing = 0;
+};
+
+struct LevelDev {
+    void* f[2] = {nullptr, nullptr};
+    uint8_t* code = nullptr;
+    Moments* mom = nullptr;
+    BNodeDev* lodiX = nullptr;
+    BNodeDev* lodiZY = nullptr;
+    int nLodiX = 0, nLodiZY = 0;
+};
+
+size_t storageBytes(int storage) { return storage == ACP_STORE_F64 ? 8 : (storage == ACP_STORE_F32_DEV ? 4 : 2); }
+
+}  // namespace
+
+struct acp_handle {
+    acp_case_desc d;
+    int device = 0;
+    std::vector<LevelHost> host;
+    std::vector<LevelDev> dev;
+    int cur = 0;  // array holding the current state (0 or 1) of every level
+    bool inited = false;
+    long long steps = 0;
+    cudaStream_t stream = nullptr;
+    bool ownStream = false;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};  // one step starting from cur == 0 / cur == 1
+    int* dErr = nullptr;
+    // probes
+    long long* dProbeNodes = nullptr;
+    int nProbes = 0;
+    double* dSeries = nullptr;
+    int* dCounter = nullptr;
+    int probeCapacity = 0;
+    int probeLevel = 0;
+    size_t devBytes = 0;
+    std::string err;
+    double c = 0, kappa = 0, shift = 0;
+    float hscale[Q];
+};
+
+namespace {
+
+int fail(acp_handle* h, int code, const char* fmt, ...) {
+    if (h) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        std::vsnprintf(buf, sizeof buf, fmt, ap);
+        va_end(ap);
+        h->err = buf;
+    }
+    return code;
+}
+
+#define CU(h, call)                                                                                       \
+    do {                                                                                                  \
+        cudaError_t e_ = (call);                                                                          \
+        if (e_ != cudaSuccess) return fail((h), ACP_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+std::once_flag g_constOnce;
+int g_constStatus = 0;
+
+// MRT bases on the host: inverse of the Gram-Schmidt basis and the
+// raw-moment back transform, uploaded once per process.
+bool invert(const double* m, double* inv, int n) {
+    std::vector<double> a(n * 2 * n);
+    for (int r = 0; r < n; ++r)
+        for (int c = 0; c < n; ++c) {
+            a[r * 2 * n + c] = m[r * n + c];
+            a[r * 2 * n + n + c] = r == c;
+        }
+    for (int c = 0; c < n; ++c) {
+        int p = c;
+        for (int r = c + 1; r < n; ++r)
+            if (std::fabs(a[r * 2 * n + c]) > std::fabs(a[p * 2 * n + c])) p = r;
+        if (std::fabs(a[p * 2 * n + c]) < 1e-12) return false;
+        for (int k = 0; k < 2 * n; ++k) std::swap(a[p * 2 * n + k], a[c * 2 * n + k]);
+        double piv = a[c * 2 * n + c];
+        for (int k = 0; k < 2 * n; ++k) a[c * 2 * n + k] /= piv;
+        for (int r = 0; r < n; ++r) {
+            if (r == c) continue;
+            double f = a[r * 2 * n + c];
+            if (f == 0) continue;
+            for (int k = 0; k < 2 * n; ++k) a[r * 2 * n + k] -= f * a[c * 2 * n + k];
+        }
+    }
+    for (int r = 0; r < n; ++r)
+        for (int c = 0; c < n; ++c) inv[r * n + c] = a[r * 2 * n + n + c];
+    return true;
+}
+
+int rmRowFull(int m, int q) {
+    const int x = ex(q), y = ey(q), z = ez(q);
+    const int v[Q] = {1, x, y, z, x * x + y * y + z * z, x * x - z * z, y * y - z * z, x * y, x * z, y * z,
+                      x * x * z, x * z * z, y * y * z, y * z * z, x * x * y, x * y * y, x * x * z * z,
+                      x * x * y * y, y * y * z * z};
+    return v[m];
+}
+
+int uploadConstants() {
+    uint32_t masks[27];
+    for (int c = 0; c < 27; ++c) masks[c] = 0;
+    for (const BoundaryClass& b : kBoundaryClasses) {
+        uint32_t m = 0;
+        for (int k = 0; k < 5 && b.push[k] >= 0; ++k) m |= 1u << b.push[k];
+        masks[faceCode(b.fx, b.fy, b.fz)] = m;
+    }
+    masks[CODE_FLUID] = 0x3FFFFu;
+    double gs[Q * Q], gsi[Q * Q], rm[Q * Q], rmi[Q * Q], mw[Q], rm2[Q][5];
+    for (int m = 0; m < Q; ++m)
+        for (int q = 0; q < Q; ++q) {
+            gs[m * Q + q] = gsRow(m, q);
+            rm[m * Q + q] = rmRowFull(m, q);
+        }
+    if (!invert(gs, gsi, Q) || !invert(rm, rmi, Q)) return ACP_ERR_INVALID;
+    for (int m = 0; m < Q; ++m) {
+        mw[m] = 0;
+        for (int q = 0; q < Q; ++q) mw[m] += gs[m * Q + q] * wq(q);
+    }
+    for (int q = 0; q < Q; ++q)
+        for (int m = 0; m < 5; ++m) rm2[q][m] = rmi[q * Q + 5 + m];
+    if (cudaMemcpyToSymbol(c_pushMask, masks, sizeof masks) != cudaSuccess) return ACP_ERR_CUDA;
+    if (cudaMemcpyToSymbol(c_gsMinv, gsi, sizeof gsi) != cudaSuccess) return ACP_ERR_CUDA;
+    if (cudaMemcpyToSymbol(c_gsMw, mw, sizeof mw) != cudaSuccess) return ACP_ERR_CUDA;
+    if (cudaMemcpyToSymbol(c_rmTinv2, rm2, sizeof rm2) != cudaSuccess) return ACP_ERR_CUDA;
+    return ACP_OK;
+}
+
+int validate(const acp_case_desc* d, std::string& why) {
+    if (!d) { why = "null case"; return ACP_ERR_INVALID; }
+    if (d->nx < 1 || d->ny < 1 || d->nz < 1) { why = "node counts must be positive"; return ACP_ERR_INVALID; }
+    if ((long long)d->nx * d->ny * d->nz > (1LL << 34)) { why = "lattice too large"; return ACP_ERR_INVALID; }
+    if (d->op < 0 || d->op > 4) { why = "unknown collision model"; return ACP_ERR_INVALID; }
+    if (d->eq_order < 2 || d->eq_order > 4) { why = "Wrong order of equilibrium! (2, 3 or 4)"; return ACP_ERR_INVALID; }
+    if (!(d->spacing > 0) || !(d->speed_of_sound > 0) || !(d->density > 0) || !(d->kinematic_viscosity > 0)) {
+        why = "spacing, speed of sound, density and viscosity must be positive";
+        return ACP_ERR_INVALID;
+    }
+    if (d->storage < 0 || d->storage > 2) { why = "unknown storage form"; return ACP_ERR_INVALID; }
+    const int dims[3] = {d->nx, d->ny, d->nz};
+    for (int a = 0; a < 3; ++a) {
+        if (d->bc[a] != ACP_BC_LODI && d->bc[a] != ACP_BC_PERIODIC) { why = "unknown boundary type"; return ACP_ERR_INVALID; }
+        if (d->bc[a] == ACP_BC_LODI && dims[a] < 4) {
+            // the second normal neighbour would be a boundary node of the
+            // opposite face, whose new array the reference reads half-updated
+            why = "a LODI axis needs at least 4 nodes";
+            return ACP_ERR_UNSUPPORTED;
+        }
+    }
+    if (d->max_level != 0 && d->max_level != 1) { why = "MaxLevel must be 0 or 1"; return ACP_ERR_INVALID; }
+    if (d->max_level == 1) { why = "two-level cases are not enabled in this build"; return ACP_ERR_UNSUPPORTED; }
+    return ACP_OK;
+}
+
+// node classes and LODI wiring of a single level
+int buildSingleLevel(acp_handle* h) {
+    const acp_case_desc& d = h->d;
+    LevelHost L;
+    L.nx = d.nx; L.ny = d.ny; L.nz = d.nz;
+    L.N = (long long)L.nx * L.ny * L.nz;
+    L.code.assign(L.N, CODE_FLUID);
+    const int dims[3] = {L.nx, L.ny, L.nz};
+    auto idx = [&](int i, int j, int k) { return ((long long)k * L.ny + j) * L.nx + i; };
+    auto wrapped = [&](int i, int j, int k, long long& out) {
+        int c[3] = {i, j, k};
+        for (int a = 0; a < 3; ++a)
+            if (c[a] < 0 || c[a] >= dims[a]) {
+                if (d.bc[a] != ACP_BC_PERIODIC) return false;
+                c[a] = (c[a] % dims[a] + dims[a]) % dims[a];
+            }
+        out = idx(c[0], c[1], c[2]);
+        return true;
+    };
+    for (int k = 0; k < L.nz; ++k)
+        for (int j = 0; j < L.ny; ++j)
+            for (int i = 0; i < L.nx; ++i) {
+                const int c[3] = {i, j, k};
+                int fc[3];
+                for (int a = 0; a < 3; ++a)
+                    fc[a] = d.bc[a] == ACP_BC_LODI ? (c[a] == 0 ? -1 : (c[a] == dims[a] - 1 ? 1 : 0)) : 0;
+                if (!fc[0] && !fc[1] && !fc[2]) continue;
+                const long long n = idx(i, j, k);
+                L.code[n] = (uint8_t)faceCode(fc[0], fc[1], fc[2]);
+                const BoundaryClass* bc = boundaryClass(fc[0], fc[1], fc[2]);
+                BNodeDev b;
+                b.n = n;
+                b.normalDir = bc->normalDir;
+                if (!wrapped(i + bc->n1[0], j + bc->n1[1], k + bc->n1[2], b.n1) ||
+                    !wrapped(i + bc->n2[0], j + bc->n2[1], k + bc->n2[2], b.n2))
+                    return fail(h, ACP_ERR_INVALID, "normal neighbour outside the lattice");
+                for (int m = 0; m < 4; ++m) b.t[m] = -1;
+                const int nface = (fc[0] != 0) + (fc[1] != 0) + (fc[2] != 0);
+                b.transverse = 0;
+                if (nface == 1) {
+                    int t[4][3];
+                    faceTangents(fc[0], fc[1], fc[2], t);
+                    for (int m = 0; m < 4; ++m)
+                        if (!wrapped(i + t[m][0], j + t[m][1], k + t[m][2], b.t[m]))
+                            return fail(h, ACP_ERR_INVALID, "tangent neighbour outside the lattice");
+                    b.transverse = d.transverse ? 1 : 0;
+                }
+                (fc[0] != 0 ? L.lodiX : L.lodiZY).push_back(b);
+            }
+    L.active = L.N;
+    L.spacing = d.spacing;
+    L.dt = d.spacing / (d.speed_of_sound * std::sqrt(3.0));
+    const double cs2 = d.speed_of_sound * d.speed_of_sound;
+    L.omega = (cs2 * L.dt) / (d.kinematic_viscosity + 0.5 * cs2 * L.dt);
+    h->host.push_back(std::move(L));
+    return ACP_OK;
+}
+
+template <typename S>
+LevelArgs<S> levelArgs(acp_handle* h, int l, int src) {
+    const LevelHost& L = h->host[l];
+    const LevelDev& D = h->dev[l];
+    LevelArgs<S> a;
+    a.nx = L.nx; a.ny = L.ny; a.nz = L.nz;
+    a.N = L.N;
+    for (int ax = 0; ax < 3; ++ax) a.per[ax] = h->d.bc[ax] == ACP_BC_PERIODIC;
+    a.A = (const S*)D.f[src];
+    a.B = (S*)D.f[1 - src];
+    a.code = D.code;
+    a.mom = D.mom;
+    a.shift = h->shift;
+    a.omega = L.omega;
+    a.kappa = h->kappa;
+    a.sigma = h->d.hybrid_sigma;
+    for (int q = 0; q < Q; ++q) a.hscale[q] = h->hscale[q];
+    return a;
+}
+
+template <typename S>
+using CollideFn = void (*)(LevelArgs<S>);
+
+template <typename S, typename R, int OP>
+CollideFn<S> pickOrder(int order, bool cubic) {
+    switch (order) {
+        case 2: return cubic ? k_collide_push<S, R, OP, 2, true, false> : k_collide_push<S, R, OP, 2, false, false>;
+        case 3: return cubic ? k_collide_push<S, R, OP, 3, true, false> : k_collide_push<S, R, OP, 3, false, false>;
+        default: return cubic ? k_collide_push<S, R, OP, 4, true, false> : k_collide_push<S, R, OP, 4, false, false>;
+    }
+}
+
+template <typename S, typename R>
+CollideFn<S> pickCollide(const acp_case_desc& d) {
+    const bool cubic = d.cubic_mach != 0;
+    switch (d.op) {
+        case OP_SRT:
+            switch (d.eq_order) {
+                case 2: return k_collide_push<S, R, OP_SRT, 2, false, false>;
+                case 3: return k_collide_push<S, R, OP_SRT, 3, false, false>;
+                default: return k_collide_push<S, R, OP_SRT, 4, false, false>;
+            }
+        case OP_MRT_GS:
+            return d.mrt_writeback ? k_collide_push<S, R, OP_MRT_GS, 2, false, true>
+                                   : k_collide_push<S, R, OP_MRT_GS, 2, false, false>;
+        case OP_MRT_RM:
+            return d.mrt_writeback ? k_collide_push<S, R, OP_MRT_RM, 2, false, true>
+                                   : k_collide_push<S, R, OP_MRT_GS, 2, false, false>;
+        case OP_RR: return pickOrder<S, R, OP_RR>(d.eq_order, cubic);
+        default: return pickOrder<S, R, OP_HRR>(d.eq_order, cubic);
+    }
+}
+
+template <typename S>
+using LodiFn = void (*)(const S*, S*, const BNodeDev*, int, LodiArgs, LevelArgs<S>);
+
+template <typename S>
+LodiFn<S> pickLodi(int order) {
+    return order == 2 ? k_lodi<S, 2> : (order == 3 ? k_lodi<S, 3> : k_lodi<S, 4>);
+}
+
+bool needsMoments(const acp_case_desc& d) { return d.op == OP_HRR || (d.op == OP_RR && d.cubic_mach); }
+
+// events recorded between the kernels of a step, for acp_step_timed
+struct PhaseTimer {
+    cudaEvent_t ev[32];
+    int kind[32];
+    int n = 0;
+    cudaStream_t stream;
+    void mark(int k) {
+        if (n < 32) {
+            kind[n] = k;
+            cudaEventRecord(ev[n], stream);
+            ++n;
+        }
+    }
+};
+
+dim3 gridOf(const LevelHost& L, int bx) { return dim3((L.nx + bx - 1) / bx, L.ny, L.nz); }
+
+// enqueue one step of a single level, reading array src
+template <typename S, typename R>
+int enqueueLevelStep(acp_handle* h, int l, int src, PhaseTimer* tm = nullptr) {
+    const LevelHost& L = h->host[l];
+    const LevelDev& D = h->dev[l];
+    LevelArgs<S> a = levelArgs<S>(h, l, src);
+    const int bx = 128;
+    if (tm) tm->mark(-1);
+    if (needsMoments(h->d)) {
+        k_moments<S><<<gridOf(L, bx), bx, 0, h->stream>>>(a);
+        if (tm) tm->mark(ACP_K_MOMENTS);
+    }
+    pickCollide<S, R>(h->d)<<<gridOf(L, bx), bx, 0, h->stream>>>(a);
+    if (tm) tm->mark(ACP_K_COLLIDE);
+    LodiArgs p;
+    p.N = L.N;
+    p.shift = h->shift;
+    p.cs = h->d.speed_of_sound;
+    p.c = h->c;
+    p.mach = h->d.mach;
+    p.k1 = h->d.k1;
+    p.rho0 = h->d.density;
+    p.dt = L.dt;
+    p.localSpacing = h->d.spacing * std::pow(2.0, -(double)l);
+    p.kappa = h->kappa;
+    p.domainLength[0] = h->d.nx * h->d.spacing;
+    p.domainLength[1] = h->d.ny * h->d.spacing;
+    p.domainLength[2] = h->d.nz * h->d.spacing;
+    p.order = h->d.eq_order;
+    p.errorFlag = h->dErr;
+    LodiFn<S> lf = pickLodi<S>(h->d.eq_order);
+    if (D.nLodiX) lf<<<(D.nLodiX + 127) / 128, 128, 0, h->stream>>>(a.A, a.B, D.lodiX, D.nLodiX, p, a);
+    if (D.nLodiZY) lf<<<(D.nLodiZY + 127) / 128, 128, 0, h->stream>>>(a.A, a.B, D.lodiZY, D.nLodiZY, p, a);
+    if (tm && (D.nLodiX || D.nLodiZY)) tm->mark(ACP_K_LODI);
+    if (h->nProbes && h->probeLevel == l) {
+        k_probes<S><<<1, 128, 0, h->stream>>>(a.B, a, h->dProbeNodes, h->nProbes, h->shift,
+                                             h->d.speed_of_sound * h->d.speed_of_sound, h->dSeries, h->dCounter,
+                                             h->probeCapacity);
+        if (tm) tm->mark(ACP_K_PROBES);
+    }
+    return ACP_OK;
+}
+
+int enqueueStep(acp_handle* h, int src, PhaseTimer* tm = nullptr) {
+    switch (h->d.storage) {
+        case ACP_STORE_F64: return enqueueLevelStep<double, double>(h, 0, src, tm);
+        case ACP_STORE_F32_DEV: return enqueueLevelStep<float, float>(h, 0, src, tm);
+        default: return enqueueLevelStep<__half, float>(h, 0, src, tm);
+    }
+}
+
+int launchesPerStep(const acp_handle* h) {
+    int n = 0;
+    for (size_t l = 0; l < h->host.size(); ++l) {
+        n += 1 + (needsMoments(h->d) ? 1 : 0);
+        n += (h->dev[l].nLodiX ? 1 : 0) + (h->dev[l].nLodiZY ? 1 : 0);
+        if (h->nProbes && h->probeLevel == (int)l) ++n;
+    }
+    return n;
+}
+
+void destroyGraphs(acp_handle* h) {
+    for (int p = 0; p < 2; ++p)
+        if (h->graph[p]) {
+            cudaGraphExecDestroy(h->graph[p]);
+            h->graph[p] = nullptr;
+        }
+}
+
+int captureGraphs(acp_handle* h) {
+    destroyGraphs(h);
+    for (int p = 0; p < 2; ++p) {
+        cudaGraph_t g;
+        CU(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+        enqueueStep(h, p);
+        cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+        if (e != cudaSuccess) return fail(h, ACP_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&h->graph[p], g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return fail(h, ACP_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+    }
+    return ACP_OK;
+}
+
+template <typename S>
+void launchToF64(acp_handle* h, int l, int arr, double* dst) {
+    LevelArgs<S> a = levelArgs<S>(h, l, 0);
+    long long total = h->host[l].N * Q;
+    k_to_f64<S><<<(unsigned)((total + 255) / 256), 256, 0, h->stream>>>((const S*)h->dev[l].f[arr], dst, h->host[l].N,
+                                                                         h->shift, a);
+}
+template <typename S>
+void launchFromF64(acp_handle* h, int l, const double* src) {
+    LevelArgs<S> a = levelArgs<S>(h, l, 0);
+    long long total = h->host[l].N * Q;
+    k_from_f64<S><<<(unsigned)((total + 255) / 256), 256, 0, h->stream>>>(src, (S*)h->dev[l].f[0], (S*)h->dev[l].f[1],
+                                                                           h->host[l].N, h->shift, a);
+}
+template <typename S>
+void launchInit(acp_handle* h, int l) {
+    LevelArgs<S> a = levelArgs<S>(h, l, 0);
+    const LevelHost& L = h->host[l];
+    InitArgs ia;
+    ia.ic = h->d.ic;
+    ia.spacingLevel = h->d.spacing / std::pow(2.0, (double)l);
+    ia.halfDomain[0] = h->d.domain_size[0] / 2.;
+    ia.halfDomain[1] = h->d.domain_size[1] / 2.;
+    ia.rho0 = h->d.density;
+    ia.eps = h->d.ic_eps;
+    ia.b = h->d.ic_b;
+    ia.cell = 1.0 / std::pow(2.0, (double)l);
+    for (int c = 0; c < 3; ++c) {
+        ia.center[c] = h->d.ic_center[c];
+        ia.off[c] = L.off[c];
+    }
+    ia.dims3 = h->d.ic_dims == 3;
+    k_init<S><<<gridOf(L, 128), 128, 0, h->stream>>>(a, ia);
+}
+
+int devAlloc(acp_handle* h, void** p, size_t bytes) {
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) return fail(h, ACP_ERR_NOMEM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+    h->devBytes += bytes;
+    return ACP_OK;
+}
+
+size_t estimateBytes(const acp_case_desc& d) {
+    const long long N = (long long)d.nx * d.ny * d.nz;
+    size_t b = (size_t)N * (2 * Q * storageBytes(d.storage) + 1);
+    if (needsMoments(d)) b += (size_t)N * sizeof(Moments);
+    long long surf = 2LL * ((long long)d.nx * d.ny + (long long)d.ny * d.nz + (long long)d.nx * d.nz);
+    b += (size_t)surf * sizeof(BNodeDev);
+    return b;
+}
+
+}  // namespace
+
+extern "C" {
+
+void acp_default_case(acp_case_desc* d) {
+    std::memset(d, 0, sizeof *d);
+    d->spacing = 2.0e-2;
+    d->domain_size[0] = 3.0; d->domain_size[1] = 3.0; d->domain_size[2] = 0.4;
+    d->nx = 151; d->ny = 151; d->nz = 21;
+    d->density = 1.17621;
+    d->kinematic_viscosity = 1.49e-5;
+    d->speed_of_sound = 347.3;
+    d->mach = 0.0;
+    d->op = ACP_OP_HRR;
+    d->eq_order = 3;
+    d->hybrid_sigma = 0.98;
+    d->bc[0] = d->bc[1] = d->bc[2] = ACP_BC_LODI;
+    d->k1 = 1.0;
+    d->ref_layer_yz = 4; d->ref_layer_x = 75; d->overlap = 1;
+    d->c2f_replace = ACP_C2F_FALL;
+    d->f2c_replace = ACP_F2C_CALL;
+    d->ic = ACP_IC_REFERENCE;
+    d->ic_eps = 1e-3; d->ic_b = 6.0; d->ic_dims = 2;
+    d->storage = ACP_STORE_F64;
+}
+
+int acp_estimate_bytes(const acp_case_desc* d, size_t* bytes) {
+    std::string why;
+    int s = validate(d, why);
+    if (s) return s;
+    *bytes = estimateBytes(*d);
+    return ACP_OK;
+}
+
+int acp_create(const acp_case_desc* d, int device, acp_handle** out) {
+    if (!out) return ACP_ERR_INVALID;
+    *out = nullptr;
+    std::string why;
+    int s = validate(d, why);
+    acp_handle* h = new acp_handle();
+    if (s) {
+        h->err = why;
+        *out = h;  // handle carries the error text; caller destroys it
+        return s;
+    }
+    h->d = *d;
+    if (device < 0) {
+        if (cudaGetDevice(&h->device) != cudaSuccess) h->device = 0;
+    } else {
+        h->device = device;
+    }
+    *out = h;
+    CU(h, cudaSetDevice(h->device));
+    std::call_once(g_constOnce, [] { g_constStatus = uploadConstants(); });
+    if (g_constStatus) return fail(h, g_constStatus, "uploading lattice constants failed");
+    h->c = d->speed_of_sound * std::sqrt(3.0);
+    h->kappa = 1.0 / (6.0 * h->c * h->c);
+    h->shift = d->storage == ACP_STORE_F64 ? 0.0 : d->density;
+    for (int q = 0; q < Q; ++q) h->hscale[q] = 1.0f;
+    if (d->storage == ACP_STORE_F16_DEV) {
+        // power-of-two scale per population: the deviation w_q * drho of a
+        // pulse of relative amplitude eps stays inside the FP16 normal range
+        const double amp = std::max(d->ic == ACP_IC_GAUSSIAN ? d->ic_eps : 0.01, 1e-6) * d->density;
+        for (int q = 0; q < Q; ++q) {
+            const double mag = 4.0 * amp * wq(q);
+            h->hscale[q] = (float)std::ldexp(1.0, (int)std::ceil(std::log2(mag)) - 14);
+        }
+    }
+    s = buildSingleLevel(h);
+    if (s) return s;
+    CU(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    h->ownStream = true;
+    if ((s = devAlloc(h, (void**)&h->dErr, sizeof(int)))) return s;
+    CU(h, cudaMemsetAsync(h->dErr, 0, sizeof(int), h->stream));
+    h->dev.resize(h->host.size());
+    const size_t sb = storageBytes(d->storage);
+    for (size_t l = 0; l < h->host.size(); ++l) {
+        LevelHost& L = h->host[l];
+        LevelDev& D = h->dev[l];
+        for (int a = 0; a < 2; ++a)
+            if ((s = devAlloc(h, &D.f[a], (size_t)L.N * Q * sb))) return s;
+        if ((s = devAlloc(h, (void**)&D.code, (size_t)L.N))) return s;
+        CU(h, cudaMemcpyAsync(D.code, L.code.data(), (size_t)L.N, cudaMemcpyHostToDevice, h->stream));
+        if (needsMoments(*d) && (s = devAlloc(h, (void**)&D.mom, (size_t)L.N * sizeof(Moments)))) return s;
+        D.nLodiX = (int)L.lodiX.size();
+        D.nLodiZY = (int)L.lodiZY.size();
+        if (D.nLodiX) {
+            if ((s = devAlloc(h, (void**)&D.lodiX, L.lodiX.size() * sizeof(BNodeDev)))) return s;
+            CU(h, cudaMemcpyAsync(D.lodiX, L.lodiX.data(), L.lodiX.size() * sizeof(BNodeDev), cudaMemcpyHostToDevice,
+                                  h->stream));
+        }
+        if (D.nLodiZY) {
+            if ((s = devAlloc(h, (void**)&D.lodiZY, L.lodiZY.size() * sizeof(BNodeDev)))) return s;
+            CU(h, cudaMemcpyAsync(D.lodiZY, L.lodiZY.data(), L.lodiZY.size() * sizeof(BNodeDev),
+                                  cudaMemcpyHostToDevice, h->stream));
+        }
+    }
+    CU(h, cudaStreamSynchronize(h->stream));
+    return ACP_OK;
+}
+
+int acp_init(acp_handle* h) {
+    if (!h || h->dev.empty()) return ACP_ERR_STATE;
+    CU(h, cudaSetDevice(h->device));
+    for (size_t l = 0; l < h->host.size(); ++l) {
+        switch (h->d.storage) {
+            case ACP_STORE_F64: launchInit<double>(h, (int)l); break;
+            case ACP_STORE_F32_DEV: launchInit<float>(h, (int)l); break;
+            default: launchInit<__half>(h, (int)l); break;
+        }
+    }
+    CU(h, cudaGetLastError());
+    h->cur = 0;
+    h->steps = 0;
+    if (h->dCounter) CU(h, cudaMemsetAsync(h->dCounter, 0, sizeof(int), h->stream));
+    CU(h, cudaMemsetAsync(h->dErr, 0, sizeof(int), h->stream));
+    int s = captureGraphs(h);
+    if (s) return s;
+    h->inited = true;
+    return ACP_OK;
+}
+
+int acp_step(acp_handle* h, int n) {
+    if (!h || !h->inited) return ACP_ERR_STATE;
+    if (n < 0) return fail(h, ACP_ERR_INVALID, "negative step count");
+    CU(h, cudaSetDevice(h->device));
+    for (int s = 0; s < n; ++s) {
+        CU(h, cudaGraphLaunch(h->graph[h->cur], h->stream));
+        h->cur ^= 1;
+        ++h->steps;
+    }
+    return ACP_OK;
+}
+
+int acp_sync(acp_handle* h) {
+    if (!h) return ACP_ERR_INVALID;
+    if (h->dev.empty()) return ACP_ERR_STATE;
+    CU(h, cudaSetDevice(h->device));
+    int flag = 0;
+    CU(h, cudaMemcpyAsync(&flag, h->dErr, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CU(h, cudaStreamSynchronize(h->stream));
+    if (flag) return fail(h, ACP_ERR_NUMERIC, "boundary density left [0.5, 1.5] x rho0 or became NaN");
+    return ACP_OK;
+}
+
+int acp_level_dims(acp_handle* h, int level, int dims[3]) {
+    if (!h || level < 0 || level >= (int)h->host.size()) return ACP_ERR_INVALID;
+    dims[0] = h->host[level].nx; dims[1] = h->host[level].ny; dims[2] = h->host[level].nz;
+    return ACP_OK;
+}
+
+int acp_active_updates(acp_handle* h, long long* coarse, long long* fine) {
+    if (!h || h->host.empty()) return ACP_ERR_STATE;
+    *coarse = h->host[0].active;
+    *fine = h->host.size() > 1 ? h->host[1].active : 0;
+    return ACP_OK;
+}
+
+int acp_read_populations(acp_handle* h, int level, double* out) {
+    if (!h || !out || level < 0 || level >= (int)h->host.size()) return ACP_ERR_INVALID;
+    CU(h, cudaSetDevice(h->device));
+    const LevelHost& L = h->host[level];
+    double* tmp = nullptr;
+    CU(h, cudaMallocAsync((void**)&tmp, (size_t)L.N * Q * sizeof(double), h->stream));
+    switch (h->d.storage) {
+        case ACP_STORE_F64: launchToF64<double>(h, level, h->cur, tmp); break;
+        case ACP_STORE_F32_DEV: launchToF64<float>(h, level, h->cur, tmp); break;
+        default: launchToF64<__half>(h, level, h->cur, tmp); break;
+    }
+    cudaError_t e = cudaMemcpyAsync(out, tmp, (size_t)L.N * Q * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+    cudaFreeAsync(tmp, h->stream);
+    if (e != cudaSuccess) return fail(h, ACP_ERR_CUDA, "copy: %s", cudaGetErrorString(e));
+    CU(h, cudaStreamSynchronize(h->stream));
+    return ACP_OK;
+}
+
+int acp_write_populations(acp_handle* h, int level, const double* in) {
+    if (!h || !in || level < 0 || level >= (int)h->host.size()) return ACP_ERR_INVALID;
+    CU(h, cudaSetDevice(h->device));
+    const LevelHost& L = h->host[level];
+    double* tmp = nullptr;
+    CU(h, cudaMallocAsync((void**)&tmp, (size_t)L.N * Q * sizeof(double), h->stream));
+    cudaError_t e = cudaMemcpyAsync(tmp, in, (size_t)L.N * Q * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) {
+        switch (h->d.storage) {
+            case ACP_STORE_F64: launchFromF64<double>(h, level, tmp); break;
+            case ACP_STORE_F32_DEV: launchFromF64<float>(h, level, tmp); break;
+            default: launchFromF64<__half>(h, level, tmp); break;
+        }
+    }
+    cudaFreeAsync(tmp, h->stream);
+    if (e != cudaSuccess) return fail(h, ACP_ERR_CUDA, "copy: %s", cudaGetErrorString(e));
+    CU(h, cudaStreamSynchronize(h->stream));
+    return ACP_OK;
+}
+
+int acp_read_field(acp_handle* h, int level, int field, double* out) {
+    if (!h || !out || level < 0 || level >= (int)h->host.size() || field < 0 || field > 4) return ACP_ERR_INVALID;
+    const LevelHost& L = h->host[level];
+    std::vector<double> f((size_t)L.N * Q);
+    int s = acp_read_populations(h, level, f.data());
+    if (s) return s;
+    for (long long n = 0; n < L.N; ++n) {
+        double rho = 0, jx = 0, jy = 0, jz = 0;
+        for (int q = 0; q < Q; ++q) {
+            const double v = f[(size_t)q * L.N + n];
+            rho += v;
+            jx += ex(q) * v;
+            jy += ey(q) * v;
+            jz += ez(q) * v;
+        }
+        double r;
+        switch (field) {
+            case ACP_FIELD_RHO: r = rho; break;
+            case ACP_FIELD_UX: r = h->c * jx / rho; break;
+            case ACP_FIELD_UY: r = h->c * jy / rho; break;
+            case ACP_FIELD_UZ: r = h->c * jz / rho; break;
+            default: r = rho * h->d.speed_of_sound * h->d.speed_of_sound; break;
+        }
+        out[n] = r;
+    }
+    return ACP_OK;
+}
+
+int acp_set_probes(acp_handle* h, int n, const int* lijk) {
+    if (!h || n < 0 || (n > 0 && !lijk)) return ACP_ERR_INVALID;
+    CU(h, cudaSetDevice(h->device));
+    std::vector<long long> nodes(n);
+    int level = n ? lijk[0] : 0;
+    for (int m = 0; m < n; ++m) {
+        const int l = lijk[4 * m];
+        if (l != level || l < 0 || l >= (int)h->host.size())
+            return fail(h, ACP_ERR_INVALID, "probes must all lie on one existing level");
+        const LevelHost& L = h->host[l];
+        const int i = lijk[4 * m + 1] - L.off[0], j = lijk[4 * m + 2] - L.off[1], k = lijk[4 * m + 3] - L.off[2];
+        if (i < 0 || i >= L.nx || j < 0 || j >= L.ny || k < 0 || k >= L.nz)
+            return fail(h, ACP_ERR_INVALID, "probe %d outside its level", m);
+        nodes[m] = ((long long)k * L.ny + j) * L.nx + i;
+    }
+    if (h->dProbeNodes) { cudaFree(h->dProbeNodes); h->dProbeNodes = nullptr; }
+    if (h->dSeries) { cudaFree(h->dSeries); h->dSeries = nullptr; }
+    if (!h->dCounter) {
+        int s = devAlloc(h, (void**)&h->dCounter, sizeof(int));
+        if (s) return s;
+    }
+    h->nProbes = n;
+    h->probeLevel = level;
+    h->probeCapacity = 1 << 16;
+    if (n) {
+        int s = devAlloc(h, (void**)&h->dProbeNodes, n * sizeof(long long));
+        if (s) return s;
+        if ((s = devAlloc(h, (void**)&h->dSeries, (size_t)n * h->probeCapacity * sizeof(double)))) return s;
+        CU(h, cudaMemcpyAsync(h->dProbeNodes, nodes.data(), n * sizeof(long long), cudaMemcpyHostToDevice, h->stream));
+    }
+    CU(h, cudaMemsetAsync(h->dCounter, 0, sizeof(int), h->stream));
+    CU(h, cudaStreamSynchronize(h->stream));
+    if (h->inited) return captureGraphs(h);
+    return ACP_OK;
+}
+
+int acp_read_probes(acp_handle* h, double* out, int max_samples, int* n_samples) {
+    if (!h || !n_samples) return ACP_ERR_INVALID;
+    CU(h, cudaSetDevice(h->device));
+    int cnt = 0;
+    if (h->dCounter) CU(h, cudaMemcpyAsync(&cnt, h->dCounter, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CU(h, cudaStreamSynchronize(h->stream));
+    cnt = std::min(cnt, h->probeCapacity);
+    const int take = std::min(cnt, max_samples);
+    if (take > 0 && out && h->nProbes)
+        CU(h, cudaMemcpy(out, h->dSeries, (size_t)take * h->nProbes * sizeof(double), cudaMemcpyDeviceToHost));
+    *n_samples = take;
+    return ACP_OK;
+}
+
+int acp_steps_done(acp_handle* h, long long* steps) {
+    if (!h || !steps) return ACP_ERR_INVALID;
+    *steps = h->steps;
+    return ACP_OK;
+}
+
+int acp_set_stream(acp_handle* h, void* stream) {
+    if (!h) return ACP_ERR_INVALID;
+    CU(h, cudaSetDevice(h->device));
+    CU(h, cudaStreamSynchronize(h->stream));
+    if (h->ownStream && stream) {
+        cudaStreamDestroy(h->stream);
+        h->ownStream = false;
+    }
+    if (stream) {
+        h->stream = (cudaStream_t)stream;
+    } else if (!h->ownStream) {
+        CU(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+        h->ownStream = true;
+    }
+    if (h->inited) return captureGraphs(h);
+    return ACP_OK;
+}
+
+int acp_device_bytes(acp_handle* h, size_t* bytes) {
+    if (!h || !bytes) return ACP_ERR_INVALID;
+    *bytes = h->devBytes;
+    return ACP_OK;
+}
+
+int acp_step_timed(acp_handle* h, int n, double* kernel_ms) {
+    if (!h || !h->inited || !kernel_ms || n < 0) return ACP_ERR_INVALID;
+    CU(h, cudaSetDevice(h->device));
+    double acc[ACP_K_COUNT] = {0, 0, 0, 0, 0};
+    PhaseTimer tm;
+    tm.stream = h->stream;
+    for (int e = 0; e < 32; ++e) CU(h, cudaEventCreate(&tm.ev[e]));
+    int status = ACP_OK;
+    for (int s = 0; s < n && status == ACP_OK; ++s) {
+        tm.n = 0;
+        enqueueStep(h, h->cur, &tm);
+        h->cur ^= 1;
+        ++h->steps;
+        cudaError_t e = cudaStreamSynchronize(h->stream);
+        if (e != cudaSuccess) { status = fail(h, ACP_ERR_CUDA, "timed step: %s", cudaGetErrorString(e)); break; }
+        for (int m = 1; m < tm.n; ++m) {
+            float ms = 0;
+            cudaEventElapsedTime(&ms, tm.ev[m - 1], tm.ev[m]);
+            if (tm.kind[m] >= 0) acc[tm.kind[m]] += ms;
+        }
+    }
+    for (int e = 0; e < 32; ++e) cudaEventDestroy(tm.ev[e]);
+    for (int k = 0; k < ACP_K_COUNT; ++k) kernel_ms[k] = n ? acc[k] / n : 0.0;
+    return status;
+}
+
+int acp_launches_per_step(acp_handle* h, int* launches) {
+    if (!h || !launches || h->dev.empty()) return ACP_ERR_INVALID;
+    *launches = launchesPerStep(h);
+    return ACP_OK;
+}
+
+int acp_boundary_wiring(const acp_case_desc* d, long long* rows, long long max_rows, long long* count) {
+    if (!count) return ACP_ERR_INVALID;
+    std::string why;
+    int s = validate(d, why);
+    if (s) return s;
+    acp_handle tmp;
+    tmp.d = *d;
+    if ((s = buildSingleLevel(&tmp))) return s;
+    const LevelHost& L = tmp.host[0];
+    std::vector<const BNodeDev*> all;
+    for (const BNodeDev& b : L.lodiX) all.push_back(&b);
+    for (const BNodeDev& b : L.lodiZY) all.push_back(&b);
+    std::sort(all.begin(), all.end(), [](const BNodeDev* a, const BNodeDev* b) { return a->n < b->n; });
+    *count = (long long)all.size();
+    if (!rows) return ACP_OK;
+    for (long long r = 0; r < (long long)all.size() && r < max_rows; ++r) {
+        const BNodeDev& b = *all[r];
+        const long long i = b.n % L.nx, j = (b.n / L.nx) % L.ny, k = b.n / ((long long)L.nx * L.ny);
+        const int code = L.code[b.n];
+        const int fx = code / 9 - 1, fy = (code / 3) % 3 - 1, fz = code % 3 - 1;
+        const BoundaryClass* bc = boundaryClass(fx, fy, fz);
+        long long mask = 0;
+        for (int m = 0; m < 5 && bc->push[m] >= 0; ++m) mask |= 1LL << bc->push[m];
+        long long* o = rows + 12 * r;
+        o[0] = i; o[1] = j; o[2] = k; o[3] = b.normalDir; o[4] = b.n1; o[5] = b.n2;
+        for (int m = 0; m < 4; ++m) o[6 + m] = b.t[m];
+        o[10] = bc->corner;
+        o[11] = mask;
+    }
+    return ACP_OK;
+}
+
+int acp_destroy(acp_handle* h) {
+    if (!h) return ACP_OK;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    destroyGraphs(h);
+    for (LevelDev& D : h->dev) {
+        cudaFree(D.f[0]);
+        cudaFree(D.f[1]);
+        cudaFree(D.code);
+        cudaFree(D.mom);
+        cudaFree(D.lodiX);
+        cudaFree(D.lodiZY);
+    }
+    cudaFree(h->dErr);
+    cudaFree(h->dProbeNodes);
+    cudaFree(h->dSeries);
+    cudaFree(h->dCounter);
+    if (h->ownStream && h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return ACP_OK;
+}
+
+const char* acp_last_error(const acp_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+const char* acp_status_string(int s) {
+    switch (s) {
+        case ACP_OK: return "ok";
+        case ACP_ERR_INVALID: return "invalid argument";
+        case ACP_ERR_CUDA: return "CUDA error";
+        case ACP_ERR_NOMEM: return "out of memory";
+        case ACP_ERR_UNSUPPORTED: return "unsupported";
+        case ACP_ERR_NUMERIC: return "numerical blow-up";
+        case ACP_ERR_TIMEOUT: return "device wait timed out";
+        case ACP_ERR_BUDGET: return "HBM budget exhausted";
+        case ACP_ERR_STATE: return "call out of order";
+        default: return "unknown status";
+    }
+}
+
+int acp_abi_version(void) { return ACP_ABI_VERSION; }
+
+}  // extern "C"

@@ -1,0 +1,531 @@
+// Kernels of one level's step.  Data layout (HBM): populations in
+// structure-of-arrays form, g[q][k][j][i] with i fastest, two ping-pong
+// arrays per level (the reference's distr_[2][19], Node.h:190); one byte per
+// node for the node class; a 32-byte moment record per node only where the
+// operator needs the neighbours' pre-collision (rho, u).
+//
+// One coarse step of a single level (Lattice::timeSteppingX,
+// Lattice.cpp:1496-2156) is:
+//   k_moments        (HRR, and RR with cubic-Mach) neighbours' pre-collision rho,u
+//   k_collide_push   collide every fluid node and push to the 18 neighbours
+//                    (FluidNode::transport); boundary nodes push their
+//                    uncollided populations inward (BoundaryNode::transport)
+//   k_lodi (x faces) LODI on the x faces, which at the corners read edge nodes
+//                    of the z faces before those are updated (Lattice.cpp:1582-1596)
+//   k_lodi (z, y)    LODI on the remaining faces; no node of this pass reads
+//                    another node's new array within the pass
+#pragma once
+#include "d3q19.cuh"
+#include <stdint.h>
+
+namespace acp {
+
+constexpr uint8_t CODE_FLUID = 13;  // face class (0,0,0)
+constexpr uint8_t CODE_DEAD = 255;
+
+// pushed-direction mask of each boundary face class (fx+1)*9+(fy+1)*3+(fz+1)
+__constant__ uint32_t c_pushMask[27];
+// MRT bases: inverse of the Gram-Schmidt basis, the basis applied to w_q, and
+// the raw-moment back-transform columns of the five relaxed moments
+__constant__ double c_gsMinv[Q][Q];
+__constant__ double c_gsMw[Q];
+__constant__ double c_rmTinv2[Q][5];
+
+struct Moments {
+    double rho, ux, uy, uz;  // lattice units, absolute density
+};
+
+template <typename S>
+struct LevelArgs {
+    int nx, ny, nz;
+    long long N;
+    int per[3];  // periodic axes
+    const S* A;  // array read this step
+    S* B;        // array written this step
+    const uint8_t* code;
+    Moments* mom;
+    double shift;   // w_q * shift is subtracted in storage (0 for the FP64 form)
+    double omega;   // collision frequency of the level
+    double kappa;   // 1/(6 c^2): fourth-order orthogonalisation constant
+    double sigma;   // HRR hybrid parameter
+    float hscale[Q];  // FP16 per-population scales (1 otherwise)
+};
+
+__device__ __forceinline__ int wrapc(int c, int n, int per) {
+    if (c < 0) return per ? c + n : -1;
+    if (c >= n) return per ? c - n : -1;
+    return c;
+}
+
+template <typename S>
+__device__ __forceinline__ float scaleOf(const LevelArgs<S>& a, int q) {
+    return a.hscale[q];
+}
+
+// ---------------------------------------------------------------------------
+// pre-collision moments of every live node (calcDensityPreCol /
+// calcVelocityPreCol, Node.cpp:32-51,121-154)
+template <typename S>
+__global__ void k_moments(LevelArgs<S> a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y, k = blockIdx.z;
+    if (i >= a.nx) return;
+    const long long n = ((long long)k * a.ny + j) * a.nx + i;
+    if (a.code[n] == CODE_DEAD) return;
+    double d = 0, jx = 0, jy = 0, jz = 0;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const double g = (double)Store<S>::load(a.A + q * a.N + n, scaleOf(a, q));
+        d += g;
+        jx += ex(q) * g;
+        jy += ey(q) * g;
+        jz += ez(q) * g;
+    }
+    const double rho = a.shift + d;
+    Moments m;
+    m.rho = rho;
+    m.ux = jx / rho;
+    m.uy = jy / rho;
+    m.uz = jz / rho;
+    a.mom[n] = m;
+}
+
+// ---------------------------------------------------------------------------
+// collision of one fluid node in registers (deviation form)
+template <typename R, int OP, int ORDER, bool CUBIC, bool MRTWB>
+struct Collider {
+    template <typename ST>
+    __device__ __forceinline__ static void run(R* g, const LevelArgs<ST>& a, int i, int j, int k) {
+        if (OP == OP_MRT_GS || OP == OP_MRT_RM) {
+            if (!MRTWB) return;  // the reference discards the MRT back transform (Node.cpp:2603,2833)
+        }
+        R drho = 0, jx = 0, jy = 0, jz = 0;
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            drho += g[q];
+            jx += R(ex(q)) * g[q];
+            jy += R(ey(q)) * g[q];
+            jz += R(ez(q)) * g[q];
+        }
+        const R rho = R(a.shift) + drho;
+        const R inv = R(1) / rho;
+        R u[3] = {jx * inv, jy * inv, jz * inv};
+        const R omega = R(a.omega);
+        const R kappa = R(a.kappa);
+
+        if (OP == OP_MRT_GS) {
+            R m[Q];
+#pragma unroll
+            for (int mm = 0; mm < Q; ++mm) {
+                R s = R(a.shift) * R(c_gsMw[mm]);
+#pragma unroll
+                for (int q = 0; q < Q; ++q)
+                    if (gsRow(mm, q) != 0) s += R(gsRow(mm, q)) * g[q];
+                m[mm] = s;
+            }
+            R meq[Q];
+#pragma unroll
+            for (int mm = 0; mm < Q; ++mm) meq[mm] = 0;
+            meq[0] = rho; meq[3] = jx; meq[5] = jy; meq[7] = jz;
+            meq[1] = (jx * jx + jy * jy + jz * jz) * inv;
+            meq[9] = (R(2) * jx * jx - jy * jy - jz * jz) * inv;
+            meq[11] = (jy * jy - jz * jz) * inv;
+            meq[13] = jx * jy * inv;
+            meq[14] = jy * jz * inv;
+            meq[15] = jx * jz * inv;
+            R dm[Q];
+#pragma unroll
+            for (int mm = 0; mm < Q; ++mm) {
+                const bool conserved = mm == 0 || mm == 3 || mm == 5 || mm == 7;
+                const bool visc = mm == 1 || mm == 9 || mm == 11 || mm == 13 || mm == 14 || mm == 15;
+                dm[mm] = conserved ? R(0) : (visc ? omega : R(1)) * (meq[mm] - m[mm]);
+            }
+#pragma unroll
+            for (int q = 0; q < Q; ++q) {
+                R acc = 0;
+#pragma unroll
+                for (int mm = 0; mm < Q; ++mm) {
+                    const bool conserved = mm == 0 || mm == 3 || mm == 5 || mm == 7;
+                    if (!conserved) acc += R(c_gsMinv[q][mm]) * dm[mm];
+                }
+                g[q] += acc;
+            }
+            return;
+        }
+
+        if (OP == OP_MRT_RM) {
+            // extended raw-moment equilibrium (Node.cpp:2627-2645)
+            const R ux = u[0], uy = u[1], uz = u[2];
+            const R u2[3] = {ux * ux, uy * uy, uz * uz};
+            R geq[Q];
+#pragma unroll
+            for (int q = 0; q < Q; ++q) {
+                const int e[3] = {ex(q), ey(q), ez(q)};
+                const int nzc = (e[0] != 0) + (e[1] != 0) + (e[2] != 0);
+                R p;
+                if (nzc == 0) {
+                    p = -(u2[0] + u2[1] + u2[2]) + R(3) * (u2[0] * u2[1] + u2[0] * u2[2] + u2[1] * u2[2]);
+                } else if (nzc == 1) {
+                    const int aa = e[0] ? 0 : (e[1] ? 1 : 2);
+                    const int bb = (aa + 1) % 3, cc = (aa + 2) % 3;
+                    const R sg = R(e[aa]);
+                    p = R(3) * sg * u[aa] + R(3) * (u2[aa] - u2[bb] - u2[cc]) - R(9) * sg * u[aa] * (u2[bb] + u2[cc]) -
+                        R(9) * u2[aa] * (u2[bb] + u2[cc]);
+                } else {
+                    const int aa = e[0] ? 0 : 1;
+                    const int bb = e[2] ? 2 : 1;
+                    const R sa = R(e[aa]), sb = R(e[bb]);
+                    p = R(3) * (sa * u[aa] + sb * u[bb]) + R(3) * (u2[aa] + u2[bb]) + R(9) * sa * sb * u[aa] * u[bb] +
+                        R(9) * (sb * u2[aa] * u[bb] + sa * u[aa] * u2[bb]) + R(9) * u2[aa] * u2[bb];
+                }
+                geq[q] = R(wq(q)) * (drho + rho * p);
+            }
+            R d[5];
+#pragma unroll
+            for (int mm = 0; mm < 5; ++mm) {
+                R s = 0;
+#pragma unroll
+                for (int q = 0; q < Q; ++q)
+                    if (rmRow2(mm, q) != 0) s += R(rmRow2(mm, q)) * (g[q] - geq[q]);
+                d[mm] = s;
+            }
+            const R om1 = R(1) - omega;
+#pragma unroll
+            for (int q = 0; q < Q; ++q) {
+                R acc = 0;
+#pragma unroll
+                for (int mm = 0; mm < 5; ++mm) acc += R(c_rmTinv2[q][mm]) * d[mm];
+                g[q] = geq[q] + om1 * acc;
+            }
+            return;
+        }
+
+        EqCoef<R, ORDER> ec;
+        ec.set(u, kappa);
+        R geq[Q];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) geq[q] = R(wq(q)) * (drho + rho * ec.poly(q, kappa));
+
+        if (OP == OP_SRT) {
+#pragma unroll
+            for (int q = 0; q < Q; ++q) g[q] += omega * (geq[q] - g[q]);
+            return;
+        }
+
+        // RR / HRR: neighbours' pre-collision moments where needed
+        R S[6] = {0, 0, 0, 0, 0, 0};
+        R hpsi[Q];
+        if (OP == OP_HRR || CUBIC) {
+            const int ip = wrapc(i + 1, a.nx, a.per[0]), im = wrapc(i - 1, a.nx, a.per[0]);
+            const int jp = wrapc(j + 1, a.ny, a.per[1]), jm = wrapc(j - 1, a.ny, a.per[1]);
+            const int kp = wrapc(k + 1, a.nz, a.per[2]), km = wrapc(k - 1, a.nz, a.per[2]);
+            const long long row = (long long)a.nx, pl = (long long)a.nx * a.ny;
+            const long long base = (long long)k * pl + (long long)j * row;
+            const Moments mxp = a.mom[base + ip], mxm = a.mom[base + im];
+            const Moments myp = a.mom[(long long)k * pl + (long long)jp * row + i];
+            const Moments mym = a.mom[(long long)k * pl + (long long)jm * row + i];
+            const Moments mzp = a.mom[(long long)kp * pl + (long long)j * row + i];
+            const Moments mzm = a.mom[(long long)km * pl + (long long)j * row + i];
+            if (OP == OP_HRR) {
+                S[0] = R(0.5) * R(mxp.ux - mxm.ux);
+                S[1] = R(0.5) * R(myp.uy - mym.uy);
+                S[2] = R(0.5) * R(mzp.uz - mzm.uz);
+                S[3] = R(0.5) * (R(0.5) * R(mxp.uy - mxm.uy) + R(0.5) * R(myp.ux - mym.ux));
+                S[4] = R(0.5) * (R(0.5) * R(mxp.uz - mxm.uz) + R(0.5) * R(mzp.ux - mzm.ux));
+                S[5] = R(0.5) * (R(0.5) * R(myp.uz - mym.uz) + R(0.5) * R(mzp.uy - mzm.uy));
+            }
+            if (CUBIC) {
+                // Psi terms of the neighbours (Node.cpp:1832-1841) and their central differences
+                auto psiT = [](const Moments& m, R* P) {
+                    const R r = R(m.rho), x = R(m.ux), y = R(m.uy), z = R(m.uz);
+                    P[0] = r * x * x * x;               // XXX
+                    P[1] = R(0.5) * r * y * z * z;      // XXY
+                    P[2] = R(0.5) * r * z * y * y;      // XXZ
+                    P[3] = R(0.5) * r * x * z * z;      // XYY
+                    P[4] = r * y * y * y;               // YYY
+                    P[5] = R(0.5) * r * z * x * x;      // YYZ
+                    P[6] = R(0.5) * r * x * y * y;      // XZZ
+                    P[7] = R(0.5) * r * y * x * x;      // YZZ
+                    P[8] = r * z * z * z;               // ZZZ
+                    P[9] = r * x * y * z;               // XYZ
+                };
+                R Pxp[10], Pxm[10], Pyp[10], Pym[10], Pzp[10], Pzm[10];
+                psiT(mxp, Pxp); psiT(mxm, Pxm); psiT(myp, Pyp); psiT(mym, Pym); psiT(mzp, Pzp); psiT(mzm, Pzm);
+                auto dX = [&](int c) { return R(0.5) * (Pxp[c] - Pxm[c]); };
+                auto dY = [&](int c) { return R(0.5) * (Pyp[c] - Pym[c]); };
+                auto dZ = [&](int c) { return R(0.5) * (Pzp[c] - Pzm[c]); };
+                R G[6];
+                G[0] = dX(0) + dY(1) + dZ(2);  // xx
+                G[1] = dX(3) + dY(4) + dZ(5);  // yy
+                G[2] = dX(6) + dY(7) + dZ(8);  // zz
+                G[3] = dX(1) + dY(3) + dZ(9);  // xy
+                G[4] = dX(2) + dY(9) + dZ(6);  // xz
+                G[5] = dX(9) + dY(5) + dZ(7);  // yz
+#pragma unroll
+                for (int q = 0; q < Q; ++q) hpsi[q] = R(2.25) * R(wq(q)) * h2dot<R>(q, G);
+            }
+        }
+        R P[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            R gn = g[q] - geq[q];
+            if (CUBIC) gn += hpsi[q];
+            P[0] += h2xx<R>(q) * gn;
+            P[1] += h2yy<R>(q) * gn;
+            P[2] += h2zz<R>(q) * gn;
+            P[3] += R(ex(q) * ey(q)) * gn;
+            P[4] += R(ex(q) * ez(q)) * gn;
+            P[5] += R(ey(q) * ez(q)) * gn;
+        }
+        R A2[6];
+        if (OP == OP_HRR) {
+            const R sg = R(a.sigma);
+            const R fd = (R(1) - sg) * (R(-2) * rho / (R(3) * omega));
+#pragma unroll
+            for (int c = 0; c < 6; ++c) A2[c] = sg * P[c] + fd * S[c];
+        } else {
+#pragma unroll
+            for (int c = 0; c < 6; ++c) A2[c] = P[c];
+        }
+        NeqCoef<R, ORDER> nc;
+        nc.set(A2, u, kappa);
+        const R om1 = R(1) - omega;
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            R v = geq[q] + om1 * R(wq(q)) * nc.poly(q, kappa);
+            if (CUBIC) v += hpsi[q];
+            g[q] = v;
+        }
+    }
+};
+
+// ---------------------------------------------------------------------------
+// collide + push (one thread per node; x fastest so that each direction's
+// loads and stores are coalesced)
+template <typename S, typename R, int OP, int ORDER, bool CUBIC, bool MRTWB>
+__global__ void __launch_bounds__(128) k_collide_push(LevelArgs<S> a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y, k = blockIdx.z;
+    if (i >= a.nx) return;
+    const long long n = ((long long)k * a.ny + j) * a.nx + i;
+    const uint8_t code = a.code[n];
+    if (code == CODE_DEAD) return;
+    R g[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) g[q] = R(Store<S>::load(a.A + q * a.N + n, scaleOf(a, q)));
+    uint32_t mask;
+    if (code == CODE_FLUID) {
+        Collider<R, OP, ORDER, CUBIC, MRTWB>::run(g, a, i, j, k);
+        mask = 0x3FFFFu;
+    } else {
+        mask = c_pushMask[code];
+    }
+    const int xs[3] = {wrapc(i - 1, a.nx, a.per[0]), i, wrapc(i + 1, a.nx, a.per[0])};
+    const int ys[3] = {wrapc(j - 1, a.ny, a.per[1]), j, wrapc(j + 1, a.ny, a.per[1])};
+    const int zs[3] = {wrapc(k - 1, a.nz, a.per[2]), k, wrapc(k + 1, a.nz, a.per[2])};
+#pragma unroll
+    for (int q = 0; q < 18; ++q) {
+        if (!(mask >> q & 1u)) continue;
+        const int ti = xs[ex(q) + 1], tj = ys[ey(q) + 1], tk = zs[ez(q) + 1];
+        if ((ti | tj | tk) < 0) continue;
+        const long long t = ((long long)tk * a.ny + tj) * a.nx + ti;
+        Store<S>::store(a.B + q * a.N + t, g[q], scaleOf(a, q));
+    }
+    Store<S>::store(a.B + 18 * a.N + n, g[18], scaleOf(a, 18));
+}
+
+// ---------------------------------------------------------------------------
+// LODI characteristic pressure boundary (Node::LODIpressureOutlet and
+// LODIpressureCalcVelocity, Node.cpp:229-504), FP64 in the reference's SI
+// units.  One thread per boundary node.
+struct BNodeDev {
+    long long n, n1, n2, t[4];  // node, normal neighbours, tangent neighbours (-1: none)
+    int normalDir;              // 0:-x 1:-y 2:+x 3:+y 4:-z 5:+z
+    int transverse;             // face node with transverse terms enabled
+};
+
+struct LodiArgs {
+    long long N;
+    double shift, cs, c, mach, k1, rho0, dt, localSpacing, kappa;
+    double domainLength[3];  // NumberOfNodes_axis * coarse spacing (Node.cpp:311,324,333,...)
+    int order;
+    int* errorFlag;
+};
+
+template <typename S>
+__device__ __forceinline__ void absMoments(const S* arr, long long N, long long n, double shift, const float* hs,
+                                           double c, double& rho, double* uSI) {
+    double d = 0, jx = 0, jy = 0, jz = 0;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const double g = (double)Store<S>::load(arr + q * N + n, hs[q]);
+        d += g;
+        jx += ex(q) * g;
+        jy += ey(q) * g;
+        jz += ez(q) * g;
+    }
+    rho = shift + d;
+    uSI[0] = c * jx / rho;
+    uSI[1] = c * jy / rho;
+    uSI[2] = c * jz / rho;
+}
+
+template <typename S, int ORDER>
+__global__ void k_lodi(const S* __restrict__ A, S* B, const BNodeDev* __restrict__ nodes, int count, LodiArgs p,
+                       LevelArgs<S> la) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    const BNodeDev b = nodes[t];
+    const float* hs = la.hscale;
+    double densB, veloB[3];
+    absMoments(A, p.N, b.n, p.shift, hs, p.c, densB, veloB);
+    double dN, d2N, vN[3], v2N[3];
+    absMoments((const S*)B, p.N, b.n1, p.shift, hs, p.c, dN, vN);
+    absMoments((const S*)B, p.N, b.n2, p.shift, hs, p.c, d2N, v2N);
+    const double ls = p.localSpacing;
+    double dG = (4. * dN - d2N - 3. * densB) / (-2. * ls);
+    double vG[3];
+    for (int c = 0; c < 3; ++c) vG[c] = (4. * vN[c] - v2N[c] - 3. * veloB[c]) / (-2. * ls);
+    double dGT[2] = {0, 0}, vGT[2][3] = {{0, 0, 0}, {0, 0, 0}};
+    if (b.transverse) {
+        double dT[4], vT[4][3];
+        for (int m = 0; m < 4; ++m) absMoments(A, p.N, b.t[m], p.shift, hs, p.c, dT[m], vT[m]);
+        dGT[0] = (dT[0] - dT[1]) / (2. * ls);
+        dGT[1] = (dT[2] - dT[3]) / (2. * ls);
+        for (int c = 0; c < 3; ++c) {
+            vGT[0][c] = (vT[0][c] - vT[1][c]) / (2. * ls);
+            vGT[1][c] = (vT[2][c] - vT[3][c]) / (2. * ls);
+        }
+    }
+    const int nd = b.normalDir;
+    int perm[3];
+    double L0;
+    if (nd == 0 || nd == 2) { perm[0] = 0; perm[1] = 1; perm[2] = 2; L0 = p.domainLength[0]; }
+    else if (nd == 1 || nd == 3) { perm[0] = 1; perm[1] = 0; perm[2] = 2; L0 = p.domainLength[1]; }
+    else { perm[0] = 2; perm[1] = 0; perm[2] = 1; L0 = p.domainLength[2]; }
+    const bool neg = nd == 0 || nd == 1 || nd == 4;
+    if (neg) {
+        dG = -dG;
+        for (int c = 0; c < 3; ++c) vG[c] = -vG[c];
+    }
+    double sVG[3], sVB[3], sT[2][3];
+    for (int c = 0; c < 3; ++c) {
+        sVG[c] = vG[perm[c]];
+        sVB[c] = veloB[perm[c]];
+        sT[0][c] = vGT[0][perm[c]];
+        sT[1][c] = vGT[1][perm[c]];
+    }
+    // LODIpressureCalcVelocity in the boundary frame
+    const double cs = p.cs, cs2 = cs * cs, csDivL = cs / L0, MaSq = p.mach * p.mach, K1 = p.k1, K2 = p.mach;
+    const double T1 = -(cs2 * (densB * (sT[0][1] + sT[1][2]) + sVB[1] * dGT[0] + sVB[2] * dGT[1]) -
+                        densB * cs * (sVB[1] * sT[0][0] + sVB[2] * sT[1][0]));
+    const double T5 = -(cs2 * (densB * (sT[0][1] + sT[1][2]) + sVB[1] * dGT[0] + sVB[2] * dGT[1]) +
+                        densB * cs * (sVB[1] * sT[0][0] + sVB[2] * sT[1][0]));
+    double L1, L5;
+    if (neg) {
+        L5 = K1 * (1 - MaSq) * csDivL * cs2 * (densB - p.rho0) - K2 * T5 + T5;
+        L1 = (sVB[0] - cs) * cs * (cs * dG - densB * sVG[0]);
+    } else {
+        L1 = K1 * (1 - MaSq) * csDivL * cs2 * (densB - p.rho0) - K2 * T1 + T1;
+        L5 = (sVB[0] + cs) * cs * (cs * dG + densB * sVG[0]);
+    }
+    const double L3 = sVB[0] * sVG[1], L4 = sVB[0] * sVG[2];
+    const double T3 = -(sVB[1] * sT[0][1] + sVB[2] * sT[1][1]) - (cs2 / densB) * dGT[0];
+    const double T4 = -(sVB[1] * sT[0][2] + sVB[2] * sT[1][2]) - (cs2 / densB) * dGT[1];
+    const double dt = p.dt;
+    const double rho = densB - dt / (2. * cs2) * (L5 + L1) + dt / (2. * cs2) * (T5 + T1);
+    double v[3];
+    v[0] = sVB[0] - dt / (2. * densB * cs) * (L5 - L1) + dt / (2. * densB * cs) * (T5 - T1);
+    v[1] = sVB[1] - dt * L3 + dt * T3;
+    v[2] = sVB[2] - dt * L4 + dt * T4;
+    double u[3];
+    for (int c = 0; c < 3; ++c) u[perm[c]] = v[c] / p.c;
+    if (!(rho > 0.5 * p.rho0 && rho < 1.5 * p.rho0)) atomicOr(p.errorFlag, 1);
+    EqCoef<double, ORDER> ec;
+    ec.set(u, p.kappa);
+    const double drho = rho - p.shift;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const double geq = wq(q) * (drho + rho * ec.poly(q, p.kappa));
+        Store<S>::store(B + q * p.N + b.n, (decltype(Store<S>::load(B, 1.f)))geq, hs[q]);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// initial condition (Lattice::initialization, Lattice.cpp:1397-1493): f is
+// the equilibrium at rest of the pulse density, in both arrays
+struct InitArgs {
+    int ic;                 // enum acp_ic
+    double spacingLevel;    // level spacing [m]
+    double halfDomain[2];   // Domain-Size-X/2, Domain-Size-Y/2
+    double rho0;
+    double eps, b, cell;    // Gaussian: amplitude, half-width (coarse cells), level cell size in coarse cells
+    double center[3];
+    int dims3;
+    int off[3];             // level index of the box origin (coarse-cell units * 2^level)
+};
+
+template <typename S>
+__global__ void k_init(LevelArgs<S> a, InitArgs ia) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y, k = blockIdx.z;
+    if (i >= a.nx) return;
+    const long long n = ((long long)k * a.ny + j) * a.nx + i;
+    const int gi = i + ia.off[0], gj = j + ia.off[1], gk = k + ia.off[2];
+    double rho;
+    if (ia.ic == 0) {
+        const double Rc = 0.06, A = 0.01, xCenter = -8. * Rc;
+        const double xNode = gi * ia.spacingLevel - ia.halfDomain[0];
+        const double yNode = gj * ia.spacingLevel - ia.halfDomain[1];
+        const double xRel = xNode - xCenter;
+        rho = ia.rho0 * (1 + A * exp(-(xRel * xRel + yNode * yNode) / (2 * Rc * Rc)));
+    } else {
+        const double dx = gi * ia.cell - ia.center[0], dy = gj * ia.cell - ia.center[1];
+        const double dz = ia.dims3 ? gk * ia.cell - ia.center[2] : 0.0;
+        rho = ia.rho0 * (1 + ia.eps * exp(-0.69314718055994530942 * (dx * dx + dy * dy + dz * dz) / (ia.b * ia.b)));
+    }
+    const double drho = rho - a.shift;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const double g = wq(q) * drho;
+        Store<S>::store(a.B + q * a.N + n, (decltype(Store<S>::load(a.B, 1.f)))g, a.hscale[q]);
+        Store<S>::store(const_cast<S*>(a.A) + q * a.N + n, (decltype(Store<S>::load(a.B, 1.f)))g, a.hscale[q]);
+    }
+}
+
+// storage <-> absolute FP64 populations
+template <typename S>
+__global__ void k_to_f64(const S* __restrict__ src, double* dst, long long N, double shift, LevelArgs<S> la) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= N * Q) return;
+    const int q = (int)(t / N);
+    dst[t] = (double)Store<S>::load(src + t, la.hscale[q]) + wq(q) * shift;
+}
+template <typename S>
+__global__ void k_from_f64(const double* __restrict__ src, S* dst0, S* dst1, long long N, double shift, LevelArgs<S> la) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= N * Q) return;
+    const int q = (int)(t / N);
+    const double g = src[t] - wq(q) * shift;
+    Store<S>::store(dst0 + t, (decltype(Store<S>::load(dst0, 1.f)))g, la.hscale[q]);
+    Store<S>::store(dst1 + t, (decltype(Store<S>::load(dst0, 1.f)))g, la.hscale[q]);
+}
+
+// pressure probes: p = rho cs^2 (Node::calcPressure, Node.cpp:64-83) at each
+// probe after the step, appended to an FP64 series
+template <typename S>
+__global__ void k_probes(const S* __restrict__ arr, LevelArgs<S> la, const long long* nodes, int count, double shift,
+                         double cs2, double* series, int* counter, int capacity) {
+    const int t = threadIdx.x;
+    const int s = *counter;
+    for (int m = t; m < count; m += blockDim.x) {
+        double d = 0;
+#pragma unroll
+        for (int q = 0; q < Q; ++q) d += (double)Store<S>::load(arr + q * la.N + nodes[m], la.hscale[q]);
+        if (s < capacity) series[(long long)s * count + m] = (shift + d) * cs2;
+    }
+    __syncthreads();
+    if (t == 0) *counter = s + 1;
+}
+
+}  // namespace acp

@@ -1,0 +1,298 @@
+"""Benchmark of the acPulse_vcLBM hot path on B200.
+
+Workload (default): the operator/scheme sweep configuration's lattice -- a
+quasi-2D Gaussian pulse on 1024 x 512 x 3 coarse nodes, periodic in y and z,
+LODI non-reflecting faces in x, HRR collision (sigma = 0.98, order 3),
+nu = 1e-4 lattice units, eps = 1e-3, b = 24 cells.  Inputs are synthetic
+(seeded pulse parameters); there is no dataset.
+
+A step is one coarse time step of the whole lattice.  `value` is the
+FP32-deviation form's throughput in MLUPS (node updates per second / 1e6)
+with the state resident in HBM; the FP64 form runs the same steps and its
+MLUPS, the FP32/FP64 ratio and the FP32 form's pressure error against FP64
+are reported beside it.  Timing: CUDA events on the stream the engine
+launches on, W warm-up steps, K timed steps, max over ranks.  The working set
+(populations, two arrays) is larger than the 126 MB L2, so no flush is needed.
+
+`--impl reference` times the CPU FP64 oracle (the restated reference, all
+host threads) on the same workload and prints the same JSON line shape.
+
+usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "MLUPS & %HBM peak: FP32-shifted vs FP64 at ≤1e-5 rel err; p99 solve latency"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--op", default="HRR")
+    ap.add_argument("--nx", type=int, default=1024)
+    ap.add_argument("--ny", type=int, default=512)
+    ap.add_argument("--nz", type=int, default=3)
+    ap.add_argument("--nu", type=float, default=1e-4)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload(args, storage):
+    from acpulse_vclbm_b200.capi import lattice_units_case
+    d = lattice_units_case(args.nx, args.ny, args.nz, op=args.op, nu_lu=args.nu, order=3,
+                           periodic=(False, True, True), eps=1e-3, b=24.0,
+                           center=(args.nx / 4.0, args.ny / 2.0, 1.0), storage=storage)
+    d.hybrid_sigma = 0.98
+    d.mrt_writeback = 1
+    return d
+
+
+def config_of(args):
+    return {"workload": f"quasi-2D Gaussian pulse, {args.nx}x{args.ny}x{args.nz} coarse nodes, single level, "
+                        f"periodic y/z, LODI x faces, {args.op} order 3, nu={args.nu:g} lu, eps=1e-3, b=24",
+            "nodes": args.nx * args.ny * args.nz, "op": args.op, "levels": 1,
+            "l2_flush": "not needed: population arrays exceed the 126 MB L2",
+            "parallelism": f"replicas x{args.gpus}"}
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def start(self):
+        def run():
+            q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap")
+            while not self._stop.is_set():
+                try:
+                    out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                         timeout=5).stdout.strip()
+                    if out:
+                        self.samples.append([v.strip() for v in out.split(",")])
+                except Exception:
+                    pass
+                self._stop.wait(0.2)
+        self._t = threading.Thread(target=run, daemon=True)
+        self._t.start()
+
+    def stop(self):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no nvidia-smi samples"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if s[3 + k] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        j = json.load(open(p))
+        return float(j["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel_key):
+    """DRAM bytes per launch of the collide kernel from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.exists(p):
+        j = json.load(open(p))
+        return j.get(kernel_key)
+    return None
+
+
+def dist_setup(n):
+    if n <= 1:
+        return None, 0
+    import torch.distributed as dist
+    import datetime
+    rank = int(os.environ.get("RANK", "0"))
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return dist, rank
+
+
+def time_gpu(L, steps, warmup, torch, stream):
+    L.step(warmup)
+    L.sync()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    s.record(stream)
+    L.step(steps)
+    e.record(stream)
+    torch.cuda.synchronize()
+    L.sync()
+    return s.elapsed_time(e)
+
+
+def cpu_oracle_mlups(desc, budget_s=12.0, max_steps=40, threads=0):
+    from oracle.pyoracle import OracleLattice
+    o = OracleLattice(desc, threads=threads)
+    o.init()
+    o.step(1)  # warm
+    n = 0
+    t0 = time.perf_counter()
+    while n < max_steps and time.perf_counter() - t0 < budget_s:
+        o.step(1)
+        n += 1
+    dt = time.perf_counter() - t0
+    nodes = desc.nx * desc.ny * desc.nz
+    return nodes * n / dt / 1e6, n, dt
+
+
+def run_reference(args):
+    dist, rank = dist_setup(args.gpus)
+    if rank != 0:
+        return
+    d = workload(args, "FP64")
+    threads = os.cpu_count() or 1
+    from oracle.pyoracle import OracleLattice
+    o = OracleLattice(d, threads=threads)
+    o.init()
+    o.step(min(args.warmup, 1))
+    t0 = time.perf_counter()
+    o.step(args.steps)
+    dt = time.perf_counter() - t0
+    nodes = d.nx * d.ny * d.nz
+    v = nodes * args.steps / dt / 1e6
+    line = {"impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": "MLUPS", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": config_of(args),
+            "cpu_baseline": {"value": round(v, 3), "unit": "MLUPS", "cores": threads, "kind": "port",
+                             "sample": f"{args.steps} coarse steps of the full workload, FP64 oracle"},
+            "e2e": {"value": round(v, 3), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_engine(args):
+    import torch
+    dist, rank = dist_setup(args.gpus)
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    from acpulse_vclbm_b200 import engine
+    # the engine launches on this stream; the timing events are recorded on it
+    tstream = torch.cuda.Stream()
+    stream = tstream.cuda_stream
+
+    d32 = workload(args, "FP32-DEV")
+    d64 = workload(args, "FP64")
+    nodes = d32.nx * d32.ny * d32.nz
+
+    L32 = engine.Lattice(d32, device=local)
+    engine.lib().acp_set_stream(L32._h, stream)
+    L32.init()
+    L64 = engine.Lattice(d64, device=local)
+    engine.lib().acp_set_stream(L64._h, stream)
+    L64.init()
+
+    if dist:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms32 = time_gpu(L32, args.steps, args.warmup, torch, tstream)
+    ms64 = time_gpu(L64, args.steps, args.warmup, torch, tstream)
+    clk = clocks.stop()
+    if dist:
+        t = torch.tensor([ms32, ms64], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms32, ms64 = t.tolist()
+
+    # accuracy of the FP32 deviation form against FP64 after the same steps
+    cs2 = d64.speed_of_sound ** 2
+    p32 = L32.field(4)
+    p64 = L64.field(4)
+    rel_err = float(np.abs(p32 - p64).max() / (d64.ic_eps * d64.density * cs2))
+
+    # per-kernel device time (events between launches) for the roofline
+    import ctypes as C
+    km = (C.c_double * 5)()
+    engine.lib().acp_step_timed.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+    engine.lib().acp_step_timed(L32._h, 20, C.cast(km, C.c_void_p))
+    collide_ms32 = km[1]
+    km64 = (C.c_double * 5)()
+    engine.lib().acp_step_timed(L64._h, 20, C.cast(km64, C.c_void_p))
+    lps = C.c_int()
+    engine.lib().acp_launches_per_step(L32._h, C.byref(lps))
+    peak, peak_kind = peaks()
+    alg_bytes = nodes * 2 * 19 * 4  # FP32 deviation storage: read 19 + write 19 per node
+    achieved = alg_bytes / (collide_ms32 * 1e-3) / 1e9
+    L32.close()
+    L64.close()
+
+    # end to end through the C ABI with host buffers: create (H2D of node
+    # classes and boundary wiring), init, K steps, D2H of the pressure field
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    Le = engine.Lattice(d32, device=local).init()
+    Le.step(args.steps)
+    Le.sync()
+    pe = Le.field(4)
+    t1 = time.perf_counter()
+    h2d = nodes + 2 * (d32.ny * d32.nz) * 80  # node classes + LODI wiring records
+    d2h = nodes * 19 * 8  # populations read back for the pressure field
+    Le.close()
+    e2e = nodes * args.steps / (t1 - t0) / 1e6
+
+    mlups32 = nodes * args.steps / (ms32 * 1e-3) / 1e6 * args.gpus
+    mlups64 = nodes * args.steps / (ms64 * 1e-3) / 1e6 * args.gpus
+    cpu = None
+    if rank == 0 and args.gpus == 1 and not args.no_cpu_baseline:
+        v, n, dt = cpu_oracle_mlups(d64, threads=os.cpu_count() or 1)
+        cpu = {"value": round(v, 3), "unit": "MLUPS", "cores": os.cpu_count(), "kind": "port",
+               "sample": f"{n} coarse steps of the full workload in {dt:.1f} s (FP64 CPU oracle, OpenMP)"}
+    if rank == 0:
+        line = {"metric": METRIC, "value": round(mlups32, 2), "unit": "MLUPS", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms32 / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic", "config": config_of(args),
+                "fp64": {"value": round(mlups64, 2), "unit": "MLUPS", "ms_per_step": ms64 / args.steps,
+                         "collide_ms": km64[1]},
+                "fp32_over_fp64": round(mlups32 / mlups64, 3),
+                "fp32_pressure_err_rel_amplitude": rel_err,
+                "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                             "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+                             "kernel": "k_collide_push (FP32 deviation)",
+                             "algorithmic_bytes_per_node": 152, "traffic": ncu_traffic("collide_fp32"),
+                             "kernel_ms": {"moments": km[0], "collide": km[1], "lodi": km[2], "probes": km[4]}},
+                "cpu_baseline": cpu,
+                "e2e": {"value": round(e2e, 2), "unit": "MLUPS", "h2d_bytes_per_step": h2d // args.steps,
+                        "d2h_bytes_per_step": d2h // args.steps},
+                "gpu_launches": lps.value * args.steps,
+                "clocks": clk}
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_engine(a)

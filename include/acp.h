@@ -165,6 +165,22 @@ int acp_set_stream(acp_handle* h, void* cuda_stream);
 int acp_device_bytes(acp_handle* h, size_t* bytes);
 /* Device bytes a case would hold, without allocating (admission by HBM footprint). */
 int acp_estimate_bytes(const acp_case_desc* d, size_t* bytes);
+/* Run n coarse steps kernel by kernel (no graph) with CUDA events between
+ * launches and return the average device time per step of each kernel kind:
+ * kernel_ms[ACP_K_*].  The per-phase timers the reference lacks (its only
+ * timing is wall clock in main.cpp:39-43,126-153). */
+enum acp_kernel_kind { ACP_K_MOMENTS = 0, ACP_K_COLLIDE = 1, ACP_K_LODI = 2, ACP_K_COUPLING = 3, ACP_K_PROBES = 4,
+                       ACP_K_COUNT = 5 };
+int acp_step_timed(acp_handle* h, int n, double* kernel_ms);
+/* Kernel launches one coarse step issues (all levels). */
+int acp_launches_per_step(acp_handle* h, int* launches);
+/* The boundary wiring a case gets (host only, no device needed), one row of
+ * 12 integers per boundary node of the coarse level: i j k normalDir n1 n2
+ * t1a t1b t2a t2b corner pushMask, neighbours as node indices (k*ny+j)*nx+i
+ * or -1, the format the reference's wiring is dumped in for comparison
+ * (Lattice::setConnectivity, Lattice.cpp:500-1394).  rows may be NULL to
+ * query *count. */
+int acp_boundary_wiring(const acp_case_desc* d, long long* rows, long long max_rows, long long* count);
 int acp_destroy(acp_handle* h);
 const char* acp_last_error(const acp_handle* h);
 const char* acp_status_string(int status);
