@@ -1,0 +1,44 @@
+"""Run a few coarse steps of one pulse case, for profilers (ncu) and quick
+timing.  Prints the per-kernel device times of acp_step_timed.
+
+usage: python -m acpulse_vclbm_b200.profile_case [--op HRR] [--storage FP32-DEV]
+           [--nx 1024 --ny 512 --nz 3] [--steps 3] [--levels 1]
+"""
+import argparse
+import ctypes as C
+
+from . import engine
+from .capi import lattice_units_case
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--op", default="HRR")
+    ap.add_argument("--storage", default="FP32-DEV")
+    ap.add_argument("--order", type=int, default=3)
+    ap.add_argument("--nx", type=int, default=1024)
+    ap.add_argument("--ny", type=int, default=512)
+    ap.add_argument("--nz", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--timed", type=int, default=0, help="also run N steps kernel by kernel with events")
+    a = ap.parse_args()
+    d = lattice_units_case(a.nx, a.ny, a.nz, op=a.op, nu_lu=1e-4, order=a.order, periodic=(False, True, True),
+                           eps=1e-3, b=24.0, center=(a.nx / 4.0, a.ny / 2.0, 1.0), storage=a.storage)
+    d.mrt_writeback = 1
+    L = engine.Lattice(d).init()
+    L.step(a.steps)
+    L.sync()
+    if a.timed:
+        km = (C.c_double * 5)()
+        engine.lib().acp_step_timed.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        engine.lib().acp_step_timed(L._h, a.timed, C.cast(km, C.c_void_p))
+        nodes = a.nx * a.ny * a.nz
+        b = {"FP64": 8, "FP32-DEV": 4, "FP16-DEV": 2}[a.storage] * 38
+        print(f"{a.op} {a.storage} order {a.order} {a.nx}x{a.ny}x{a.nz}: moments {km[0]*1e3:.1f} us, "
+              f"collide {km[1]*1e3:.1f} us ({nodes * b / (km[1] * 1e-3) / 1e9:.0f} GB/s algorithmic), "
+              f"lodi {km[2]*1e3:.1f} us")
+    L.close()
+
+
+if __name__ == "__main__":
+    main()
