@@ -33,7 +33,6 @@ struct LevelHost {
 struct LevelDev {
     void* f[2] = {nullptr, nullptr};
     uint8_t* code = nullptr;
-    Moments* mom = nullptr;
     BNodeDev* lodiX = nullptr;
     BNodeDev* lodiZY = nullptr;
     int nLodiX = 0, nLodiZY = 0;
@@ -160,7 +159,8 @@ int uploadConstants() {
 int validate(const acp_case_desc* d, std::string& why) {
     if (!d) { why = "null case"; return ACP_ERR_INVALID; }
     if (d->nx < 1 || d->ny < 1 || d->nz < 1) { why = "node counts must be positive"; return ACP_ERR_INVALID; }
-    if ((long long)d->nx * d->ny * d->nz > (1LL << 34)) { why = "lattice too large"; return ACP_ERR_INVALID; }
+    // element indices of a level are 32-bit: 19 populations x nodes < 2^31
+    if ((long long)d->nx * d->ny * d->nz > 100000000LL) { why = "more than 1e8 nodes in one level"; return ACP_ERR_UNSUPPORTED; }
     if (d->op < 0 || d->op > 4) { why = "unknown collision model"; return ACP_ERR_INVALID; }
     if (d->eq_order < 2 || d->eq_order > 4) { why = "Wrong order of equilibrium! (2, 3 or 4)"; return ACP_ERR_INVALID; }
     if (!(d->spacing > 0) || !(d->speed_of_sound > 0) || !(d->density > 0) || !(d->kinematic_viscosity > 0)) {
@@ -252,7 +252,6 @@ LevelArgs<S> levelArgs(acp_handle* h, int l, int src) {
     a.A = (const S*)D.f[src];
     a.B = (S*)D.f[1 - src];
     a.code = D.code;
-    a.mom = D.mom;
     a.shift = h->shift;
     a.omega = L.omega;
     a.kappa = h->kappa;
@@ -265,17 +264,17 @@ template <typename S>
 using CollideFn = void (*)(LevelArgs<S>);
 
 template <typename S, typename R, int OP>
-CollideFn<S> pickOrder(int order, bool cubic) {
+CollideFn<S> pickOrder(int order, bool) {
     switch (order) {
-        case 2: return cubic ? k_collide_push<S, R, OP, 2, true, false> : k_collide_push<S, R, OP, 2, false, false>;
-        case 3: return cubic ? k_collide_push<S, R, OP, 3, true, false> : k_collide_push<S, R, OP, 3, false, false>;
-        default: return cubic ? k_collide_push<S, R, OP, 4, true, false> : k_collide_push<S, R, OP, 4, false, false>;
+        case 2: return k_collide_push<S, R, OP, 2, false, false>;
+        case 3: return k_collide_push<S, R, OP, 3, false, false>;
+        default: return k_collide_push<S, R, OP, 4, false, false>;
     }
 }
 
 template <typename S, typename R>
 CollideFn<S> pickCollide(const acp_case_desc& d) {
-    const bool cubic = d.cubic_mach != 0;
+
     switch (d.op) {
         case OP_SRT:
             switch (d.eq_order) {
@@ -289,8 +288,27 @@ CollideFn<S> pickCollide(const acp_case_desc& d) {
         case OP_MRT_RM:
             return d.mrt_writeback ? k_collide_push<S, R, OP_MRT_RM, 2, false, true>
                                    : k_collide_push<S, R, OP_MRT_GS, 2, false, false>;
-        case OP_RR: return pickOrder<S, R, OP_RR>(d.eq_order, cubic);
-        default: return pickOrder<S, R, OP_HRR>(d.eq_order, cubic);
+        default: return pickOrder<S, R, OP_RR>(d.eq_order, false);
+    }
+}
+
+template <typename S>
+using TiledFn = void (*)(LevelArgs<S>, int);
+
+template <typename S, typename R>
+TiledFn<S> pickTiled(const acp_case_desc& d) {
+    const bool cubic = d.cubic_mach != 0;
+    if (d.op == OP_RR) {
+        switch (d.eq_order) {
+            case 2: return k_collide_push_tiled<S, R, OP_RR, 2, true>;
+            case 3: return k_collide_push_tiled<S, R, OP_RR, 3, true>;
+            default: return k_collide_push_tiled<S, R, OP_RR, 4, true>;
+        }
+    }
+    switch (d.eq_order) {
+        case 2: return cubic ? k_collide_push_tiled<S, R, OP_HRR, 2, true> : k_collide_push_tiled<S, R, OP_HRR, 2, false>;
+        case 3: return cubic ? k_collide_push_tiled<S, R, OP_HRR, 3, true> : k_collide_push_tiled<S, R, OP_HRR, 3, false>;
+        default: return cubic ? k_collide_push_tiled<S, R, OP_HRR, 4, true> : k_collide_push_tiled<S, R, OP_HRR, 4, false>;
     }
 }
 
@@ -330,10 +348,18 @@ int enqueueLevelStep(acp_handle* h, int l, int src, PhaseTimer* tm = nullptr) {
     const int bx = 128;
     if (tm) tm->mark(-1);
     if (needsMoments(h->d)) {
-        k_moments<S><<<gridOf(L, bx), bx, 0, h->stream>>>(a);
-        if (tm) tm->mark(ACP_K_MOMENTS);
+        // z-marching tiles; a periodic z axis of <= 3 planes is resident at once
+        const int bxy = ((L.nx + TX - 1) / TX) * ((L.ny + TY - 1) / TY);
+        int chunk = L.nz;
+        if (!(h->d.bc[2] == ACP_BC_PERIODIC && L.nz <= 3)) {
+            const int want = (4 * 148 + bxy - 1) / bxy;  // z chunks for >= 4 blocks per SM
+            chunk = std::max(8, (L.nz + want - 1) / want);
+        }
+        dim3 grid((L.nx + TX - 1) / TX, (L.ny + TY - 1) / TY, (L.nz + chunk - 1) / chunk);
+        pickTiled<S, R>(h->d)<<<grid, dim3(TX, TY), 0, h->stream>>>(a, chunk);
+    } else {
+        pickCollide<S, R>(h->d)<<<gridOf(L, bx), bx, 0, h->stream>>>(a);
     }
-    pickCollide<S, R>(h->d)<<<gridOf(L, bx), bx, 0, h->stream>>>(a);
     if (tm) tm->mark(ACP_K_COLLIDE);
     LodiArgs p;
     p.N = L.N;
@@ -375,7 +401,7 @@ int enqueueStep(acp_handle* h, int src, PhaseTimer* tm = nullptr) {
 int launchesPerStep(const acp_handle* h) {
     int n = 0;
     for (size_t l = 0; l < h->host.size(); ++l) {
-        n += 1 + (needsMoments(h->d) ? 1 : 0);
+        n += 1;
         n += (h->dev[l].nLodiX ? 1 : 0) + (h->dev[l].nLodiZY ? 1 : 0);
         if (h->nProbes && h->probeLevel == (int)l) ++n;
     }
@@ -450,7 +476,6 @@ int devAlloc(acp_handle* h, void** p, size_t bytes) {
 size_t estimateBytes(const acp_case_desc& d) {
     const long long N = (long long)d.nx * d.ny * d.nz;
     size_t b = (size_t)N * (2 * Q * storageBytes(d.storage) + 1);
-    if (needsMoments(d)) b += (size_t)N * sizeof(Moments);
     long long surf = 2LL * ((long long)d.nx * d.ny + (long long)d.ny * d.nz + (long long)d.nx * d.nz);
     b += (size_t)surf * sizeof(BNodeDev);
     return b;
@@ -539,7 +564,6 @@ int acp_create(const acp_case_desc* d, int device, acp_handle** out) {
             if ((s = devAlloc(h, &D.f[a], (size_t)L.N * Q * sb))) return s;
         if ((s = devAlloc(h, (void**)&D.code, (size_t)L.N))) return s;
         CU(h, cudaMemcpyAsync(D.code, L.code.data(), (size_t)L.N, cudaMemcpyHostToDevice, h->stream));
-        if (needsMoments(*d) && (s = devAlloc(h, (void**)&D.mom, (size_t)L.N * sizeof(Moments)))) return s;
         D.nLodiX = (int)L.lodiX.size();
         D.nLodiZY = (int)L.lodiZY.size();
         if (D.nLodiX) {
@@ -833,7 +857,6 @@ int acp_destroy(acp_handle* h) {
         cudaFree(D.f[0]);
         cudaFree(D.f[1]);
         cudaFree(D.code);
-        cudaFree(D.mom);
         cudaFree(D.lodiX);
         cudaFree(D.lodiZY);
     }

@@ -31,8 +31,10 @@ __constant__ double c_gsMinv[Q][Q];
 __constant__ double c_gsMw[Q];
 __constant__ double c_rmTinv2[Q][5];
 
-struct Moments {
-    double rho, ux, uy, uz;  // lattice units, absolute density
+// pre-collision density (absolute) and lattice velocity of a node
+template <typename R>
+struct MomR {
+    R rho, ux, uy, uz;
 };
 
 template <typename S>
@@ -43,7 +45,6 @@ struct LevelArgs {
     const S* A;  // array read this step
     S* B;        // array written this step
     const uint8_t* code;
-    Moments* mom;
     double shift;   // w_q * shift is subtracted in storage (0 for the FP64 form)
     double omega;   // collision frequency of the level
     double kappa;   // 1/(6 c^2): fourth-order orthogonalisation constant
@@ -56,6 +57,11 @@ __device__ __forceinline__ int wrapc(int c, int n, int per) {
     if (c >= n) return per ? c - n : -1;
     return c;
 }
+// any distance: periodic axes wrap modulo n, others report -1 outside [0, n)
+__device__ __forceinline__ int wrapm(int c, int n, int per) {
+    if (c >= 0 && c < n) return c;
+    return per ? ((c % n) + n) % n : -1;
+}
 
 template <typename S>
 __device__ __forceinline__ float scaleOf(const LevelArgs<S>& a, int q) {
@@ -63,39 +69,11 @@ __device__ __forceinline__ float scaleOf(const LevelArgs<S>& a, int q) {
 }
 
 // ---------------------------------------------------------------------------
-// pre-collision moments of every live node (calcDensityPreCol /
-// calcVelocityPreCol, Node.cpp:32-51,121-154)
-template <typename S>
-__global__ void k_moments(LevelArgs<S> a) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y, k = blockIdx.z;
-    if (i >= a.nx) return;
-    const long long n = ((long long)k * a.ny + j) * a.nx + i;
-    if (a.code[n] == CODE_DEAD) return;
-    double d = 0, jx = 0, jy = 0, jz = 0;
-#pragma unroll
-    for (int q = 0; q < Q; ++q) {
-        const double g = (double)Store<S>::load(a.A + q * a.N + n, scaleOf(a, q));
-        d += g;
-        jx += ex(q) * g;
-        jy += ey(q) * g;
-        jz += ez(q) * g;
-    }
-    const double rho = a.shift + d;
-    Moments m;
-    m.rho = rho;
-    m.ux = jx / rho;
-    m.uy = jy / rho;
-    m.uz = jz / rho;
-    a.mom[n] = m;
-}
-
-// ---------------------------------------------------------------------------
 // collision of one fluid node in registers (deviation form)
 template <typename R, int OP, int ORDER, bool CUBIC, bool MRTWB>
 struct Collider {
     template <typename ST>
-    __device__ __forceinline__ static void run(R* g, const LevelArgs<ST>& a, int i, int j, int k) {
+    __device__ __forceinline__ static void run(R* g, const LevelArgs<ST>& a, const MomR<R>* nb) {
         if (OP == OP_MRT_GS || OP == OP_MRT_RM) {
             if (!MRTWB) return;  // the reference discards the MRT back transform (Node.cpp:2603,2833)
         }
@@ -212,42 +190,38 @@ struct Collider {
             return;
         }
 
-        // RR / HRR: neighbours' pre-collision moments where needed
+        // RR / HRR: neighbours' pre-collision moments (+x, -x, +y, -y, +z, -z)
         R S[6] = {0, 0, 0, 0, 0, 0};
         R hpsi[Q];
         if (OP == OP_HRR || CUBIC) {
-            const int ip = wrapc(i + 1, a.nx, a.per[0]), im = wrapc(i - 1, a.nx, a.per[0]);
-            const int jp = wrapc(j + 1, a.ny, a.per[1]), jm = wrapc(j - 1, a.ny, a.per[1]);
-            const int kp = wrapc(k + 1, a.nz, a.per[2]), km = wrapc(k - 1, a.nz, a.per[2]);
-            const long long row = (long long)a.nx, pl = (long long)a.nx * a.ny;
-            const long long base = (long long)k * pl + (long long)j * row;
-            const Moments mxp = a.mom[base + ip], mxm = a.mom[base + im];
-            const Moments myp = a.mom[(long long)k * pl + (long long)jp * row + i];
-            const Moments mym = a.mom[(long long)k * pl + (long long)jm * row + i];
-            const Moments mzp = a.mom[(long long)kp * pl + (long long)j * row + i];
-            const Moments mzm = a.mom[(long long)km * pl + (long long)j * row + i];
+            const MomR<R>& mxp = nb[0];
+            const MomR<R>& mxm = nb[1];
+            const MomR<R>& myp = nb[2];
+            const MomR<R>& mym = nb[3];
+            const MomR<R>& mzp = nb[4];
+            const MomR<R>& mzm = nb[5];
             if (OP == OP_HRR) {
-                S[0] = R(0.5) * R(mxp.ux - mxm.ux);
-                S[1] = R(0.5) * R(myp.uy - mym.uy);
-                S[2] = R(0.5) * R(mzp.uz - mzm.uz);
-                S[3] = R(0.5) * (R(0.5) * R(mxp.uy - mxm.uy) + R(0.5) * R(myp.ux - mym.ux));
-                S[4] = R(0.5) * (R(0.5) * R(mxp.uz - mxm.uz) + R(0.5) * R(mzp.ux - mzm.ux));
-                S[5] = R(0.5) * (R(0.5) * R(myp.uz - mym.uz) + R(0.5) * R(mzp.uy - mzm.uy));
+                S[0] = R(0.5) * (mxp.ux - mxm.ux);
+                S[1] = R(0.5) * (myp.uy - mym.uy);
+                S[2] = R(0.5) * (mzp.uz - mzm.uz);
+                S[3] = R(0.25) * ((mxp.uy - mxm.uy) + (myp.ux - mym.ux));
+                S[4] = R(0.25) * ((mxp.uz - mxm.uz) + (mzp.ux - mzm.ux));
+                S[5] = R(0.25) * ((myp.uz - mym.uz) + (mzp.uy - mzm.uy));
             }
             if (CUBIC) {
                 // Psi terms of the neighbours (Node.cpp:1832-1841) and their central differences
-                auto psiT = [](const Moments& m, R* P) {
-                    const R r = R(m.rho), x = R(m.ux), y = R(m.uy), z = R(m.uz);
-                    P[0] = r * x * x * x;               // XXX
-                    P[1] = R(0.5) * r * y * z * z;      // XXY
-                    P[2] = R(0.5) * r * z * y * y;      // XXZ
-                    P[3] = R(0.5) * r * x * z * z;      // XYY
-                    P[4] = r * y * y * y;               // YYY
-                    P[5] = R(0.5) * r * z * x * x;      // YYZ
-                    P[6] = R(0.5) * r * x * y * y;      // XZZ
-                    P[7] = R(0.5) * r * y * x * x;      // YZZ
-                    P[8] = r * z * z * z;               // ZZZ
-                    P[9] = r * x * y * z;               // XYZ
+                auto psiT = [](const MomR<R>& m, R* P) {
+                    const R r = m.rho, x = m.ux, y = m.uy, z = m.uz;
+                    P[0] = r * x * x * x;           // XXX
+                    P[1] = R(0.5) * r * y * z * z;  // XXY
+                    P[2] = R(0.5) * r * z * y * y;  // XXZ
+                    P[3] = R(0.5) * r * x * z * z;  // XYY
+                    P[4] = r * y * y * y;           // YYY
+                    P[5] = R(0.5) * r * z * x * x;  // YYZ
+                    P[6] = R(0.5) * r * x * y * y;  // XZZ
+                    P[7] = R(0.5) * r * y * x * x;  // YZZ
+                    P[8] = r * z * z * z;           // ZZZ
+                    P[9] = r * x * y * z;           // XYZ
                 };
                 R Pxp[10], Pxm[10], Pyp[10], Pym[10], Pzp[10], Pzm[10];
                 psiT(mxp, Pxp); psiT(mxm, Pxm); psiT(myp, Pyp); psiT(mym, Pym); psiT(mzp, Pzp); psiT(mzm, Pzm);
@@ -300,38 +274,176 @@ struct Collider {
 };
 
 // ---------------------------------------------------------------------------
-// collide + push (one thread per node; x fastest so that each direction's
-// loads and stores are coalesced)
+// push of a node's 18 moving populations and the rest population.  Element
+// offsets of the neighbours are formed once per thread (wrapped on periodic
+// axes); fluid nodes push everywhere, boundary nodes along their class mask.
+struct NbOffsets {
+    int dx[3], dy[3], dz[3];  // offsets for e = -1, 0, +1 along each axis
+};
+
+template <typename S>
+__device__ __forceinline__ NbOffsets nbOffsets(const LevelArgs<S>& a, int i, int j, int k) {
+    NbOffsets o;
+    const int row = a.nx, pl = a.nx * a.ny;
+    o.dx[0] = (i == 0) ? (a.nx - 1) : -1;
+    o.dx[1] = 0;
+    o.dx[2] = (i == a.nx - 1) ? -(a.nx - 1) : 1;
+    o.dy[0] = (j == 0) ? (a.ny - 1) * row : -row;
+    o.dy[1] = 0;
+    o.dy[2] = (j == a.ny - 1) ? -(a.ny - 1) * row : row;
+    o.dz[0] = (k == 0) ? (a.nz - 1) * pl : -pl;
+    o.dz[1] = 0;
+    o.dz[2] = (k == a.nz - 1) ? -(a.nz - 1) * pl : pl;
+    return o;
+}
+
+template <typename S, typename R>
+__device__ __forceinline__ void pushNode(const LevelArgs<S>& a, const R* g, int n, uint32_t mask, const NbOffsets& o) {
+    S* B = a.B;
+#pragma unroll
+    for (int q = 0; q < 18; ++q) {
+        if (!(mask >> q & 1u)) continue;
+        const int t = n + o.dx[ex(q) + 1] + o.dy[ey(q) + 1] + o.dz[ez(q) + 1];
+        Store<S>::store(B + (long long)q * a.N + t, g[q], scaleOf(a, q));
+    }
+    Store<S>::store(B + 18LL * a.N + n, g[18], scaleOf(a, 18));
+}
+
+// collide + push for operators without neighbour data (SRT, RR, MRT): one
+// thread per node, x fastest so each direction's loads and stores coalesce
 template <typename S, typename R, int OP, int ORDER, bool CUBIC, bool MRTWB>
 __global__ void __launch_bounds__(128) k_collide_push(LevelArgs<S> a) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y, k = blockIdx.z;
     if (i >= a.nx) return;
-    const long long n = ((long long)k * a.ny + j) * a.nx + i;
+    const int n = (k * a.ny + j) * a.nx + i;
     const uint8_t code = a.code[n];
     if (code == CODE_DEAD) return;
     R g[Q];
 #pragma unroll
-    for (int q = 0; q < Q; ++q) g[q] = R(Store<S>::load(a.A + q * a.N + n, scaleOf(a, q)));
+    for (int q = 0; q < Q; ++q) g[q] = R(Store<S>::load(a.A + (long long)q * a.N + n, scaleOf(a, q)));
     uint32_t mask;
     if (code == CODE_FLUID) {
-        Collider<R, OP, ORDER, CUBIC, MRTWB>::run(g, a, i, j, k);
+        Collider<R, OP, ORDER, CUBIC, MRTWB>::run(g, a, (const MomR<R>*)nullptr);
         mask = 0x3FFFFu;
     } else {
         mask = c_pushMask[code];
     }
-    const int xs[3] = {wrapc(i - 1, a.nx, a.per[0]), i, wrapc(i + 1, a.nx, a.per[0])};
-    const int ys[3] = {wrapc(j - 1, a.ny, a.per[1]), j, wrapc(j + 1, a.ny, a.per[1])};
-    const int zs[3] = {wrapc(k - 1, a.nz, a.per[2]), k, wrapc(k + 1, a.nz, a.per[2])};
+    pushNode<S, R>(a, g, n, mask, nbOffsets(a, i, j, k));
+}
+
+// ---------------------------------------------------------------------------
+// collide + push for the operators that read the six axis neighbours'
+// pre-collision (rho, u): HRR (finite-difference strain rate, Node.cpp:1750-1889)
+// and RR with the cubic-Mach correction.  A block owns a TX x TY column of
+// nodes and marches through z; the moments of the planes z-1, z, z+1 of the
+// column and of its one-node ring are formed from the populations in shared
+// memory, so no moment array travels through HBM.  Planes of a periodic z axis
+// of at most three nodes are all resident at once.
+constexpr int TX = 32, TY = 8;
+
+template <typename S, typename R>
+__device__ __forceinline__ MomR<R> nodeMoments(const LevelArgs<S>& a, int n) {
+    R d = 0, jx = 0, jy = 0, jz = 0;
 #pragma unroll
-    for (int q = 0; q < 18; ++q) {
-        if (!(mask >> q & 1u)) continue;
-        const int ti = xs[ex(q) + 1], tj = ys[ey(q) + 1], tk = zs[ez(q) + 1];
-        if ((ti | tj | tk) < 0) continue;
-        const long long t = ((long long)tk * a.ny + tj) * a.nx + ti;
-        Store<S>::store(a.B + q * a.N + t, g[q], scaleOf(a, q));
+    for (int q = 0; q < Q; ++q) {
+        const R g = R(Store<S>::load(a.A + (long long)q * a.N + n, scaleOf(a, q)));
+        d += g;
+        jx += R(ex(q)) * g;
+        jy += R(ey(q)) * g;
+        jz += R(ez(q)) * g;
     }
-    Store<S>::store(a.B + 18 * a.N + n, g[18], scaleOf(a, 18));
+    MomR<R> m;
+    m.rho = R(a.shift) + d;
+    const R inv = R(1) / m.rho;
+    m.ux = jx * inv;
+    m.uy = jy * inv;
+    m.uz = jz * inv;
+    return m;
+}
+
+template <typename S, typename R>
+__device__ __forceinline__ void loadPlaneMoments(const LevelArgs<S>& a, MomR<R> (*slot)[TX + 2], int x0, int y0, int z) {
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+    // own node (on a periodic axis a thread past the end holds the wrapped
+    // node, which is the neighbour of the last node of a partial tile)
+    {
+        const int i = wrapm(x0 + tx, a.nx, a.per[0]), j = wrapm(y0 + ty, a.ny, a.per[1]);
+        if (i >= 0 && j >= 0) {
+            const int n = (z * a.ny + j) * a.nx + i;
+            if (a.code[n] != CODE_DEAD) slot[ty + 1][tx + 1] = nodeMoments<S, R>(a, n);
+        }
+    }
+    // one-node ring (axis neighbours only): bottom row, top row, left column, right column
+    if (tid < 2 * TX + 2 * TY) {
+        int i, j, si, sj;
+        if (tid < TX) { i = x0 + tid; j = y0 - 1; si = tid + 1; sj = 0; }
+        else if (tid < 2 * TX) { i = x0 + tid - TX; j = y0 + TY; si = tid - TX + 1; sj = TY + 1; }
+        else if (tid < 2 * TX + TY) { i = x0 - 1; j = y0 + tid - 2 * TX; si = 0; sj = tid - 2 * TX + 1; }
+        else { i = x0 + TX; j = y0 + tid - 2 * TX - TY; si = TX + 1; sj = tid - 2 * TX - TY + 1; }
+        i = wrapm(i, a.nx, a.per[0]);
+        j = wrapm(j, a.ny, a.per[1]);
+        if (i >= 0 && j >= 0) {
+            const int n = (z * a.ny + j) * a.nx + i;
+            if (a.code[n] != CODE_DEAD) slot[sj][si] = nodeMoments<S, R>(a, n);
+        }
+    }
+}
+
+template <typename S, typename R, int OP, int ORDER, bool CUBIC>
+__global__ void __launch_bounds__(TX * TY) k_collide_push_tiled(LevelArgs<S> a, int zChunk) {
+    __shared__ MomR<R> sm[3][TY + 2][TX + 2];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+    const int i = x0 + tx, j = y0 + ty;
+    const int zBeg = blockIdx.z * zChunk;
+    const int zEnd = min(a.nz, zBeg + zChunk);
+    const bool allResident = a.per[2] && a.nz <= 3;
+    // rolling planes: slot of the unwrapped plane u in [zBeg-1, zEnd] is (u - zBeg + 1) mod 3
+    auto key = [&](int u) { return (u - zBeg + 1) % 3; };
+    if (allResident) {
+        for (int z = 0; z < a.nz; ++z) loadPlaneMoments<S, R>(a, sm[z], x0, y0, z);
+    } else {
+        const int zm = wrapc(zBeg - 1, a.nz, a.per[2]);
+        if (zm >= 0) loadPlaneMoments<S, R>(a, sm[key(zBeg - 1)], x0, y0, zm);
+        loadPlaneMoments<S, R>(a, sm[key(zBeg)], x0, y0, zBeg);
+    }
+    for (int z = zBeg; z < zEnd; ++z) {
+        if (!allResident) {
+            const int zp = wrapc(z + 1, a.nz, a.per[2]);
+            if (zp >= 0) loadPlaneMoments<S, R>(a, sm[key(z + 1)], x0, y0, zp);
+        }
+        __syncthreads();
+        if (i < a.nx && j < a.ny) {
+            const int n = (z * a.ny + j) * a.nx + i;
+            const uint8_t code = a.code[n];
+            if (code != CODE_DEAD) {
+                R g[Q];
+#pragma unroll
+                for (int q = 0; q < Q; ++q) g[q] = R(Store<S>::load(a.A + (long long)q * a.N + n, scaleOf(a, q)));
+                uint32_t mask;
+                if (code == CODE_FLUID) {
+                    // fluid nodes are interior or on periodic axes: every axis neighbour exists
+                    const int sc = allResident ? z : key(z);
+                    const int sp = allResident ? wrapm(z + 1, a.nz, 1) : key(z + 1);
+                    const int sn = allResident ? wrapm(z - 1, a.nz, 1) : key(z - 1);
+                    MomR<R> nb[6];
+                    nb[0] = sm[sc][ty + 1][tx + 2];
+                    nb[1] = sm[sc][ty + 1][tx];
+                    nb[2] = sm[sc][ty + 2][tx + 1];
+                    nb[3] = sm[sc][ty][tx + 1];
+                    nb[4] = sm[sp][ty + 1][tx + 1];
+                    nb[5] = sm[sn][ty + 1][tx + 1];
+                    Collider<R, OP, ORDER, CUBIC, false>::run(g, a, nb);
+                    mask = 0x3FFFFu;
+                } else {
+                    mask = c_pushMask[code];
+                }
+                pushNode<S, R>(a, g, n, mask, nbOffsets(a, i, j, z));
+            }
+        }
+        __syncthreads();  // the slot of z-1 is refilled with z+2 next
+    }
 }
 
 // ---------------------------------------------------------------------------

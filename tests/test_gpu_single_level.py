@@ -155,3 +155,29 @@ def test_numeric_blowup_is_reported():
         L.sync()
     assert e.value.status == ACP_ERR_NUMERIC
     L.close()
+
+
+# the z-marching tiles of the neighbour-moment kernels: partial tiles on
+# periodic axes, chunked z with the rolling planes, one- and two-plane
+# periodic z, and all-LODI boxes
+TILE_CASES = [
+    ("partial-xy-periodic", (37, 11, 3), (True, True, True)),
+    ("all-lodi-chunked-z", (20, 12, 21), (False, False, False)),
+    ("lodi-x-periodic-y-long-z", (24, 10, 40), (False, True, True)),
+    ("single-plane", (36, 20, 1), (False, False, True)),
+    ("two-planes", (36, 20, 2), (False, False, True)),
+    ("periodic-x-small", (9, 13, 5), (True, False, True)),
+]
+
+
+@pytest.mark.parametrize("name,dims,per", TILE_CASES, ids=[c[0] for c in TILE_CASES])
+@pytest.mark.parametrize("op,cubic", [("HRR", 0), ("HRR", 1), ("RR", 1)])
+def test_tiled_neighbour_kernels_match_oracle(name, dims, per, op, cubic):
+    nx, ny, nz = dims
+    d = lattice_units_case(nx, ny, nz, op=op, nu_lu=1e-3, order=3, periodic=per, eps=2e-2, b=3.0,
+                           center=(nx / 2.0 - 0.3, ny / 2.0 + 0.2, nz / 2.0 - 0.1), ic_dims=3)
+    d.cubic_mach = cubic
+    f = run_gpu(d, 40)
+    fo = run_oracle(d, 40)
+    err = np.abs(f - fo).max() / d.ic_eps
+    assert err < 1e-9, err
