@@ -153,6 +153,12 @@ int uploadConstants() {
     if (cudaMemcpyToSymbol(c_gsMinv, gsi, sizeof gsi) != cudaSuccess) return ACP_ERR_CUDA;
     if (cudaMemcpyToSymbol(c_gsMw, mw, sizeof mw) != cudaSuccess) return ACP_ERR_CUDA;
     if (cudaMemcpyToSymbol(c_rmTinv2, rm2, sizeof rm2) != cudaSuccess) return ACP_ERR_CUDA;
+    float gsif[Q * Q], rm2f[Q][5];
+    for (int k = 0; k < Q * Q; ++k) gsif[k] = (float)gsi[k];
+    for (int q = 0; q < Q; ++q)
+        for (int m = 0; m < 5; ++m) rm2f[q][m] = (float)rm2[q][m];
+    if (cudaMemcpyToSymbol(c_gsMinvF, gsif, sizeof gsif) != cudaSuccess) return ACP_ERR_CUDA;
+    if (cudaMemcpyToSymbol(c_rmTinv2F, rm2f, sizeof rm2f) != cudaSuccess) return ACP_ERR_CUDA;
     return ACP_OK;
 }
 

@@ -30,6 +30,8 @@ __constant__ uint32_t c_pushMask[27];
 __constant__ double c_gsMinv[Q][Q];
 __constant__ double c_gsMw[Q];
 __constant__ double c_rmTinv2[Q][5];
+__constant__ float c_gsMinvF[Q][Q];
+__constant__ float c_rmTinv2F[Q][5];
 
 // pre-collision density (absolute) and lattice velocity of a node
 template <typename R>
@@ -69,13 +71,32 @@ __device__ __forceinline__ float scaleOf(const LevelArgs<S>& a, int q) {
 }
 
 // ---------------------------------------------------------------------------
-// collision of one fluid node in registers (deviation form)
+// collision of one fluid node in registers (deviation form).  The
+// post-collision populations are handed to `emit(q, value)` as they are
+// formed, so the regularised operators never hold the old populations and
+// the equilibrium at the same time (the equilibrium is formed twice instead).
+template <typename R>
+struct RT;
+template <>
+struct RT<double> {
+    __device__ __forceinline__ static double gsMinv(int q, int m) { return c_gsMinv[q][m]; }
+    __device__ __forceinline__ static double rmTinv(int q, int m) { return c_rmTinv2[q][m]; }
+};
+template <>
+struct RT<float> {
+    __device__ __forceinline__ static float gsMinv(int q, int m) { return c_gsMinvF[q][m]; }
+    __device__ __forceinline__ static float rmTinv(int q, int m) { return c_rmTinv2F[q][m]; }
+};
+
 template <typename R, int OP, int ORDER, bool CUBIC, bool MRTWB>
 struct Collider {
-    template <typename ST>
-    __device__ __forceinline__ static void run(R* g, const LevelArgs<ST>& a, const MomR<R>* nb) {
-        if (OP == OP_MRT_GS || OP == OP_MRT_RM) {
-            if (!MRTWB) return;  // the reference discards the MRT back transform (Node.cpp:2603,2833)
+    template <typename ST, typename Emit>
+    __device__ __forceinline__ static void run(R* g, const LevelArgs<ST>& a, const R* nb, Emit& emit) {
+        if ((OP == OP_MRT_GS || OP == OP_MRT_RM) && !MRTWB) {
+            // the reference discards the MRT back transform (Node.cpp:2603,2833)
+#pragma unroll
+            for (int q = 0; q < Q; ++q) emit(q, g[q]);
+            return;
         }
         R drho = 0, jx = 0, jy = 0, jz = 0;
 #pragma unroll
@@ -92,52 +113,48 @@ struct Collider {
         const R kappa = R(a.kappa);
 
         if (OP == OP_MRT_GS) {
-            R m[Q];
-#pragma unroll
-            for (int mm = 0; mm < Q; ++mm) {
-                R s = R(a.shift) * R(c_gsMw[mm]);
-#pragma unroll
-                for (int q = 0; q < Q; ++q)
-                    if (gsRow(mm, q) != 0) s += R(gsRow(mm, q)) * g[q];
-                m[mm] = s;
-            }
-            R meq[Q];
-#pragma unroll
-            for (int mm = 0; mm < Q; ++mm) meq[mm] = 0;
-            meq[0] = rho; meq[3] = jx; meq[5] = jy; meq[7] = jz;
-            meq[1] = (jx * jx + jy * jy + jz * jz) * inv;
-            meq[9] = (R(2) * jx * jx - jy * jy - jz * jz) * inv;
-            meq[11] = (jy * jy - jz * jz) * inv;
-            meq[13] = jx * jy * inv;
-            meq[14] = jy * jz * inv;
-            meq[15] = jx * jz * inv;
             R dm[Q];
 #pragma unroll
             for (int mm = 0; mm < Q; ++mm) {
+                R m = R(a.shift) * R(c_gsMw[mm]);
+#pragma unroll
+                for (int q = 0; q < Q; ++q)
+                    if (gsRow(mm, q) != 0) m += R(gsRow(mm, q)) * g[q];
+                R meq = 0;
+                switch (mm) {
+                    case 0: meq = rho; break;
+                    case 1: meq = (jx * jx + jy * jy + jz * jz) * inv; break;
+                    case 3: meq = jx; break;
+                    case 5: meq = jy; break;
+                    case 7: meq = jz; break;
+                    case 9: meq = (R(2) * jx * jx - jy * jy - jz * jz) * inv; break;
+                    case 11: meq = (jy * jy - jz * jz) * inv; break;
+                    case 13: meq = jx * jy * inv; break;
+                    case 14: meq = jy * jz * inv; break;
+                    case 15: meq = jx * jz * inv; break;
+                    default: meq = 0;
+                }
                 const bool conserved = mm == 0 || mm == 3 || mm == 5 || mm == 7;
                 const bool visc = mm == 1 || mm == 9 || mm == 11 || mm == 13 || mm == 14 || mm == 15;
-                dm[mm] = conserved ? R(0) : (visc ? omega : R(1)) * (meq[mm] - m[mm]);
+                dm[mm] = conserved ? R(0) : (visc ? omega : R(1)) * (meq - m);
             }
 #pragma unroll
             for (int q = 0; q < Q; ++q) {
-                R acc = 0;
+                R acc = g[q];
 #pragma unroll
                 for (int mm = 0; mm < Q; ++mm) {
                     const bool conserved = mm == 0 || mm == 3 || mm == 5 || mm == 7;
-                    if (!conserved) acc += R(c_gsMinv[q][mm]) * dm[mm];
+                    if (!conserved) acc += RT<R>::gsMinv(q, mm) * dm[mm];
                 }
-                g[q] += acc;
+                emit(q, acc);
             }
             return;
         }
 
         if (OP == OP_MRT_RM) {
             // extended raw-moment equilibrium (Node.cpp:2627-2645)
-            const R ux = u[0], uy = u[1], uz = u[2];
-            const R u2[3] = {ux * ux, uy * uy, uz * uz};
-            R geq[Q];
-#pragma unroll
-            for (int q = 0; q < Q; ++q) {
+            const R u2[3] = {u[0] * u[0], u[1] * u[1], u[2] * u[2]};
+            auto geqRM = [&](int q) -> R {
                 const int e[3] = {ex(q), ey(q), ez(q)};
                 const int nzc = (e[0] != 0) + (e[1] != 0) + (e[2] != 0);
                 R p;
@@ -156,94 +173,54 @@ struct Collider {
                     p = R(3) * (sa * u[aa] + sb * u[bb]) + R(3) * (u2[aa] + u2[bb]) + R(9) * sa * sb * u[aa] * u[bb] +
                         R(9) * (sb * u2[aa] * u[bb] + sa * u[aa] * u2[bb]) + R(9) * u2[aa] * u2[bb];
                 }
-                geq[q] = R(wq(q)) * (drho + rho * p);
-            }
-            R d[5];
+                return R(wq(q)) * (drho + rho * p);
+            };
+            R d[5] = {0, 0, 0, 0, 0};
 #pragma unroll
-            for (int mm = 0; mm < 5; ++mm) {
-                R s = 0;
+            for (int q = 0; q < Q; ++q) {
+                const R gn = g[q] - geqRM(q);
 #pragma unroll
-                for (int q = 0; q < Q; ++q)
-                    if (rmRow2(mm, q) != 0) s += R(rmRow2(mm, q)) * (g[q] - geq[q]);
-                d[mm] = s;
+                for (int mm = 0; mm < 5; ++mm)
+                    if (rmRow2(mm, q) != 0) d[mm] += R(rmRow2(mm, q)) * gn;
             }
             const R om1 = R(1) - omega;
 #pragma unroll
             for (int q = 0; q < Q; ++q) {
                 R acc = 0;
 #pragma unroll
-                for (int mm = 0; mm < 5; ++mm) acc += R(c_rmTinv2[q][mm]) * d[mm];
-                g[q] = geq[q] + om1 * acc;
+                for (int mm = 0; mm < 5; ++mm) acc += RT<R>::rmTinv(q, mm) * d[mm];
+                emit(q, geqRM(q) + om1 * acc);
             }
             return;
         }
 
         EqCoef<R, ORDER> ec;
         ec.set(u, kappa);
-        R geq[Q];
-#pragma unroll
-        for (int q = 0; q < Q; ++q) geq[q] = R(wq(q)) * (drho + rho * ec.poly(q, kappa));
+        auto geq = [&](int q) -> R { return R(wq(q)) * (drho + rho * ec.poly(q, kappa)); };
 
         if (OP == OP_SRT) {
 #pragma unroll
-            for (int q = 0; q < Q; ++q) g[q] += omega * (geq[q] - g[q]);
+            for (int q = 0; q < Q; ++q) emit(q, g[q] + omega * (geq(q) - g[q]));
             return;
         }
 
-        // RR / HRR: neighbours' pre-collision moments (+x, -x, +y, -y, +z, -z)
+        // RR / HRR: strain rate S and cubic-Mach gradient G from the six axis neighbours
         R S[6] = {0, 0, 0, 0, 0, 0};
-        R hpsi[Q];
+        R G[6] = {0, 0, 0, 0, 0, 0};
         if (OP == OP_HRR || CUBIC) {
-            const MomR<R>& mxp = nb[0];
-            const MomR<R>& mxm = nb[1];
-            const MomR<R>& myp = nb[2];
-            const MomR<R>& mym = nb[3];
-            const MomR<R>& mzp = nb[4];
-            const MomR<R>& mzm = nb[5];
-            if (OP == OP_HRR) {
-                S[0] = R(0.5) * (mxp.ux - mxm.ux);
-                S[1] = R(0.5) * (myp.uy - mym.uy);
-                S[2] = R(0.5) * (mzp.uz - mzm.uz);
-                S[3] = R(0.25) * ((mxp.uy - mxm.uy) + (myp.ux - mym.ux));
-                S[4] = R(0.25) * ((mxp.uz - mxm.uz) + (mzp.ux - mzm.ux));
-                S[5] = R(0.25) * ((myp.uz - mym.uz) + (mzp.uy - mzm.uy));
-            }
-            if (CUBIC) {
-                // Psi terms of the neighbours (Node.cpp:1832-1841) and their central differences
-                auto psiT = [](const MomR<R>& m, R* P) {
-                    const R r = m.rho, x = m.ux, y = m.uy, z = m.uz;
-                    P[0] = r * x * x * x;           // XXX
-                    P[1] = R(0.5) * r * y * z * z;  // XXY
-                    P[2] = R(0.5) * r * z * y * y;  // XXZ
-                    P[3] = R(0.5) * r * x * z * z;  // XYY
-                    P[4] = r * y * y * y;           // YYY
-                    P[5] = R(0.5) * r * z * x * x;  // YYZ
-                    P[6] = R(0.5) * r * x * y * y;  // XZZ
-                    P[7] = R(0.5) * r * y * x * x;  // YZZ
-                    P[8] = r * z * z * z;           // ZZZ
-                    P[9] = r * x * y * z;           // XYZ
-                };
-                R Pxp[10], Pxm[10], Pyp[10], Pym[10], Pzp[10], Pzm[10];
-                psiT(mxp, Pxp); psiT(mxm, Pxm); psiT(myp, Pyp); psiT(mym, Pym); psiT(mzp, Pzp); psiT(mzm, Pzm);
-                auto dX = [&](int c) { return R(0.5) * (Pxp[c] - Pxm[c]); };
-                auto dY = [&](int c) { return R(0.5) * (Pyp[c] - Pym[c]); };
-                auto dZ = [&](int c) { return R(0.5) * (Pzp[c] - Pzm[c]); };
-                R G[6];
-                G[0] = dX(0) + dY(1) + dZ(2);  // xx
-                G[1] = dX(3) + dY(4) + dZ(5);  // yy
-                G[2] = dX(6) + dY(7) + dZ(8);  // zz
-                G[3] = dX(1) + dY(3) + dZ(9);  // xy
-                G[4] = dX(2) + dY(9) + dZ(6);  // xz
-                G[5] = dX(9) + dY(5) + dZ(7);  // yz
 #pragma unroll
-                for (int q = 0; q < Q; ++q) hpsi[q] = R(2.25) * R(wq(q)) * h2dot<R>(q, G);
+            for (int c = 0; c < 6; ++c) {
+                S[c] = nb[c];
+                G[c] = nb[6 + c];
             }
         }
+        // half time step times the cubic-Mach correction of direction q
+        auto hpsi = [&](int q) -> R { return R(2.25) * R(wq(q)) * h2dot<R>(q, G); };
         R P[6] = {0, 0, 0, 0, 0, 0};
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
-            R gn = g[q] - geq[q];
-            if (CUBIC) gn += hpsi[q];
+            R gn = g[q] - geq(q);
+            if (CUBIC) gn += hpsi(q);
             P[0] += h2xx<R>(q) * gn;
             P[1] += h2yy<R>(q) * gn;
             P[2] += h2zz<R>(q) * gn;
@@ -266,9 +243,9 @@ struct Collider {
         const R om1 = R(1) - omega;
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
-            R v = geq[q] + om1 * R(wq(q)) * nc.poly(q, kappa);
-            if (CUBIC) v += hpsi[q];
-            g[q] = v;
+            R v = geq(q) + om1 * R(wq(q)) * nc.poly(q, kappa);
+            if (CUBIC) v += hpsi(q);
+            emit(q, v);
         }
     }
 };
@@ -297,17 +274,24 @@ __device__ __forceinline__ NbOffsets nbOffsets(const LevelArgs<S>& a, int i, int
     return o;
 }
 
-template <typename S, typename R>
-__device__ __forceinline__ void pushNode(const LevelArgs<S>& a, const R* g, int n, uint32_t mask, const NbOffsets& o) {
-    S* B = a.B;
-#pragma unroll
-    for (int q = 0; q < 18; ++q) {
-        if (!(mask >> q & 1u)) continue;
-        const int t = n + o.dx[ex(q) + 1] + o.dy[ey(q) + 1] + o.dz[ez(q) + 1];
-        Store<S>::store(B + (long long)q * a.N + t, g[q], scaleOf(a, q));
+// stores population q of node n into its push target (direction q's
+// neighbour; the rest population stays), skipping directions off the mask
+template <typename S>
+struct Pusher {
+    const LevelArgs<S>& a;
+    int n;
+    uint32_t mask;
+    NbOffsets o;
+    template <typename V>
+    __device__ __forceinline__ void operator()(int q, V v) const {
+        if (q == 18) {
+            Store<S>::store(a.B + 18LL * a.N + n, v, scaleOf(a, 18));
+        } else if (mask >> q & 1u) {
+            const int t = n + o.dx[ex(q) + 1] + o.dy[ey(q) + 1] + o.dz[ez(q) + 1];
+            Store<S>::store(a.B + (long long)q * a.N + t, v, scaleOf(a, q));
+        }
     }
-    Store<S>::store(B + 18LL * a.N + n, g[18], scaleOf(a, 18));
-}
+};
 
 // collide + push for operators without neighbour data (SRT, RR, MRT): one
 // thread per node, x fastest so each direction's loads and stores coalesce
@@ -322,14 +306,14 @@ __global__ void __launch_bounds__(128) k_collide_push(LevelArgs<S> a) {
     R g[Q];
 #pragma unroll
     for (int q = 0; q < Q; ++q) g[q] = R(Store<S>::load(a.A + (long long)q * a.N + n, scaleOf(a, q)));
-    uint32_t mask;
     if (code == CODE_FLUID) {
-        Collider<R, OP, ORDER, CUBIC, MRTWB>::run(g, a, (const MomR<R>*)nullptr);
-        mask = 0x3FFFFu;
+        Pusher<S> emit{a, n, 0x3FFFFu, nbOffsets(a, i, j, k)};
+        Collider<R, OP, ORDER, CUBIC, MRTWB>::run(g, a, (const R*)nullptr, emit);
     } else {
-        mask = c_pushMask[code];
+        Pusher<S> emit{a, n, c_pushMask[code], nbOffsets(a, i, j, k)};
+#pragma unroll
+        for (int q = 0; q < Q; ++q) emit(q, g[q]);
     }
-    pushNode<S, R>(a, g, n, mask, nbOffsets(a, i, j, k));
 }
 
 // ---------------------------------------------------------------------------
@@ -390,8 +374,59 @@ __device__ __forceinline__ void loadPlaneMoments(const LevelArgs<S>& a, MomR<R> 
     }
 }
 
+// strain rate S = {xx,yy,zz,xy,xz,yz} (central differences of the
+// neighbours' velocities, Node.cpp:1882-1888) and the cubic-Mach gradient
+// G of the Psi terms (Node.cpp:1832-1878), both in lattice units, from the
+// six axis neighbours' moments (+x, -x, +y, -y, +z, -z)
+template <typename R, bool STRAIN, bool CUBIC>
+__device__ __forceinline__ void neighbourTerms(const MomR<R>& mxp, const MomR<R>& mxm, const MomR<R>& myp,
+                                               const MomR<R>& mym, const MomR<R>& mzp, const MomR<R>& mzm, R* SG) {
+#pragma unroll
+    for (int c = 0; c < 12; ++c) SG[c] = 0;
+    if (STRAIN) {
+        SG[0] = R(0.5) * (mxp.ux - mxm.ux);
+        SG[1] = R(0.5) * (myp.uy - mym.uy);
+        SG[2] = R(0.5) * (mzp.uz - mzm.uz);
+        SG[3] = R(0.25) * ((mxp.uy - mxm.uy) + (myp.ux - mym.ux));
+        SG[4] = R(0.25) * ((mxp.uz - mxm.uz) + (mzp.ux - mzm.ux));
+        SG[5] = R(0.25) * ((myp.uz - mym.uz) + (mzp.uy - mzm.uy));
+    }
+    if (CUBIC) {
+        auto psiT = [](const MomR<R>& m, R* P) {
+            const R r = m.rho, x = m.ux, y = m.uy, z = m.uz;
+            P[0] = r * x * x * x;           // XXX
+            P[1] = R(0.5) * r * y * z * z;  // XXY
+            P[2] = R(0.5) * r * z * y * y;  // XXZ
+            P[3] = R(0.5) * r * x * z * z;  // XYY
+            P[4] = r * y * y * y;           // YYY
+            P[5] = R(0.5) * r * z * x * x;  // YYZ
+            P[6] = R(0.5) * r * x * y * y;  // XZZ
+            P[7] = R(0.5) * r * y * x * x;  // YZZ
+            P[8] = r * z * z * z;           // ZZZ
+            P[9] = r * x * y * z;           // XYZ
+        };
+        R* G = SG + 6;
+        R Pp[10], Pm[10];
+        psiT(mxp, Pp); psiT(mxm, Pm);
+        G[0] += R(0.5) * (Pp[0] - Pm[0]); G[1] += R(0.5) * (Pp[3] - Pm[3]); G[2] += R(0.5) * (Pp[6] - Pm[6]);
+        G[3] += R(0.5) * (Pp[1] - Pm[1]); G[4] += R(0.5) * (Pp[2] - Pm[2]); G[5] += R(0.5) * (Pp[9] - Pm[9]);
+        psiT(myp, Pp); psiT(mym, Pm);
+        G[0] += R(0.5) * (Pp[1] - Pm[1]); G[1] += R(0.5) * (Pp[4] - Pm[4]); G[2] += R(0.5) * (Pp[7] - Pm[7]);
+        G[3] += R(0.5) * (Pp[3] - Pm[3]); G[4] += R(0.5) * (Pp[9] - Pm[9]); G[5] += R(0.5) * (Pp[5] - Pm[5]);
+        psiT(mzp, Pp); psiT(mzm, Pm);
+        G[0] += R(0.5) * (Pp[2] - Pm[2]); G[1] += R(0.5) * (Pp[5] - Pm[5]); G[2] += R(0.5) * (Pp[8] - Pm[8]);
+        G[3] += R(0.5) * (Pp[9] - Pm[9]); G[4] += R(0.5) * (Pp[6] - Pm[6]); G[5] += R(0.5) * (Pp[7] - Pm[7]);
+    }
+}
+
+// register cap: 2 blocks per SM for FP64 compute, 3 for FP32
+template <typename R>
+struct TiledMinBlocks {
+    static constexpr int value = sizeof(R) == 8 ? 2 : 3;
+};
+
 template <typename S, typename R, int OP, int ORDER, bool CUBIC>
-__global__ void __launch_bounds__(TX * TY) k_collide_push_tiled(LevelArgs<S> a, int zChunk) {
+__global__ void __launch_bounds__(TX * TY, TiledMinBlocks<R>::value) k_collide_push_tiled(LevelArgs<S> a, int zChunk) {
     __shared__ MomR<R> sm[3][TY + 2][TX + 2];
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
@@ -421,25 +456,22 @@ __global__ void __launch_bounds__(TX * TY) k_collide_push_tiled(LevelArgs<S> a, 
                 R g[Q];
 #pragma unroll
                 for (int q = 0; q < Q; ++q) g[q] = R(Store<S>::load(a.A + (long long)q * a.N + n, scaleOf(a, q)));
-                uint32_t mask;
                 if (code == CODE_FLUID) {
                     // fluid nodes are interior or on periodic axes: every axis neighbour exists
                     const int sc = allResident ? z : key(z);
                     const int sp = allResident ? wrapm(z + 1, a.nz, 1) : key(z + 1);
                     const int sn = allResident ? wrapm(z - 1, a.nz, 1) : key(z - 1);
-                    MomR<R> nb[6];
-                    nb[0] = sm[sc][ty + 1][tx + 2];
-                    nb[1] = sm[sc][ty + 1][tx];
-                    nb[2] = sm[sc][ty + 2][tx + 1];
-                    nb[3] = sm[sc][ty][tx + 1];
-                    nb[4] = sm[sp][ty + 1][tx + 1];
-                    nb[5] = sm[sn][ty + 1][tx + 1];
-                    Collider<R, OP, ORDER, CUBIC, false>::run(g, a, nb);
-                    mask = 0x3FFFFu;
+                    R SG[12];
+                    neighbourTerms<R, OP == OP_HRR, CUBIC>(sm[sc][ty + 1][tx + 2], sm[sc][ty + 1][tx],
+                                                           sm[sc][ty + 2][tx + 1], sm[sc][ty][tx + 1],
+                                                           sm[sp][ty + 1][tx + 1], sm[sn][ty + 1][tx + 1], SG);
+                    Pusher<S> emit{a, n, 0x3FFFFu, nbOffsets(a, i, j, z)};
+                    Collider<R, OP, ORDER, CUBIC, false>::run(g, a, SG, emit);
                 } else {
-                    mask = c_pushMask[code];
+                    Pusher<S> emit{a, n, c_pushMask[code], nbOffsets(a, i, j, z)};
+#pragma unroll
+                    for (int q = 0; q < Q; ++q) emit(q, g[q]);
                 }
-                pushNode<S, R>(a, g, n, mask, nbOffsets(a, i, j, z));
             }
         }
         __syncthreads();  // the slot of z-1 is refilled with z+2 next
