@@ -300,25 +300,6 @@ CollideFn<S> pickCollide(const acp_case_desc& d) {
 
 template <typename S>
 using TiledFn = void (*)(LevelArgs<S>, int);
-template <typename S>
-using ResidentFn = void (*)(LevelArgs<S>);
-
-template <typename S, typename R>
-ResidentFn<S> pickResident(const acp_case_desc& d) {
-    const bool cubic = d.cubic_mach != 0;
-    if (d.op == OP_RR) {
-        switch (d.eq_order) {
-            case 2: return k_collide_push_resident<S, R, OP_RR, 2, true>;
-            case 3: return k_collide_push_resident<S, R, OP_RR, 3, true>;
-            default: return k_collide_push_resident<S, R, OP_RR, 4, true>;
-        }
-    }
-    switch (d.eq_order) {
-        case 2: return cubic ? k_collide_push_resident<S, R, OP_HRR, 2, true> : k_collide_push_resident<S, R, OP_HRR, 2, false>;
-        case 3: return cubic ? k_collide_push_resident<S, R, OP_HRR, 3, true> : k_collide_push_resident<S, R, OP_HRR, 3, false>;
-        default: return cubic ? k_collide_push_resident<S, R, OP_HRR, 4, true> : k_collide_push_resident<S, R, OP_HRR, 4, false>;
-    }
-}
 
 template <typename S, typename R>
 TiledFn<S> pickTiled(const acp_case_desc& d) {
@@ -375,17 +356,13 @@ int enqueueLevelStep(acp_handle* h, int l, int src, PhaseTimer* tm = nullptr) {
     if (needsMoments(h->d)) {
         // z-marching tiles; a periodic z axis of <= 3 planes is resident at once
         const int bxy = ((L.nx + TX - 1) / TX) * ((L.ny + TY - 1) / TY);
-        if (h->d.bc[2] == ACP_BC_PERIODIC && L.nz <= 3) {
-            const size_t dyn = (size_t)L.nz * Q * TX * TY * sizeof(R);
-            ResidentFn<S> fn = pickResident<S, R>(h->d);
-            cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
-            fn<<<dim3((L.nx + TX - 1) / TX, (L.ny + TY - 1) / TY, 1), dim3(TX, TY), dyn, h->stream>>>(a);
-        } else {
+        int chunk = L.nz;
+        if (!(h->d.bc[2] == ACP_BC_PERIODIC && L.nz <= 3)) {
             const int want = (4 * 148 + bxy - 1) / bxy;  // z chunks for >= 4 blocks per SM
-            const int chunk = std::max(8, (L.nz + want - 1) / want);
-            dim3 grid((L.nx + TX - 1) / TX, (L.ny + TY - 1) / TY, (L.nz + chunk - 1) / chunk);
-            pickTiled<S, R>(h->d)<<<grid, dim3(TX, TY), 0, h->stream>>>(a, chunk);
+            chunk = std::max(8, (L.nz + want - 1) / want);
         }
+        dim3 grid((L.nx + TX - 1) / TX, (L.ny + TY - 1) / TY, (L.nz + chunk - 1) / chunk);
+        pickTiled<S, R>(h->d)<<<grid, dim3(TX, TY), 0, h->stream>>>(a, chunk);
     } else {
         pickCollide<S, R>(h->d)<<<gridOf(L, bx), bx, 0, h->stream>>>(a);
     }

@@ -347,39 +347,15 @@ __device__ __forceinline__ MomR<R> nodeMoments(const LevelArgs<S>& a, int n) {
 }
 
 template <typename S, typename R>
-__device__ __forceinline__ void loadPlaneMoments(const LevelArgs<S>& a, MomR<R> (*slot)[TX + 2], int x0, int y0, int z,
-                                                 R* stage = nullptr) {
+__device__ __forceinline__ void loadPlaneMoments(const LevelArgs<S>& a, MomR<R> (*slot)[TX + 2], int x0, int y0, int z) {
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
     // own node (on a periodic axis a thread past the end holds the wrapped
-    // node, which is the neighbour of the last node of a partial tile); with
-    // `stage` the populations are also kept in shared memory, [q][tid]
+    // node, which is the neighbour of the last node of a partial tile)
     {
         const int i = wrapm(x0 + tx, a.nx, a.per[0]), j = wrapm(y0 + ty, a.ny, a.per[1]);
         if (i >= 0 && j >= 0) {
             const int n = (z * a.ny + j) * a.nx + i;
-            if (a.code[n] != CODE_DEAD) {
-                if (stage) {
-                    R d = 0, jx = 0, jy = 0, jz = 0;
-#pragma unroll
-                    for (int q = 0; q < Q; ++q) {
-                        const R g = R(Store<S>::load(a.A + (long long)q * a.N + n, scaleOf(a, q)));
-                        stage[q * TX * TY + tid] = g;
-                        d += g;
-                        jx += R(ex(q)) * g;
-                        jy += R(ey(q)) * g;
-                        jz += R(ez(q)) * g;
-                    }
-                    MomR<R> m;
-                    m.rho = R(a.shift) + d;
-                    const R inv = R(1) / m.rho;
-                    m.ux = jx * inv;
-                    m.uy = jy * inv;
-                    m.uz = jz * inv;
-                    slot[ty + 1][tx + 1] = m;
-                } else {
-                    slot[ty + 1][tx + 1] = nodeMoments<S, R>(a, n);
-                }
-            }
+            if (a.code[n] != CODE_DEAD) slot[ty + 1][tx + 1] = nodeMoments<S, R>(a, n);
         }
     }
     // one-node ring (axis neighbours only): bottom row, top row, left column, right column
@@ -443,62 +419,22 @@ __device__ __forceinline__ void neighbourTerms(const MomR<R>& mxp, const MomR<R>
     }
 }
 
-// register cap: 2 blocks per SM for FP64 compute, 3 for FP32
+// Register cap of the tiled kernel: blocks of 256 threads per SM for FP64 /
+// FP32 compute.  Measured on the 1024x512x3 HRR pulse, this per-plane form
+// (moments of planes z-1..z+1 in shared memory, own populations re-read from
+// L2 for the collision) beat both staging every plane's populations in shared
+// memory behind one barrier and a two-plane-deep software pipeline.
+#ifndef ACP_TILED_MINB_F64
+#define ACP_TILED_MINB_F64 2
+#endif
+#ifndef ACP_TILED_MINB_F32
+#define ACP_TILED_MINB_F32 3
+#endif
 template <typename R>
 struct TiledMinBlocks {
-    static constexpr int value = sizeof(R) == 8 ? 2 : 3;
+    static constexpr int value = sizeof(R) == 8 ? ACP_TILED_MINB_F64 : ACP_TILED_MINB_F32;
 };
 
-template <typename S, typename R, int OP, int ORDER, bool CUBIC>
-__device__ __forceinline__ void tiledNode(const LevelArgs<S>& a, const R* gsrc, int gstride, MomR<R> (*sc)[TX + 2],
-                                          MomR<R> (*sp)[TX + 2], MomR<R> (*sn)[TX + 2], int i, int j, int z) {
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    const int n = (z * a.ny + j) * a.nx + i;
-    const uint8_t code = a.code[n];
-    if (code == CODE_DEAD) return;
-    R g[Q];
-    if (gsrc) {
-#pragma unroll
-        for (int q = 0; q < Q; ++q) g[q] = gsrc[q * gstride];
-    } else {
-#pragma unroll
-        for (int q = 0; q < Q; ++q) g[q] = R(Store<S>::load(a.A + (long long)q * a.N + n, scaleOf(a, q)));
-    }
-    if (code == CODE_FLUID) {
-        // fluid nodes are interior or on periodic axes: every axis neighbour exists
-        R SG[12];
-        neighbourTerms<R, OP == OP_HRR, CUBIC>(sc[ty + 1][tx + 2], sc[ty + 1][tx], sc[ty + 2][tx + 1], sc[ty][tx + 1],
-                                               sp[ty + 1][tx + 1], sn[ty + 1][tx + 1], SG);
-        Pusher<S> emit{a, n, 0x3FFFFu, nbOffsets(a, i, j, z)};
-        Collider<R, OP, ORDER, CUBIC, false>::run(g, a, SG, emit);
-    } else {
-        Pusher<S> emit{a, n, c_pushMask[code], nbOffsets(a, i, j, z)};
-#pragma unroll
-        for (int q = 0; q < Q; ++q) emit(q, g[q]);
-    }
-}
-
-// periodic z axis of at most three planes: the moments and the populations
-// of every plane of the tile stay in shared memory, one barrier per block
-template <typename S, typename R, int OP, int ORDER, bool CUBIC>
-__global__ void __launch_bounds__(TX * TY, TiledMinBlocks<R>::value) k_collide_push_resident(LevelArgs<S> a) {
-    __shared__ MomR<R> sm[3][TY + 2][TX + 2];
-    extern __shared__ unsigned char dyn[];
-    R* stage = reinterpret_cast<R*>(dyn);  // [plane][q][TX*TY]
-    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
-    const int i = x0 + tx, j = y0 + ty;
-    for (int z = 0; z < a.nz; ++z) loadPlaneMoments<S, R>(a, sm[z], x0, y0, z, stage + z * Q * TX * TY);
-    __syncthreads();
-    if (i < a.nx && j < a.ny) {
-        for (int z = 0; z < a.nz; ++z)
-            tiledNode<S, R, OP, ORDER, CUBIC>(a, stage + z * Q * TX * TY + tid, TX * TY, sm[z],
-                                              sm[wrapm(z + 1, a.nz, 1)], sm[wrapm(z - 1, a.nz, 1)], i, j, z);
-    }
-}
-
-// general z: a block owns a z chunk of its column and keeps three planes of
-// moments in a ring of shared-memory slots
 template <typename S, typename R, int OP, int ORDER, bool CUBIC>
 __global__ void __launch_bounds__(TX * TY, TiledMinBlocks<R>::value) k_collide_push_tiled(LevelArgs<S> a, int zChunk) {
     __shared__ MomR<R> sm[3][TY + 2][TX + 2];
@@ -507,18 +443,47 @@ __global__ void __launch_bounds__(TX * TY, TiledMinBlocks<R>::value) k_collide_p
     const int i = x0 + tx, j = y0 + ty;
     const int zBeg = blockIdx.z * zChunk;
     const int zEnd = min(a.nz, zBeg + zChunk);
-    // slot of the unwrapped plane u in [zBeg-1, zEnd] is (u - zBeg + 1) mod 3
+    const bool allResident = a.per[2] && a.nz <= 3;
+    // rolling planes: slot of the unwrapped plane u in [zBeg-1, zEnd] is (u - zBeg + 1) mod 3
     auto key = [&](int u) { return (u - zBeg + 1) % 3; };
-    const int zm = wrapc(zBeg - 1, a.nz, a.per[2]);
-    if (zm >= 0) loadPlaneMoments<S, R>(a, sm[key(zBeg - 1)], x0, y0, zm);
-    loadPlaneMoments<S, R>(a, sm[key(zBeg)], x0, y0, zBeg);
+    if (allResident) {
+        for (int z = 0; z < a.nz; ++z) loadPlaneMoments<S, R>(a, sm[z], x0, y0, z);
+    } else {
+        const int zm = wrapc(zBeg - 1, a.nz, a.per[2]);
+        if (zm >= 0) loadPlaneMoments<S, R>(a, sm[key(zBeg - 1)], x0, y0, zm);
+        loadPlaneMoments<S, R>(a, sm[key(zBeg)], x0, y0, zBeg);
+    }
     for (int z = zBeg; z < zEnd; ++z) {
-        const int zp = wrapc(z + 1, a.nz, a.per[2]);
-        if (zp >= 0) loadPlaneMoments<S, R>(a, sm[key(z + 1)], x0, y0, zp);
+        if (!allResident) {
+            const int zp = wrapc(z + 1, a.nz, a.per[2]);
+            if (zp >= 0) loadPlaneMoments<S, R>(a, sm[key(z + 1)], x0, y0, zp);
+        }
         __syncthreads();
-        if (i < a.nx && j < a.ny)
-            tiledNode<S, R, OP, ORDER, CUBIC>(a, (const R*)nullptr, 0, sm[key(z)], sm[key(z + 1)], sm[key(z - 1)], i,
-                                              j, z);
+        if (i < a.nx && j < a.ny) {
+            const int n = (z * a.ny + j) * a.nx + i;
+            const uint8_t code = a.code[n];
+            if (code != CODE_DEAD) {
+                R g[Q];
+#pragma unroll
+                for (int q = 0; q < Q; ++q) g[q] = R(Store<S>::load(a.A + (long long)q * a.N + n, scaleOf(a, q)));
+                if (code == CODE_FLUID) {
+                    // fluid nodes are interior or on periodic axes: every axis neighbour exists
+                    const int sc = allResident ? z : key(z);
+                    const int sp = allResident ? wrapm(z + 1, a.nz, 1) : key(z + 1);
+                    const int sn = allResident ? wrapm(z - 1, a.nz, 1) : key(z - 1);
+                    R SG[12];
+                    neighbourTerms<R, OP == OP_HRR, CUBIC>(sm[sc][ty + 1][tx + 2], sm[sc][ty + 1][tx],
+                                                           sm[sc][ty + 2][tx + 1], sm[sc][ty][tx + 1],
+                                                           sm[sp][ty + 1][tx + 1], sm[sn][ty + 1][tx + 1], SG);
+                    Pusher<S> emit{a, n, 0x3FFFFu, nbOffsets(a, i, j, z)};
+                    Collider<R, OP, ORDER, CUBIC, false>::run(g, a, SG, emit);
+                } else {
+                    Pusher<S> emit{a, n, c_pushMask[code], nbOffsets(a, i, j, z)};
+#pragma unroll
+                    for (int q = 0; q < Q; ++q) emit(q, g[q]);
+                }
+            }
+        }
         __syncthreads();  // the slot of z-1 is refilled with z+2 next
     }
 }
