@@ -24,6 +24,7 @@ struct LevelHost {
     int nx = 0, ny = 0, nz = 0;
     long long N = 0;
     int off[3] = {0, 0, 0};  // box origin in this level's global node index
+    int per[3] = {0, 0, 0};  // periodic axes of this level
     std::vector<uint8_t> code;
     std::vector<BNodeDev> lodiX, lodiZY;
     long long active = 0;
@@ -53,6 +54,13 @@ struct acp_handle {
     cudaStream_t stream = nullptr;
     bool ownStream = false;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};  // one step starting from cur == 0 / cur == 1
+    // two-level coupling (fine state always in array 0 between coarse steps)
+    std::vector<C2FDev> c2fHost;
+    std::vector<F2CDev> f2cHost;
+    int nCoinc = 0, nMid = 0, nCen = 0;
+    C2FDev* dC2F = nullptr;
+    F2CDev* dF2C = nullptr;
+    void* dPre = nullptr;  // coarse populations before the coarse step, [Q][nCoinc]
     int* dErr = nullptr;
     // probes
     long long* dProbeNodes = nullptr;
@@ -128,8 +136,21 @@ int rmRowFull(int m, int q) {
 }
 
 int uploadConstants() {
-    uint32_t masks[27];
-    for (int c = 0; c < 27; ++c) masks[c] = 0;
+    uint32_t masks[54];
+    for (int c = 0; c < 54; ++c) masks[c] = 0;
+    // coupling nodes: every direction except those leaving the level across its box faces
+    for (int c = 0; c < 27; ++c) {
+        const int f[3] = {c / 9 - 1, (c / 3) % 3 - 1, c % 3 - 1};
+        uint32_t m = 0;
+        for (int q = 0; q < 18; ++q) {
+            const int e[3] = {ex(q), ey(q), ez(q)};
+            bool out = false;
+            for (int a = 0; a < 3; ++a)
+                if (f[a] != 0 && e[a] == f[a]) out = true;
+            if (!out) m |= 1u << q;
+        }
+        masks[27 + c] = m;
+    }
     for (const BoundaryClass& b : kBoundaryClasses) {
         uint32_t m = 0;
         for (int k = 0; k < 5 && b.push[k] >= 0; ++k) m |= 1u << b.push[k];
@@ -185,7 +206,276 @@ int validate(const acp_case_desc* d, std::string& why) {
         }
     }
     if (d->max_level != 0 && d->max_level != 1) { why = "MaxLevel must be 0 or 1"; return ACP_ERR_INVALID; }
-    if (d->max_level == 1) { why = "two-level cases are not enabled in this build"; return ACP_ERR_UNSUPPORTED; }
+    if (d->max_level == 1) {
+        if (d->layout != ACP_LAYOUT_BOX) {
+            why = "two-level cases use the box layout (Refinement-Layout BOX)";
+            return ACP_ERR_UNSUPPORTED;
+        }
+        if (d->coupling != ACP_COUPLING_STD || d->overlap != 1) {
+            why = "the direct-coupling schemes (Overlap 0) are not built; use STD with Overlap 1";
+            return ACP_ERR_UNSUPPORTED;
+        }
+        bool spans[3];
+        for (int a = 0; a < 3; ++a) {
+            if (d->box_lo[a] < 0 || d->box_hi[a] >= dims[a] || d->box_lo[a] > d->box_hi[a]) {
+                why = "refined box outside the lattice";
+                return ACP_ERR_INVALID;
+            }
+            spans[a] = d->box_lo[a] == 0 && d->box_hi[a] == dims[a] - 1;
+            if (!(spans[a] && d->bc[a] == ACP_BC_PERIODIC) && d->box_hi[a] - d->box_lo[a] < 4) {
+                why = "the refined box needs at least 4 coarse cells per axis";
+                return ACP_ERR_INVALID;
+            }
+        }
+        for (int a = 0; a < 3; ++a)
+            if (d->bc[a] == ACP_BC_LODI && (d->box_lo[a] == 0 || d->box_hi[a] == dims[a] - 1))
+                for (int b = 0; b < 3; ++b)
+                    if (b != a && !spans[b]) {
+                        // otherwise coupling nodes would sit on LODI faces
+                        why = "a refined box touching a LODI face must span the other two axes";
+                        return ACP_ERR_UNSUPPORTED;
+                    }
+        const long long fine = (2LL * (d->box_hi[0] - d->box_lo[0]) + 2) * (2LL * (d->box_hi[1] - d->box_lo[1]) + 2) *
+                               (2LL * (d->box_hi[2] - d->box_lo[2]) + 2);
+        if (fine > 100000000LL) { why = "more than 1e8 nodes in the fine level"; return ACP_ERR_UNSUPPORTED; }
+    }
+    return ACP_OK;
+}
+
+// LODI wiring and node classes of a level whose dead / coupling nodes are
+// marked in L.code (CODE_DEAD, CODE_IFACE0 + class); the LODI faces are the
+// domain faces the level's box reaches
+int wireLevel(acp_handle* h, LevelHost& L, int level) {
+    const acp_case_desc& d = h->d;
+    const int dims[3] = {L.nx, L.ny, L.nz};
+    const int dom[3] = {d.nx, d.ny, d.nz};
+    int lodiLo[3], lodiHi[3];
+    for (int a = 0; a < 3; ++a) {
+        const bool lodi = d.bc[a] == ACP_BC_LODI;
+        lodiLo[a] = lodi && L.off[a] == 0;
+        lodiHi[a] = lodi && (L.off[a] + dims[a] - 1 == (dom[a] - 1) << level);
+    }
+    auto idx = [&](int i, int j, int k) { return ((long long)k * L.ny + j) * L.nx + i; };
+    auto inRange = [&](int i, int j, int k, long long& out) {
+        int c[3] = {i, j, k};
+        for (int a = 0; a < 3; ++a)
+            if (c[a] < 0 || c[a] >= dims[a]) {
+                if (!L.per[a]) return false;
+                c[a] = (c[a] % dims[a] + dims[a]) % dims[a];
+            }
+        out = idx(c[0], c[1], c[2]);
+        return true;
+    };
+    for (int k = 0; k < L.nz; ++k)
+        for (int j = 0; j < L.ny; ++j)
+            for (int i = 0; i < L.nx; ++i) {
+                const long long n = idx(i, j, k);
+                if (L.code[n] == CODE_DEAD) continue;
+                const int c[3] = {i, j, k};
+                int fc[3];
+                for (int a = 0; a < 3; ++a) fc[a] = (lodiLo[a] && c[a] == 0) ? -1 : ((lodiHi[a] && c[a] == dims[a] - 1) ? 1 : 0);
+                if (!fc[0] && !fc[1] && !fc[2]) continue;
+                if (L.code[n] != CODE_FLUID) return fail(h, ACP_ERR_INVALID, "a coupling node on a LODI face");
+                L.code[n] = (uint8_t)faceCode(fc[0], fc[1], fc[2]);
+                const BoundaryClass* bc = boundaryClass(fc[0], fc[1], fc[2]);
+                BNodeDev b;
+                b.n = n;
+                b.normalDir = bc->normalDir;
+                if (!inRange(i + bc->n1[0], j + bc->n1[1], k + bc->n1[2], b.n1) ||
+                    !inRange(i + bc->n2[0], j + bc->n2[1], k + bc->n2[2], b.n2))
+                    return fail(h, ACP_ERR_INVALID, "normal neighbour outside the lattice");
+                for (int m = 0; m < 4; ++m) b.t[m] = -1;
+                b.transverse = 0;
+                if ((fc[0] != 0) + (fc[1] != 0) + (fc[2] != 0) == 1) {
+                    int t[4][3];
+                    faceTangents(fc[0], fc[1], fc[2], t);
+                    for (int m = 0; m < 4; ++m)
+                        if (!inRange(i + t[m][0], j + t[m][1], k + t[m][2], b.t[m]))
+                            return fail(h, ACP_ERR_INVALID, "tangent neighbour outside the lattice");
+                    b.transverse = d.transverse ? 1 : 0;
+                }
+                (fc[0] != 0 ? L.lodiX : L.lodiZY).push_back(b);
+            }
+    L.active = 0;
+    for (long long n = 0; n < L.N; ++n) L.active += L.code[n] != CODE_DEAD;
+    L.spacing = d.spacing / std::pow(2.0, (double)level);
+    L.dt = d.spacing / (d.speed_of_sound * std::sqrt(3.0)) / std::pow(2.0, (double)level);
+    const double cs2 = d.speed_of_sound * d.speed_of_sound;
+    L.omega = (cs2 * L.dt) / (d.kinematic_viscosity + 0.5 * cs2 * L.dt);
+    return ACP_OK;
+}
+
+// replaced populations of a coupling node on faces f (outward normals):
+// all, the missing ones (arriving across a face), or missing and in-plane
+uint32_t replaceMask(int mode, const int* f) {
+    uint32_t m = 0;
+    for (int q = 0; q < Q; ++q) {
+        const int e[3] = {ex(q), ey(q), ez(q)};
+        bool missing = false, inplane = false;
+        for (int a = 0; a < 3; ++a)
+            if (f[a] != 0) {
+                if (e[a] == -f[a]) missing = true;
+                if (e[a] == 0) inplane = true;
+            }
+        if (mode == 2 || missing || (mode == 1 && inplane)) m |= 1u << q;
+    }
+    return m;
+}
+
+// two levels, box layout: the coarse level covers the domain with the box
+// interior (beyond the one-cell overlap) dead, the fine level covers the box
+int buildTwoLevel(acp_handle* h) {
+    const acp_case_desc& d = h->d;
+    const int dom[3] = {d.nx, d.ny, d.nz};
+    int lo[3], hi[3], loIf[3], hiIf[3], spans[3];
+    for (int a = 0; a < 3; ++a) {
+        lo[a] = d.box_lo[a];
+        hi[a] = d.box_hi[a];
+        spans[a] = lo[a] == 0 && hi[a] == dom[a] - 1;
+        const bool lodi = d.bc[a] == ACP_BC_LODI;
+        loIf[a] = !spans[a] && !(lo[a] == 0 && lodi);
+        hiIf[a] = !spans[a] && !(hi[a] == dom[a] - 1 && lodi);
+    }
+    // coarse
+    LevelHost C;
+    C.nx = d.nx; C.ny = d.ny; C.nz = d.nz;
+    C.N = (long long)C.nx * C.ny * C.nz;
+    for (int a = 0; a < 3; ++a) C.per[a] = d.bc[a] == ACP_BC_PERIODIC;
+    C.code.assign(C.N, CODE_FLUID);
+    for (int k = 0; k < C.nz; ++k)
+        for (int j = 0; j < C.ny; ++j)
+            for (int i = 0; i < C.nx; ++i) {
+                const int c[3] = {i, j, k};
+                bool dead = true, inner = true;
+                for (int a = 0; a < 3; ++a) {
+                    const int dlo = loIf[a] ? lo[a] + 2 : lo[a], dhi = hiIf[a] ? hi[a] - 2 : hi[a];
+                    const int ilo = loIf[a] ? lo[a] + 1 : lo[a], ihi = hiIf[a] ? hi[a] - 1 : hi[a];
+                    if (c[a] < dlo || c[a] > dhi) dead = false;
+                    if (c[a] < ilo || c[a] > ihi) inner = false;
+                }
+                const long long n = ((long long)k * C.ny + j) * C.nx + i;
+                if (dead) C.code[n] = CODE_DEAD;
+                else if (inner) C.code[n] = CODE_IFACE0 + CODE_FLUID;  // pushes everywhere (into dead nodes too)
+            }
+    int s = wireLevel(h, C, 0);
+    if (s) return s;
+    // fine
+    LevelHost F;
+    int fd[3];
+    for (int a = 0; a < 3; ++a) {
+        F.per[a] = spans[a] && d.bc[a] == ACP_BC_PERIODIC;
+        fd[a] = F.per[a] ? 2 * dom[a] : 2 * (hi[a] - lo[a]) + 1;
+        F.off[a] = 2 * lo[a];
+    }
+    F.nx = fd[0]; F.ny = fd[1]; F.nz = fd[2];
+    F.N = (long long)F.nx * F.ny * F.nz;
+    F.code.assign(F.N, CODE_FLUID);
+    auto fidx = [&](int i, int j, int k) { return ((long long)k * F.ny + j) * F.nx + i; };
+    for (int k = 0; k < F.nz; ++k)
+        for (int j = 0; j < F.ny; ++j)
+            for (int i = 0; i < F.nx; ++i) {
+                const int c[3] = {i, j, k};
+                int f[3];
+                bool iface = false;
+                for (int a = 0; a < 3; ++a) {
+                    f[a] = (loIf[a] && c[a] == 0) ? -1 : ((hiIf[a] && c[a] == fd[a] - 1) ? 1 : 0);
+                    iface = iface || f[a] != 0;
+                }
+                if (iface) F.code[fidx(i, j, k)] = (uint8_t)(CODE_IFACE0 + faceCode(f[0], f[1], f[2]));
+            }
+    if ((s = wireLevel(h, F, 1))) return s;
+    // coupling lists
+    auto fineLocal = [&](const int* g, int& out) {
+        int c[3];
+        for (int a = 0; a < 3; ++a) {
+            c[a] = g[a] - F.off[a];
+            if (F.per[a]) c[a] = (c[a] % fd[a] + fd[a]) % fd[a];
+            if (c[a] < 0 || c[a] >= fd[a]) return false;
+        }
+        out = (int)fidx(c[0], c[1], c[2]);
+        return true;
+    };
+    std::vector<C2FDev> coinc, mid, cen;
+    for (int k = 0; k < F.nz; ++k)
+        for (int j = 0; j < F.ny; ++j)
+            for (int i = 0; i < F.nx; ++i) {
+                const long long n = fidx(i, j, k);
+                if (F.code[n] < CODE_IFACE0 || F.code[n] == CODE_DEAD) continue;
+                const int c[3] = {i, j, k};
+                int g[3], f[3], odd[3], nodd = 0;
+                for (int a = 0; a < 3; ++a) {
+                    g[a] = c[a] + F.off[a];
+                    f[a] = (loIf[a] && c[a] == 0) ? -1 : ((hiIf[a] && c[a] == fd[a] - 1) ? 1 : 0);
+                    odd[a] = g[a] & 1;
+                    nodd += odd[a];
+                }
+                C2FDev cn;
+                cn.n = (int)n;
+                cn.src = -1;
+                cn.mask = replaceMask(d.c2f_replace, f);
+                for (int m = 0; m < 4; ++m) { cn.st[m] = -1; cn.w[m] = 0.f; }
+                if (nodd == 0) {
+                    int cc[3];
+                    for (int a = 0; a < 3; ++a) cc[a] = ((g[a] / 2) % dom[a] + dom[a]) % dom[a];
+                    cn.src = (int)(((long long)cc[2] * C.ny + cc[1]) * C.nx + cc[0]);
+                    coinc.push_back(cn);
+                    continue;
+                }
+                int ax = 0;
+                for (int a = 2; a >= 0; --a)
+                    if (odd[a]) { ax = a; break; }
+                const int off[4] = {-3, -1, 1, 3};
+                int pts[4];
+                bool ok[4];
+                for (int m = 0; m < 4; ++m) {
+                    int gg[3] = {g[0], g[1], g[2]};
+                    gg[ax] += off[m];
+                    ok[m] = fineLocal(gg, pts[m]) && F.code[pts[m]] >= CODE_IFACE0 && F.code[pts[m]] != CODE_DEAD;
+                }
+                if (!ok[1] || !ok[2]) return fail(h, ACP_ERR_INVALID, "interpolation stencil missing on the interface");
+                if (ok[0] && ok[3]) {
+                    const float w[4] = {-1.f / 16.f, 9.f / 16.f, 9.f / 16.f, -1.f / 16.f};
+                    for (int m = 0; m < 4; ++m) { cn.st[m] = pts[m]; cn.w[m] = w[m]; }
+                } else {
+                    cn.st[0] = pts[1]; cn.w[0] = 0.5f;
+                    cn.st[1] = pts[2]; cn.w[1] = 0.5f;
+                }
+                (nodd == 1 ? mid : cen).push_back(cn);
+            }
+    h->nCoinc = (int)coinc.size();
+    h->nMid = (int)mid.size();
+    h->nCen = (int)cen.size();
+    h->c2fHost.clear();
+    h->c2fHost.insert(h->c2fHost.end(), coinc.begin(), coinc.end());
+    h->c2fHost.insert(h->c2fHost.end(), mid.begin(), mid.end());
+    h->c2fHost.insert(h->c2fHost.end(), cen.begin(), cen.end());
+    h->f2cHost.clear();
+    for (int k = 0; k < C.nz; ++k)
+        for (int j = 0; j < C.ny; ++j)
+            for (int i = 0; i < C.nx; ++i) {
+                const long long n = ((long long)k * C.ny + j) * C.nx + i;
+                if (C.code[n] != CODE_IFACE0 + CODE_FLUID) continue;
+                const int c[3] = {i, j, k};
+                int g[3], f[3];
+                for (int a = 0; a < 3; ++a) {
+                    g[a] = 2 * c[a];
+                    f[a] = (loIf[a] && c[a] == lo[a] + 1) ? 1 : ((hiIf[a] && c[a] == hi[a] - 1) ? -1 : 0);
+                }
+                F2CDev fn;
+                fn.n = (int)n;
+                fn.mask = replaceMask(d.f2c_replace, f);
+                if (!fineLocal(g, fn.partner)) return fail(h, ACP_ERR_INVALID, "fine partner outside the box");
+                int m = 0;
+                for (int dz = -1; dz <= 1; ++dz)
+                    for (int dy = -1; dy <= 1; ++dy)
+                        for (int dx = -1; dx <= 1; ++dx) {
+                            int gg[3] = {g[0] + dx, g[1] + dy, g[2] + dz};
+                            if (!fineLocal(gg, fn.cube[m++])) return fail(h, ACP_ERR_INVALID, "F2C neighbourhood outside the box");
+                        }
+                h->f2cHost.push_back(fn);
+            }
+    h->host.push_back(std::move(C));
+    h->host.push_back(std::move(F));
     return ACP_OK;
 }
 
@@ -238,6 +528,7 @@ int buildSingleLevel(acp_handle* h) {
                 }
                 (fc[0] != 0 ? L.lodiX : L.lodiZY).push_back(b);
             }
+    for (int a = 0; a < 3; ++a) L.per[a] = d.bc[a] == ACP_BC_PERIODIC;
     L.active = L.N;
     L.spacing = d.spacing;
     L.dt = d.spacing / (d.speed_of_sound * std::sqrt(3.0));
@@ -254,7 +545,7 @@ LevelArgs<S> levelArgs(acp_handle* h, int l, int src) {
     LevelArgs<S> a;
     a.nx = L.nx; a.ny = L.ny; a.nz = L.nz;
     a.N = L.N;
-    for (int ax = 0; ax < 3; ++ax) a.per[ax] = h->d.bc[ax] == ACP_BC_PERIODIC;
+    for (int ax = 0; ax < 3; ++ax) a.per[ax] = L.per[ax];
     a.A = (const S*)D.f[src];
     a.B = (S*)D.f[1 - src];
     a.code = D.code;
@@ -357,7 +648,7 @@ int enqueueLevelStep(acp_handle* h, int l, int src, PhaseTimer* tm = nullptr) {
         // z-marching tiles; a periodic z axis of <= 3 planes is resident at once
         const int bxy = ((L.nx + TX - 1) / TX) * ((L.ny + TY - 1) / TY);
         int chunk = L.nz;
-        if (!(h->d.bc[2] == ACP_BC_PERIODIC && L.nz <= 3)) {
+        if (!(L.per[2] && L.nz <= 3)) {
             const int want = (4 * 148 + bxy - 1) / bxy;  // z chunks for >= 4 blocks per SM
             chunk = std::max(8, (L.nz + want - 1) / want);
         }
@@ -387,8 +678,85 @@ int enqueueLevelStep(acp_handle* h, int l, int src, PhaseTimer* tm = nullptr) {
     if (D.nLodiX) lf<<<(D.nLodiX + 127) / 128, 128, 0, h->stream>>>(a.A, a.B, D.lodiX, D.nLodiX, p, a);
     if (D.nLodiZY) lf<<<(D.nLodiZY + 127) / 128, 128, 0, h->stream>>>(a.A, a.B, D.lodiZY, D.nLodiZY, p, a);
     if (tm && (D.nLodiX || D.nLodiZY)) tm->mark(ACP_K_LODI);
-    if (h->nProbes && h->probeLevel == l) {
-        k_probes<S><<<1, 128, 0, h->stream>>>(a.B, a, h->dProbeNodes, h->nProbes, h->shift,
+    return ACP_OK;
+}
+
+CouplingArgs couplingArgs(const acp_handle* h) {
+    CouplingArgs c;
+    c.Nc = h->host[0].N;
+    c.Nf = h->host[1].N;
+    c.shiftC = h->shift;
+    c.kappa = h->kappa;
+    c.omegaC = h->host[0].omega;
+    c.omegaF = h->host[1].omega;
+    c.alphaC2F = c.omegaC / (2.0 * c.omegaF);
+    c.alphaF2C = 2.0 * c.omegaF / c.omegaC;
+    c.mrtStyle = h->d.scaling_style == ACP_SCALING_MRT;
+    c.filter = h->d.f2c_filter;
+    return c;
+}
+
+// C2F onto the fine array `fdst` from the coarse array `cnew` (blended with
+// the saved coarse state by weight 1 - th)
+template <typename S, typename R>
+void enqueueC2F(acp_handle* h, int cnew, int fdst, R th) {
+    LevelArgs<S> la = levelArgs<S>(h, 1, 0);
+    const CouplingArgs c = couplingArgs(h);
+    const S* Bc = (const S*)h->dev[0].f[cnew];
+    S* Ff = (S*)h->dev[1].f[fdst];
+    const R* pre = (const R*)h->dPre;
+    const int o = h->d.eq_order;
+    if (h->nCoinc) {
+        const unsigned g = (h->nCoinc + 127) / 128;
+        if (o == 2) k_c2f_coincident<S, R, 2><<<g, 128, 0, h->stream>>>(Bc, Ff, h->dC2F, h->nCoinc, pre, th, c, la);
+        else if (o == 3) k_c2f_coincident<S, R, 3><<<g, 128, 0, h->stream>>>(Bc, Ff, h->dC2F, h->nCoinc, pre, th, c, la);
+        else k_c2f_coincident<S, R, 4><<<g, 128, 0, h->stream>>>(Bc, Ff, h->dC2F, h->nCoinc, pre, th, c, la);
+    }
+    if (h->nMid)
+        k_c2f_interp<S, R><<<(h->nMid + 127) / 128, 128, 0, h->stream>>>(Ff, h->dC2F + h->nCoinc, h->nMid, c, la);
+    if (h->nCen)
+        k_c2f_interp<S, R><<<(h->nCen + 127) / 128, 128, 0, h->stream>>>(Ff, h->dC2F + h->nCoinc + h->nMid, h->nCen, c, la);
+}
+
+// one coarse step: single level, or the two-level sequence of
+// Lattice::nestedTimeStepping* (Lattice.cpp:4354-5771)
+template <typename S, typename R>
+int enqueueStepT(acp_handle* h, int src, PhaseTimer* tm) {
+    if (h->host.size() == 1) {
+        enqueueLevelStep<S, R>(h, 0, src, tm);
+    } else {
+        LevelArgs<S> lc = levelArgs<S>(h, 0, src);
+        const CouplingArgs c = couplingArgs(h);
+        if (tm) tm->mark(-1);
+        if (h->nCoinc)
+            k_c2f_save<S, R><<<(h->nCoinc + 127) / 128, 128, 0, h->stream>>>(lc.A, h->dC2F, h->nCoinc, (R*)h->dPre, lc);
+        if (tm) tm->mark(ACP_K_COUPLING);
+        enqueueLevelStep<S, R>(h, 0, src, tm);  // coarse t -> t+1
+        enqueueLevelStep<S, R>(h, 1, 0, tm);    // fine t -> t+1/2
+        if (tm) tm->mark(-1);
+        enqueueC2F<S, R>(h, 1 - src, 1, R(0.5));  // C2F at t+1/2
+        if (tm) tm->mark(ACP_K_COUPLING);
+        enqueueLevelStep<S, R>(h, 1, 1, tm);    // fine t+1/2 -> t+1
+        if (tm) tm->mark(-1);
+        if (!h->f2cHost.empty()) {
+            LevelArgs<S> lf = levelArgs<S>(h, 1, 0);
+            const unsigned g = ((unsigned)h->f2cHost.size() + 127) / 128;
+            const S* Ff = (const S*)h->dev[1].f[0];
+            S* Bc = (S*)h->dev[0].f[1 - src];
+            const int n = (int)h->f2cHost.size();
+            const int o = h->d.eq_order;
+            if (o == 2) k_f2c<S, R, 2><<<g, 128, 0, h->stream>>>(Ff, Bc, h->dF2C, n, c, lf);
+            else if (o == 3) k_f2c<S, R, 3><<<g, 128, 0, h->stream>>>(Ff, Bc, h->dF2C, n, c, lf);
+            else k_f2c<S, R, 4><<<g, 128, 0, h->stream>>>(Ff, Bc, h->dF2C, n, c, lf);
+        }
+        enqueueC2F<S, R>(h, 1 - src, 0, R(1.0));  // C2F at t+1
+        if (tm) tm->mark(ACP_K_COUPLING);
+    }
+    if (h->nProbes) {
+        const int l = h->probeLevel;
+        LevelArgs<S> a = levelArgs<S>(h, l, 0);
+        const S* cur = (const S*)h->dev[l].f[l == 0 ? 1 - src : 0];
+        k_probes<S><<<1, 128, 0, h->stream>>>(cur, a, h->dProbeNodes, h->nProbes, h->shift,
                                              h->d.speed_of_sound * h->d.speed_of_sound, h->dSeries, h->dCounter,
                                              h->probeCapacity);
         if (tm) tm->mark(ACP_K_PROBES);
@@ -398,19 +766,23 @@ int enqueueLevelStep(acp_handle* h, int l, int src, PhaseTimer* tm = nullptr) {
 
 int enqueueStep(acp_handle* h, int src, PhaseTimer* tm = nullptr) {
     switch (h->d.storage) {
-        case ACP_STORE_F64: return enqueueLevelStep<double, double>(h, 0, src, tm);
-        case ACP_STORE_F32_DEV: return enqueueLevelStep<float, float>(h, 0, src, tm);
-        default: return enqueueLevelStep<__half, float>(h, 0, src, tm);
+        case ACP_STORE_F64: return enqueueStepT<double, double>(h, src, tm);
+        case ACP_STORE_F32_DEV: return enqueueStepT<float, float>(h, src, tm);
+        default: return enqueueStepT<__half, float>(h, src, tm);
     }
 }
 
 int launchesPerStep(const acp_handle* h) {
     int n = 0;
     for (size_t l = 0; l < h->host.size(); ++l) {
-        n += 1;
-        n += (h->dev[l].nLodiX ? 1 : 0) + (h->dev[l].nLodiZY ? 1 : 0);
-        if (h->nProbes && h->probeLevel == (int)l) ++n;
+        const int per = 1 + (h->dev[l].nLodiX ? 1 : 0) + (h->dev[l].nLodiZY ? 1 : 0);
+        n += l == 0 ? per : 2 * per;  // the fine level takes two sub-steps
     }
+    if (h->host.size() == 2) {
+        const int c2f = (h->nCoinc ? 1 : 0) + (h->nMid ? 1 : 0) + (h->nCen ? 1 : 0);
+        n += (h->nCoinc ? 1 : 0) + 2 * c2f + (h->f2cHost.empty() ? 0 : 1);
+    }
+    if (h->nProbes) ++n;
     return n;
 }
 
@@ -480,11 +852,25 @@ int devAlloc(acp_handle* h, void** p, size_t bytes) {
 }
 
 size_t estimateBytes(const acp_case_desc& d) {
-    const long long N = (long long)d.nx * d.ny * d.nz;
-    size_t b = (size_t)N * (2 * Q * storageBytes(d.storage) + 1);
+    const size_t per = 2 * Q * storageBytes(d.storage) + 1;  // two population arrays and the node class
+    long long nodes = (long long)d.nx * d.ny * d.nz;
     long long surf = 2LL * ((long long)d.nx * d.ny + (long long)d.ny * d.nz + (long long)d.nx * d.nz);
-    b += (size_t)surf * sizeof(BNodeDev);
-    return b;
+    if (d.max_level == 1) {
+        const int dom[3] = {d.nx, d.ny, d.nz};
+        long long f[3];
+        for (int a = 0; a < 3; ++a) {
+            const bool spans = d.box_lo[a] == 0 && d.box_hi[a] == dom[a] - 1;
+            f[a] = spans && d.bc[a] == ACP_BC_PERIODIC ? 2LL * dom[a] : 2LL * (d.box_hi[a] - d.box_lo[a]) + 1;
+        }
+        nodes += f[0] * f[1] * f[2];
+        const long long fsurf = 2 * (f[0] * f[1] + f[1] * f[2] + f[0] * f[2]);
+        surf += fsurf;
+        // coupling lists and the saved coarse populations
+        const size_t rb = d.storage == ACP_STORE_F64 ? 8 : 4;
+        return (size_t)nodes * per + (size_t)surf * sizeof(BNodeDev) +
+               (size_t)fsurf * (sizeof(C2FDev) + sizeof(F2CDev) / 4 + Q * rb);
+    }
+    return (size_t)nodes * per + (size_t)surf * sizeof(BNodeDev);
 }
 
 }  // namespace
@@ -555,7 +941,7 @@ int acp_create(const acp_case_desc* d, int device, acp_handle** out) {
             h->hscale[q] = (float)std::ldexp(1.0, (int)std::ceil(std::log2(mag)) - 14);
         }
     }
-    s = buildSingleLevel(h);
+    s = d->max_level == 1 ? buildTwoLevel(h) : buildSingleLevel(h);
     if (s) return s;
     CU(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     h->ownStream = true;
@@ -580,6 +966,20 @@ int acp_create(const acp_case_desc* d, int device, acp_handle** out) {
         if (D.nLodiZY) {
             if ((s = devAlloc(h, (void**)&D.lodiZY, L.lodiZY.size() * sizeof(BNodeDev)))) return s;
             CU(h, cudaMemcpyAsync(D.lodiZY, L.lodiZY.data(), L.lodiZY.size() * sizeof(BNodeDev),
+                                  cudaMemcpyHostToDevice, h->stream));
+        }
+    }
+    if (h->host.size() == 2) {
+        const size_t rb = d->storage == ACP_STORE_F64 ? sizeof(double) : sizeof(float);
+        if (!h->c2fHost.empty()) {
+            if ((s = devAlloc(h, (void**)&h->dC2F, h->c2fHost.size() * sizeof(C2FDev)))) return s;
+            CU(h, cudaMemcpyAsync(h->dC2F, h->c2fHost.data(), h->c2fHost.size() * sizeof(C2FDev),
+                                  cudaMemcpyHostToDevice, h->stream));
+        }
+        if (h->nCoinc && (s = devAlloc(h, &h->dPre, (size_t)h->nCoinc * Q * rb))) return s;
+        if (!h->f2cHost.empty()) {
+            if ((s = devAlloc(h, (void**)&h->dF2C, h->f2cHost.size() * sizeof(F2CDev)))) return s;
+            CU(h, cudaMemcpyAsync(h->dF2C, h->f2cHost.data(), h->f2cHost.size() * sizeof(F2CDev),
                                   cudaMemcpyHostToDevice, h->stream));
         }
     }
@@ -651,9 +1051,9 @@ int acp_read_populations(acp_handle* h, int level, double* out) {
     double* tmp = nullptr;
     CU(h, cudaMallocAsync((void**)&tmp, (size_t)L.N * Q * sizeof(double), h->stream));
     switch (h->d.storage) {
-        case ACP_STORE_F64: launchToF64<double>(h, level, h->cur, tmp); break;
-        case ACP_STORE_F32_DEV: launchToF64<float>(h, level, h->cur, tmp); break;
-        default: launchToF64<__half>(h, level, h->cur, tmp); break;
+        case ACP_STORE_F64: launchToF64<double>(h, level, level == 0 ? h->cur : 0, tmp); break;
+        case ACP_STORE_F32_DEV: launchToF64<float>(h, level, level == 0 ? h->cur : 0, tmp); break;
+        default: launchToF64<__half>(h, level, level == 0 ? h->cur : 0, tmp); break;
     }
     cudaError_t e = cudaMemcpyAsync(out, tmp, (size_t)L.N * Q * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
     cudaFreeAsync(tmp, h->stream);
@@ -867,6 +1267,9 @@ int acp_destroy(acp_handle* h) {
         cudaFree(D.lodiZY);
     }
     cudaFree(h->dErr);
+    cudaFree(h->dC2F);
+    cudaFree(h->dF2C);
+    cudaFree(h->dPre);
     cudaFree(h->dProbeNodes);
     cudaFree(h->dSeries);
     cudaFree(h->dCounter);

@@ -20,11 +20,18 @@
 
 namespace acp {
 
-constexpr uint8_t CODE_FLUID = 13;  // face class (0,0,0)
+// node classes: 0..26 LODI boundary node of face class
+// (fx+1)*9+(fy+1)*3+(fz+1) (13 = none: fluid); 27 + c a coupling node (fine
+// C2F target on the box faces of class c, or coarse F2C target with c = 13),
+// which collides like fluid but pushes only inside its level; 255 covered by
+// the other level
+constexpr uint8_t CODE_FLUID = 13;
+constexpr uint8_t CODE_IFACE0 = 27;
 constexpr uint8_t CODE_DEAD = 255;
+__host__ __device__ constexpr bool collides(uint8_t c) { return c == CODE_FLUID || (c >= CODE_IFACE0 && c < CODE_IFACE0 + 27); }
 
-// pushed-direction mask of each boundary face class (fx+1)*9+(fy+1)*3+(fz+1)
-__constant__ uint32_t c_pushMask[27];
+// pushed-direction mask of each node class
+__constant__ uint32_t c_pushMask[54];
 // MRT bases: inverse of the Gram-Schmidt basis, the basis applied to w_q, and
 // the raw-moment back-transform columns of the five relaxed moments
 __constant__ double c_gsMinv[Q][Q];
@@ -90,6 +97,10 @@ struct RT<float> {
 
 template <typename R, int OP, int ORDER, bool CUBIC, bool MRTWB>
 struct Collider {
+    // nb: strain S and cubic-Mach gradient G of the node (12 values), or null
+    // for a coupling node, whose neighbours are not all on its level: there the
+    // hybrid operator falls back to the population-based Pi1 (sigma = 1) and
+    // the cubic-Mach correction is dropped
     template <typename ST, typename Emit>
     __device__ __forceinline__ static void run(R* g, const LevelArgs<ST>& a, const R* nb, Emit& emit) {
         if ((OP == OP_MRT_GS || OP == OP_MRT_RM) && !MRTWB) {
@@ -207,7 +218,7 @@ struct Collider {
         // RR / HRR: strain rate S and cubic-Mach gradient G from the six axis neighbours
         R S[6] = {0, 0, 0, 0, 0, 0};
         R G[6] = {0, 0, 0, 0, 0, 0};
-        if (OP == OP_HRR || CUBIC) {
+        if ((OP == OP_HRR || CUBIC) && nb) {
 #pragma unroll
             for (int c = 0; c < 6; ++c) {
                 S[c] = nb[c];
@@ -230,7 +241,7 @@ struct Collider {
         }
         R A2[6];
         if (OP == OP_HRR) {
-            const R sg = R(a.sigma);
+            const R sg = nb ? R(a.sigma) : R(1);
             const R fd = (R(1) - sg) * (R(-2) * rho / (R(3) * omega));
 #pragma unroll
             for (int c = 0; c < 6; ++c) A2[c] = sg * P[c] + fd * S[c];
@@ -306,8 +317,8 @@ __global__ void __launch_bounds__(128) k_collide_push(LevelArgs<S> a) {
     R g[Q];
 #pragma unroll
     for (int q = 0; q < Q; ++q) g[q] = R(Store<S>::load(a.A + (long long)q * a.N + n, scaleOf(a, q)));
-    if (code == CODE_FLUID) {
-        Pusher<S> emit{a, n, 0x3FFFFu, nbOffsets(a, i, j, k)};
+    if (collides(code)) {
+        Pusher<S> emit{a, n, c_pushMask[code], nbOffsets(a, i, j, k)};
         Collider<R, OP, ORDER, CUBIC, MRTWB>::run(g, a, (const R*)nullptr, emit);
     } else {
         Pusher<S> emit{a, n, c_pushMask[code], nbOffsets(a, i, j, k)};
@@ -466,7 +477,10 @@ __global__ void __launch_bounds__(TX * TY, TiledMinBlocks<R>::value) k_collide_p
                 R g[Q];
 #pragma unroll
                 for (int q = 0; q < Q; ++q) g[q] = R(Store<S>::load(a.A + (long long)q * a.N + n, scaleOf(a, q)));
-                if (code == CODE_FLUID) {
+                if (code >= CODE_IFACE0) {
+                    Pusher<S> emit{a, n, c_pushMask[code], nbOffsets(a, i, j, z)};
+                    Collider<R, OP, ORDER, CUBIC, false>::run(g, a, (const R*)nullptr, emit);
+                } else if (code == CODE_FLUID) {
                     // fluid nodes are interior or on periodic axes: every axis neighbour exists
                     const int sc = allResident ? z : key(z);
                     const int sp = allResident ? wrapm(z + 1, a.nz, 1) : key(z + 1);
@@ -680,6 +694,176 @@ __global__ void k_probes(const S* __restrict__ arr, LevelArgs<S> la, const long 
     }
     __syncthreads();
     if (t == 0) *counter = s + 1;
+}
+
+// ---------------------------------------------------------------------------
+// grid coupling (box layout, overlap of one coarse cell, 2:1 sub-cycling).
+// The reference declares these operators (GridCoupling.h:28-45) but its
+// GridCoupling.cpp is absent; they follow the call order of
+// Lattice::nestedTimeStepping* (Lattice.cpp:4354-5771): C2F at t+1/2 with
+// linear time interpolation of the coarse state and at t+1, spatial
+// interpolation of the fine coupling nodes between coarse positions, F2C of
+// the coarse nodes one cell inside the fine box, non-equilibrium rescaled by
+// the ratio of (relaxation time x time step) of the levels.
+struct C2FDev {
+    int n;           // fine node
+    int src;         // coarse node (coincident) or -1
+    int st[4];       // interpolation stencil (fine nodes) or -1
+    float w[4];
+    uint32_t mask;   // populations replaced
+};
+struct F2CDev {
+    int n;           // coarse node
+    int partner;     // coincident fine node
+    uint32_t mask;
+    int cube[27];    // 3x3x3 fine neighbourhood, x fastest
+};
+struct CouplingArgs {
+    long long Nc, Nf;  // node counts of the coarse and fine arrays
+    double shiftC;     // storage shift (both levels)
+    double kappa;
+    double alphaC2F, alphaF2C;  // population-based rescaling factors
+    double omegaC, omegaF;
+    int mrtStyle;      // Scaling-Style MRTSTYLE
+    int filter;        // F2C-Filter
+};
+
+// equilibrium split of one node's populations (deviation form)
+template <typename R, int ORDER>
+__device__ __forceinline__ void eqSplit(const R* g, R shift, R kappa, R* geq) {
+    R drho = 0, jx = 0, jy = 0, jz = 0;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        drho += g[q];
+        jx += R(ex(q)) * g[q];
+        jy += R(ey(q)) * g[q];
+        jz += R(ez(q)) * g[q];
+    }
+    const R rho = shift + drho;
+    const R inv = R(1) / rho;
+    R u[3] = {jx * inv, jy * inv, jz * inv};
+    EqCoef<R, ORDER> ec;
+    ec.set(u, kappa);
+#pragma unroll
+    for (int q = 0; q < Q; ++q) geq[q] = R(wq(q)) * (drho + rho * ec.poly(q, kappa));
+}
+
+// rescale a non-equilibrium part between levels: population based, or per
+// moment of the Gram-Schmidt basis (factor of the viscous moments from the
+// collision frequencies, 1/2 or 2 for the others)
+template <typename R>
+__device__ __forceinline__ void rescaleNeq(R* neq, const CouplingArgs& c, bool toFine) {
+    if (!c.mrtStyle) {
+        const R a = R(toFine ? c.alphaC2F : c.alphaF2C);
+#pragma unroll
+        for (int q = 0; q < Q; ++q) neq[q] *= a;
+        return;
+    }
+    R m[Q];
+#pragma unroll
+    for (int mm = 0; mm < Q; ++mm) {
+        R s = 0;
+#pragma unroll
+        for (int q = 0; q < Q; ++q)
+            if (gsRow(mm, q) != 0) s += R(gsRow(mm, q)) * neq[q];
+        const bool visc = mm == 1 || mm == 9 || mm == 11 || mm == 13 || mm == 14 || mm == 15;
+        const R f = visc ? R(toFine ? c.alphaC2F : c.alphaF2C) : R(toFine ? 0.5 : 2.0);
+        m[mm] = f * s;
+    }
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        R acc = 0;
+#pragma unroll
+        for (int mm = 0; mm < Q; ++mm) acc += RT<R>::gsMinv(q, mm) * m[mm];
+        neq[q] = acc;
+    }
+}
+
+// populations of the coincident coupling sources before the coarse step
+template <typename S, typename R>
+__global__ void k_c2f_save(const S* __restrict__ Ac, const C2FDev* __restrict__ nodes, int count, R* pre,
+                           LevelArgs<S> la) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    const int src = nodes[t].src;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) pre[(long long)q * count + t] = R(Store<S>::load(Ac + (long long)q * la.N + src, la.hscale[q]));
+}
+
+// C2F on the fine nodes at coarse positions: coarse state at (1-th)*t + th*(t+1)
+template <typename S, typename R, int ORDER>
+__global__ void k_c2f_coincident(const S* __restrict__ Bc, S* Ff, const C2FDev* __restrict__ nodes, int count,
+                                 const R* __restrict__ pre, R th, CouplingArgs c, LevelArgs<S> la) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    const C2FDev nd = nodes[t];
+    R g[Q], geq[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const R now = R(Store<S>::load(Bc + (long long)q * c.Nc + nd.src, la.hscale[q]));
+        g[q] = (R(1) - th) * pre[(long long)q * count + t] + th * now;
+    }
+    eqSplit<R, ORDER>(g, R(c.shiftC), R(c.kappa), geq);
+#pragma unroll
+    for (int q = 0; q < Q; ++q) g[q] -= geq[q];
+    rescaleNeq<R>(g, c, true);
+#pragma unroll
+    for (int q = 0; q < Q; ++q)
+        if (nd.mask >> q & 1u) Store<S>::store(Ff + (long long)q * c.Nf + nd.n, geq[q] + g[q], la.hscale[q]);
+}
+
+// C2F on the other fine coupling nodes: interpolation along the face from
+// the nodes written before (mid nodes from coincident ones, centre nodes from
+// mid nodes)
+template <typename S, typename R>
+__global__ void k_c2f_interp(S* Ff, const C2FDev* __restrict__ nodes, int count, CouplingArgs c, LevelArgs<S> la) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    const C2FDev nd = nodes[t];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        if (!(nd.mask >> q & 1u)) continue;
+        R acc = 0;
+#pragma unroll
+        for (int m = 0; m < 4; ++m)
+            if (nd.st[m] >= 0) acc += R(nd.w[m]) * R(Store<S>::load(Ff + (long long)q * c.Nf + nd.st[m], la.hscale[q]));
+        Store<S>::store(Ff + (long long)q * c.Nf + nd.n, acc, la.hscale[q]);
+    }
+}
+
+// F2C on the coarse nodes one cell inside the fine box
+template <typename S, typename R, int ORDER>
+__global__ void k_f2c(const S* __restrict__ Ff, S* Bc, const F2CDev* __restrict__ nodes, int count, CouplingArgs c,
+                      LevelArgs<S> la) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    const F2CDev& nd = nodes[t];
+    R g[Q], geq[Q], neq[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) g[q] = R(Store<S>::load(Ff + (long long)q * c.Nf + nd.partner, la.hscale[q]));
+    eqSplit<R, ORDER>(g, R(c.shiftC), R(c.kappa), geq);
+    if (c.filter == 0) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) neq[q] = g[q] - geq[q];
+    } else {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) neq[q] = 0;
+        for (int m = 0; m < 27; ++m) {
+            const int dx = m % 3, dy = (m / 3) % 3, dz = m / 9;
+            const R wgt = c.filter == 1 ? R(1.0 / 27.0)
+                                        : R((dx == 1 ? 0.5 : 0.25) * (dy == 1 ? 0.5 : 0.25) * (dz == 1 ? 0.5 : 0.25));
+            R h[Q], heq[Q];
+#pragma unroll
+            for (int q = 0; q < Q; ++q) h[q] = R(Store<S>::load(Ff + (long long)q * c.Nf + nd.cube[m], la.hscale[q]));
+            eqSplit<R, ORDER>(h, R(c.shiftC), R(c.kappa), heq);
+#pragma unroll
+            for (int q = 0; q < Q; ++q) neq[q] += wgt * (h[q] - heq[q]);
+        }
+    }
+    rescaleNeq<R>(neq, c, false);
+#pragma unroll
+    for (int q = 0; q < Q; ++q)
+        if (nd.mask >> q & 1u) Store<S>::store(Bc + (long long)q * c.Nc + nd.n, geq[q] + neq[q], la.hscale[q]);
 }
 
 }  // namespace acp

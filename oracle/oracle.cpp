@@ -27,7 +27,12 @@
 
 namespace orc {
 
-enum NodeType : unsigned char { NT_INTERIOR = 0, NT_BOUNDARY = 1 };
+enum NodeType : unsigned char {
+    NT_INTERIOR = 0,  // fluid, all neighbours on the level
+    NT_BOUNDARY = 1,  // LODI boundary node
+    NT_IFACE = 2,     // fluid coupling node: fine C2F target or coarse F2C target
+    NT_DEAD = 3       // covered by the other level
+};
 
 struct BNode {
     long n;           // node index
@@ -41,6 +46,8 @@ struct BNode {
 struct Level {
     int nx, ny, nz;
     long N;
+    int org[3] = {0, 0, 0};  // global node index (of this level) of local node 0
+    int per[3] = {0, 0, 0};  // periodic axes of this level
     std::vector<double> f[2];  // [N][19] per ping-pong array (Node::distr_)
     std::vector<double> preCol;
     std::vector<double> psi;   // Node::psi_ (cubic-Mach correction, persistent)
@@ -167,10 +174,30 @@ struct Oracle {
     Mat19 gsM, gsMinv, rmM, rmMinv;
     std::string err;
     int threads = 1;
+    // two-level state (box layout)
+    int altf = 1;               // fine array holding the state
+    struct C2FNode {            // fine coupling node
+        long n;                 // fine node
+        int kind;               // 0 coincident, 1 mid, 2 centre
+        long src;               // coincident: coarse node; mid/centre: -
+        long st[4];             // stencil fine nodes (mid/centre), -1 unused
+        double w[4];
+        unsigned mask;          // populations replaced
+    };
+    struct F2CNode {
+        long n;                 // coarse node
+        long partner;           // coincident fine node
+        long cube[27];          // 3x3x3 fine neighbourhood (x fastest)
+        unsigned mask;
+    };
+    std::vector<C2FNode> c2f;   // ordered: coincident, mid, centre
+    std::vector<F2CNode> f2c;
+    std::vector<double> pre;    // coarse populations before the coarse step, per coincident C2F node
+    int boxLo[3], boxHi[3], loIf[3], hiIf[3], spans[3];
 
     bool build() {
         const acp_case_desc& d = desc;
-        if (d.max_level != 0) { err = "oracle: two-level cases are built by the two-level oracle"; return false; }
+        if (d.max_level == 1) return buildTwoLevel();
         k.setup(d.speed_of_sound, d.spacing, d.kinematic_viscosity, d.density, d.mach, d.k1, d.hybrid_sigma, d.eq_order,
                 d.cubic_mach != 0 && (d.op == ACP_OP_RR || d.op == ACP_OP_HRR), d.transverse != 0);
         gsBasis(gsM);
@@ -260,16 +287,17 @@ struct Oracle {
                 for (int j = 0; j < L.ny; ++j)
                     for (int i = 0; i < L.nx; ++i) {
                         double rho;
+                        const int gi = i + L.org[0], gj = j + L.org[1], gk = kk + L.org[2];
                         if (desc.ic == ACP_IC_REFERENCE) {
                             double Rc = 0.06, A = 0.01, xCenter = -8. * Rc;
-                            double xNode = i * sp - desc.domain_size[0] / 2.;
-                            double yNode = j * sp - desc.domain_size[1] / 2.;
+                            double xNode = gi * sp - desc.domain_size[0] / 2.;
+                            double yNode = gj * sp - desc.domain_size[1] / 2.;
                             double xRel = xNode - xCenter;
                             rho = desc.density * (1 + A * std::exp(-(xRel * xRel + yNode * yNode) / (2 * Rc * Rc)));
                         } else {
                             double s = 1. / std::pow(2., (double)l);
-                            double dx = i * s - desc.ic_center[0], dy = j * s - desc.ic_center[1];
-                            double dz = desc.ic_dims == 3 ? kk * s - desc.ic_center[2] : 0.;
+                            double dx = gi * s - desc.ic_center[0], dy = gj * s - desc.ic_center[1];
+                            double dz = desc.ic_dims == 3 ? gk * s - desc.ic_center[2] : 0.;
                             double r2 = dx * dx + dy * dy + dz * dz;
                             rho = desc.density * (1 + desc.ic_eps * std::exp(-std::log(2.) * r2 / (desc.ic_b * desc.ic_b)));
                         }
@@ -285,6 +313,7 @@ struct Oracle {
                     }
         }
         alt = 1;
+        altf = 1;
         steps = 0;
     }
 
@@ -352,8 +381,11 @@ struct Oracle {
             for (int q = 0; q < Q; ++q) f[q] += L.omega * (eq[q] - f[q]);
             return;
         }
-        bool needStrain = (op == ACP_OP_HRR) || k.cubic;
+        const bool iface = L.type[n] == NT_IFACE;
+        bool needStrain = ((op == ACP_OP_HRR) || k.cubic) && !iface;
         double S[6] = {0, 0, 0, 0, 0, 0};
+        if (iface)
+            for (int q = 0; q < Q; ++q) psi[q] = 0.;  // no finite differences across the interface
         if (needStrain) {
             // neighbours' pre-collision moments (calcDensityPreCol/VelocityPreCol)
             double nbRho[6], nbU[6][3], dist[6];
@@ -375,7 +407,7 @@ struct Oracle {
             double kinVisc = k.nu;
             double dynVisc = kinVisc * densH;
             double invPreFactor = -((dt * k.cs2) / (L.omega * kinVisc));
-            double sg = k.sigma, a[6];
+            double sg = iface ? 1. : k.sigma, a[6];  // coupling nodes: recursive regularisation of Pi1
             for (int c = 0; c < 6; ++c) a[c] = sg * P[c] + (1. - sg) * invPreFactor * (2. * dynVisc * S[c]);
             recursiveNeq(k, k.order, a, u, neq);
         }
@@ -449,19 +481,25 @@ struct Oracle {
         for (int q = 0; q < Q; ++q) out[q] = eq[q];
     }
 
-    void stepSingle() {
-        Level& L = lev[0];
-        int a = alt, nw = 1 - alt;
+    // one step of a level reading array `a` (Lattice::timeStepping*, and the
+    // per-level phases of Lattice::nestedTimeStepping*): save pre-collision
+    // populations, collide in place and push, boundary pushes, LODI passes
+    void stepLevel(int l, int a) {
+        Level& L = lev[l];
+        int nw = 1 - a;
         double* A = L.f[a].data();
         double* B = L.f[nw].data();
         std::memcpy(L.preCol.data(), A, sizeof(double) * L.N * Q);
         const long N = L.N;
 #pragma omp parallel for num_threads(threads) schedule(static)
         for (long n = 0; n < N; ++n) {
-            if (L.type[n] != NT_INTERIOR) continue;
+            if (L.type[n] != NT_INTERIOR && L.type[n] != NT_IFACE) continue;
             double* f = &A[n * Q];
             collideNode(L, n, f);
-            for (int q = 0; q < 18; ++q) B[L.nb[n * 18 + q] * Q + q] = f[q];
+            for (int q = 0; q < 18; ++q) {
+                const long t = L.nb[n * 18 + q];
+                if (t >= 0) B[t * Q + q] = f[q];
+            }
             B[n * Q + 18] = f[18];
         }
         for (const BNode& b : L.bnodes) {
@@ -475,9 +513,410 @@ struct Oracle {
             const long nb = (long)L.bnodes.size();
 #pragma omp parallel for num_threads(threads) schedule(static)
             for (long m = 0; m < nb; ++m)
-                if (L.bnodes[m].pass == pass) lodiNode(L, 0, L.bnodes[m], nw);
+                if (L.bnodes[m].pass == pass) lodiNode(L, l, L.bnodes[m], nw);
         }
-        alt = nw;
+    }
+
+    void stepSingle() {
+        stepLevel(0, alt);
+        alt = 1 - alt;
+        ++steps;
+    }
+
+    // ------------------------------------------------------------------
+    // two levels, box layout: the refined box [lo, hi] (coarse nodes) is
+    // covered by the fine level; coarse and fine overlap by one coarse cell
+    // (Overlap 1, the standard scheme).  The fine nodes on the box faces that
+    // are interfaces take their populations from the coarse level (C2F), the
+    // coarse nodes one cell inside the box take theirs from the fine level
+    // (F2C), with the coarse step, two fine sub-steps and the couplings in the
+    // order of Lattice::nestedTimeStepping* (Lattice.cpp:4354-5771).
+    bool buildTwoLevel() {
+        const acp_case_desc& d = desc;
+        k.setup(d.speed_of_sound, d.spacing, d.kinematic_viscosity, d.density, d.mach, d.k1, d.hybrid_sigma, d.eq_order,
+                d.cubic_mach != 0 && (d.op == ACP_OP_RR || d.op == ACP_OP_HRR), d.transverse != 0);
+        gsBasis(gsM);
+        rmBasis(rmM);
+        if (!invert19(gsM, gsMinv) || !invert19(rmM, rmMinv)) { err = "moment basis not invertible"; return false; }
+        if (d.layout != ACP_LAYOUT_BOX) { err = "two-level oracle: box layout only"; return false; }
+        const int dims[3] = {d.nx, d.ny, d.nz};
+        for (int a = 0; a < 3; ++a) {
+            boxLo[a] = d.box_lo[a];
+            boxHi[a] = d.box_hi[a];
+            spans[a] = boxLo[a] == 0 && boxHi[a] == dims[a] - 1;
+            const bool lodi = d.bc[a] == ACP_BC_LODI;
+            loIf[a] = !spans[a] && !(boxLo[a] == 0 && lodi);
+            hiIf[a] = !spans[a] && !(boxHi[a] == dims[a] - 1 && lodi);
+            if (d.bc[a] == ACP_BC_LODI && dims[a] < 4) { err = "LODI axes need at least 4 nodes"; return false; }
+            if (!(spans[a] && d.bc[a] == ACP_BC_PERIODIC) && boxHi[a] - boxLo[a] < 4) { err = "box too thin"; return false; }
+            if (boxLo[a] < 0 || boxHi[a] >= dims[a] || boxLo[a] > boxHi[a]) { err = "box outside the lattice"; return false; }
+        }
+        // a box reaching a LODI face spans the other two axes: no coupling node on a LODI face
+        for (int a = 0; a < 3; ++a)
+            if (d.bc[a] == ACP_BC_LODI && (boxLo[a] == 0 || boxHi[a] == dims[a] - 1))
+                for (int b = 0; b < 3; ++b)
+                    if (b != a && !spans[b]) { err = "a box touching a LODI face must span the other axes"; return false; }
+        lev.resize(2);
+        // ---- coarse level: the whole domain
+        {
+            Level& L = lev[0];
+            L.nx = d.nx; L.ny = d.ny; L.nz = d.nz;
+            for (int a = 0; a < 3; ++a) L.per[a] = d.bc[a] == ACP_BC_PERIODIC;
+            initLevelArrays(L, 0);
+            for (int kk = 0; kk < L.nz; ++kk)
+                for (int j = 0; j < L.ny; ++j)
+                    for (int i = 0; i < L.nx; ++i) {
+                        const int c[3] = {i, j, kk};
+                        bool dead = true, inner = true;
+                        for (int a = 0; a < 3; ++a) {
+                            const int dlo = loIf[a] ? boxLo[a] + 2 : boxLo[a], dhi = hiIf[a] ? boxHi[a] - 2 : boxHi[a];
+                            const int ilo = loIf[a] ? boxLo[a] + 1 : boxLo[a], ihi = hiIf[a] ? boxHi[a] - 1 : boxHi[a];
+                            if (c[a] < dlo || c[a] > dhi) dead = false;
+                            if (c[a] < ilo || c[a] > ihi) inner = false;
+                        }
+                        const long n = L.idx(i, j, kk);
+                        L.type[n] = dead ? NT_DEAD : (inner ? NT_IFACE : NT_INTERIOR);
+                    }
+            if (!wireLevel(L)) return false;
+        }
+        // ---- fine level: the box at twice the resolution
+        {
+            Level& L = lev[1];
+            int fd[3];
+            for (int a = 0; a < 3; ++a) {
+                L.per[a] = spans[a] && d.bc[a] == ACP_BC_PERIODIC;
+                fd[a] = L.per[a] ? 2 * dims[a] : 2 * (boxHi[a] - boxLo[a]) + 1;
+                L.org[a] = 2 * boxLo[a];
+            }
+            L.nx = fd[0]; L.ny = fd[1]; L.nz = fd[2];
+            initLevelArrays(L, 1);
+            for (int kk = 0; kk < L.nz; ++kk)
+                for (int j = 0; j < L.ny; ++j)
+                    for (int i = 0; i < L.nx; ++i) {
+                        const int c[3] = {i, j, kk};
+                        bool iface = false;
+                        for (int a = 0; a < 3; ++a)
+                            if ((loIf[a] && c[a] == 0) || (hiIf[a] && c[a] == fd[a] - 1)) iface = true;
+                        L.type[L.idx(i, j, kk)] = iface ? NT_IFACE : NT_INTERIOR;
+                    }
+            if (!wireLevel(L)) return false;
+        }
+        buildCouplings();
+        return true;
+    }
+
+    void initLevelArrays(Level& L, int l) {
+        L.N = (long)L.nx * L.ny * L.nz;
+        for (int a = 0; a < 2; ++a) L.f[a].assign(L.N * Q, 0.);
+        L.preCol.assign(L.N * Q, 0.);
+        L.psi.assign(L.N * Q, 0.);
+        L.type.assign(L.N, NT_INTERIOR);
+        L.nb.assign(L.N * 18, -1);
+        L.dt = k.dt(l);
+        L.omega = k.omega(l);
+        L.spacing = k.spacing / std::pow(2., (double)l);
+    }
+
+    // push targets and LODI wiring of a level whose node types are set; LODI
+    // faces are the domain faces the level's box reaches
+    bool wireLevel(Level& L) {
+        const int dims[3] = {L.nx, L.ny, L.nz};
+        int lodiLo[3], lodiHi[3];
+        for (int a = 0; a < 3; ++a) {
+            const bool lodi = desc.bc[a] == ACP_BC_LODI;
+            // the level's local index 0 / last lies on a domain face
+            lodiLo[a] = lodi && L.org[a] == 0;
+            const int domTop = (&desc.nx)[a] - 1;
+            const int scale = L.org[a] == 0 && &L == &lev[0] ? 1 : 2;
+            lodiHi[a] = lodi && (&L == &lev[0] ? true : (L.org[a] + dims[a] - 1 == scale * domTop));
+        }
+        auto inRange = [&](int i, int j, int kk, long& out) {
+            int c[3] = {i, j, kk};
+            for (int a = 0; a < 3; ++a)
+                if (c[a] < 0 || c[a] >= dims[a]) {
+                    if (!L.per[a]) return false;
+                    c[a] = (c[a] % dims[a] + dims[a]) % dims[a];
+                }
+            out = L.idx(c[0], c[1], c[2]);
+            return true;
+        };
+        for (int kk = 0; kk < L.nz; ++kk)
+            for (int j = 0; j < L.ny; ++j)
+                for (int i = 0; i < L.nx; ++i) {
+                    const long n = L.idx(i, j, kk);
+                    if (L.type[n] == NT_DEAD) continue;
+                    const int c[3] = {i, j, kk};
+                    int fc[3];
+                    for (int a = 0; a < 3; ++a)
+                        fc[a] = (lodiLo[a] && c[a] == 0) ? -1 : ((lodiHi[a] && c[a] == dims[a] - 1) ? 1 : 0);
+                    if (fc[0] || fc[1] || fc[2]) {
+                        if (L.type[n] == NT_IFACE) { err = "a coupling node on a LODI face"; return false; }
+                        L.type[n] = NT_BOUNDARY;
+                        const BClass* bc = boundaryClass(fc[0], fc[1], fc[2]);
+                        BNode b;
+                        b.n = n;
+                        b.cls = (int)(bc - kBoundaryClasses);
+                        b.corner = bc->corner;
+                        if (!inRange(i + bc->n1[0], j + bc->n1[1], kk + bc->n1[2], b.n1) ||
+                            !inRange(i + bc->n2[0], j + bc->n2[1], kk + bc->n2[2], b.n2)) {
+                            err = "normal neighbour missing"; return false;
+                        }
+                        for (int m = 0; m < 4; ++m) b.t[m] = -1;
+                        if ((fc[0] != 0) + (fc[1] != 0) + (fc[2] != 0) == 1) {
+                            int t[4][3];
+                            faceTangents(fc[0], fc[1], fc[2], t);
+                            for (int m = 0; m < 4; ++m)
+                                if (!inRange(i + t[m][0], j + t[m][1], kk + t[m][2], b.t[m])) { err = "tangent missing"; return false; }
+                        }
+                        for (int m = 0; m < 5 && bc->push[m] >= 0; ++m) {
+                            const int q = bc->push[m];
+                            long t;
+                            if (!inRange(i + EX[q], j + EY[q], kk + EZ[q], t)) { err = "push target missing"; return false; }
+                            L.nb[n * 18 + q] = t;
+                        }
+                        b.pass = fc[0] != 0 ? 0 : (fc[2] != 0 ? 1 : 2);
+                        L.bnodes.push_back(b);
+                        continue;
+                    }
+                    for (int q = 0; q < 18; ++q) {
+                        long t;
+                        if (inRange(i + EX[q], j + EY[q], kk + EZ[q], t)) L.nb[n * 18 + q] = t;
+                        else if (L.type[n] == NT_INTERIOR) { err = "interior neighbour missing"; return false; }
+                    }
+                }
+        return true;
+    }
+
+    // replaced-population masks (Coarse-to-Fine / Fine-to-Coarse keywords,
+    // BoundaryConditions.txt:71-83): all, missing, or missing and in-plane
+    static unsigned replaceMask(int mode, const int* face) {
+        unsigned m = 0;
+        for (int q = 0; q < Q; ++q) {
+            const int e[3] = {EX[q], EY[q], EZ[q]};
+            bool missing = false, inplane = false;
+            for (int a = 0; a < 3; ++a)
+                if (face[a] != 0) {
+                    if (e[a] == -face[a]) missing = true;
+                    if (e[a] == 0) inplane = true;
+                }
+            if (mode == 2 || missing || (mode == 1 && inplane)) m |= 1u << q;
+        }
+        return m;
+    }
+
+    void buildCouplings() {
+        Level& C = lev[0];
+        Level& F = lev[1];
+        const int fd[3] = {F.nx, F.ny, F.nz};
+        auto fineIdx = [&](const int* g, long& out) {  // fine global -> local
+            int c[3];
+            for (int a = 0; a < 3; ++a) {
+                c[a] = g[a] - F.org[a];
+                if (F.per[a]) c[a] = (c[a] % fd[a] + fd[a]) % fd[a];
+                if (c[a] < 0 || c[a] >= fd[a]) return false;
+            }
+            out = F.idx(c[0], c[1], c[2]);
+            return true;
+        };
+        std::vector<C2FNode> coinc, mid, cen;
+        for (int kk = 0; kk < F.nz; ++kk)
+            for (int j = 0; j < F.ny; ++j)
+                for (int i = 0; i < F.nx; ++i) {
+                    const long n = F.idx(i, j, kk);
+                    if (F.type[n] != NT_IFACE) continue;
+                    const int c[3] = {i, j, kk};
+                    int g[3], face[3], odd[3], nodd = 0;
+                    for (int a = 0; a < 3; ++a) {
+                        g[a] = c[a] + F.org[a];
+                        face[a] = (loIf[a] && c[a] == 0) ? -1 : ((hiIf[a] && c[a] == fd[a] - 1) ? 1 : 0);
+                        odd[a] = g[a] & 1;
+                        nodd += odd[a];
+                    }
+                    C2FNode cn;
+                    cn.n = n;
+                    cn.mask = replaceMask(desc.c2f_replace, face);
+                    for (int m = 0; m < 4; ++m) { cn.st[m] = -1; cn.w[m] = 0; }
+                    cn.src = -1;
+                    if (nodd == 0) {
+                        cn.kind = 0;
+                        int cc[3];
+                        for (int a = 0; a < 3; ++a) {
+                            cc[a] = g[a] / 2;
+                            if (C.per[a]) cc[a] = (cc[a] % (&desc.nx)[a] + (&desc.nx)[a]) % (&desc.nx)[a];
+                        }
+                        cn.src = C.idx(cc[0], cc[1], cc[2]);
+                        coinc.push_back(cn);
+                        continue;
+                    }
+                    // interpolation axis: the odd axis (mid) or the higher odd axis (centre)
+                    int ax = -1;
+                    for (int a = 2; a >= 0; --a)
+                        if (odd[a]) { ax = a; break; }
+                    cn.kind = nodd == 1 ? 1 : 2;
+                    long pts[4];
+                    bool ok[4];
+                    const int off[4] = {-3, -1, 1, 3};
+                    for (int m = 0; m < 4; ++m) {
+                        int gg[3] = {g[0], g[1], g[2]};
+                        gg[ax] += off[m];
+                        ok[m] = fineIdx(gg, pts[m]) && F.type[pts[m]] == NT_IFACE;
+                    }
+                    if (ok[0] && ok[3]) {
+                        const double w[4] = {-1. / 16., 9. / 16., 9. / 16., -1. / 16.};
+                        for (int m = 0; m < 4; ++m) { cn.st[m] = pts[m]; cn.w[m] = w[m]; }
+                    } else {
+                        cn.st[0] = pts[1]; cn.w[0] = 0.5;
+                        cn.st[1] = pts[2]; cn.w[1] = 0.5;
+                    }
+                    (nodd == 1 ? mid : cen).push_back(cn);
+                }
+        c2f.clear();
+        c2f.insert(c2f.end(), coinc.begin(), coinc.end());
+        c2f.insert(c2f.end(), mid.begin(), mid.end());
+        c2f.insert(c2f.end(), cen.begin(), cen.end());
+        pre.assign(coinc.size() * Q, 0.);
+        f2c.clear();
+        for (int kk = 0; kk < C.nz; ++kk)
+            for (int j = 0; j < C.ny; ++j)
+                for (int i = 0; i < C.nx; ++i) {
+                    const long n = C.idx(i, j, kk);
+                    if (C.type[n] != NT_IFACE) continue;
+                    F2CNode fn;
+                    fn.n = n;
+                    const int c[3] = {i, j, kk};
+                    int g[3], face[3];
+                    for (int a = 0; a < 3; ++a) {
+                        g[a] = 2 * c[a];
+                        // the coarse coupling node lies one cell inside the box face it faces
+                        face[a] = (loIf[a] && c[a] == boxLo[a] + 1) ? 1 : ((hiIf[a] && c[a] == boxHi[a] - 1) ? -1 : 0);
+                    }
+                    fineIdx(g, fn.partner);
+                    int m = 0;
+                    for (int dz = -1; dz <= 1; ++dz)
+                        for (int dy = -1; dy <= 1; ++dy)
+                            for (int dx = -1; dx <= 1; ++dx) {
+                                int gg[3] = {g[0] + dx, g[1] + dy, g[2] + dz};
+                                fineIdx(gg, fn.cube[m++]);
+                            }
+                    // populations arriving from the dead interior of the box are the missing ones
+                    fn.mask = replaceMask(desc.f2c_replace, face);
+                    f2c.push_back(fn);
+                }
+    }
+
+    // equilibrium of a population array's own moments and the non-equilibrium part
+    void splitEq(const double* f, double* eq, double& rho, double* u, double) {
+        plainMoments(k, f, rho, u);
+        equilibrium(k, k.order, rho, u, eq);
+    }
+
+    // scale the non-equilibrium part between levels: population based
+    // (SRTSTYLE) or moment based in the Gram-Schmidt basis (MRTSTYLE)
+    void rescale(const double* neq, double* out, bool toFine) {
+        const double wc = lev[0].omega, wf = lev[1].omega;
+        if (desc.scaling_style == ACP_SCALING_SRT) {
+            const double a = toFine ? wc / (2. * wf) : 2. * wf / wc;
+            for (int q = 0; q < Q; ++q) out[q] = a * neq[q];
+            return;
+        }
+        double m[Q];
+        for (int r = 0; r < Q; ++r) {
+            m[r] = 0;
+            for (int q = 0; q < Q; ++q) m[r] += gsM.a[r][q] * neq[q];
+            const bool visc = r == 1 || r == 9 || r == 11 || r == 13 || r == 14 || r == 15;
+            const double a = visc ? (toFine ? wc / (2. * wf) : 2. * wf / wc) : (toFine ? 0.5 : 2.0);
+            m[r] *= a;
+        }
+        for (int q = 0; q < Q; ++q) {
+            out[q] = 0;
+            for (int r = 0; r < Q; ++r) out[q] += gsMinv.a[q][r] * m[r];
+        }
+    }
+
+    // C2F: coarse state (blend of `pre` and the coarse array `cnew` with
+    // weight `th` on cnew) onto the fine array `fnew`
+    void coarseToFine(int cnew, int fnew, double th) {
+        Level& C = lev[0];
+        Level& F = lev[1];
+        double* FB = F.f[fnew].data();
+        const double* CB = C.f[cnew].data();
+        long ic = 0;
+        for (const C2FNode& cn : c2f) {
+            double v[Q];
+            if (cn.kind == 0) {
+                double f[Q], eq[Q], rho, u[3], neq[Q], sc[Q];
+                for (int q = 0; q < Q; ++q) f[q] = (1. - th) * pre[ic * Q + q] + th * CB[cn.src * Q + q];
+                ++ic;
+                splitEq(f, eq, rho, u, C.dt);
+                for (int q = 0; q < Q; ++q) neq[q] = f[q] - eq[q];
+                rescale(neq, sc, true);
+                for (int q = 0; q < Q; ++q) v[q] = eq[q] + sc[q];
+            } else {
+                for (int q = 0; q < Q; ++q) {
+                    double acc = 0;
+                    for (int m = 0; m < 4; ++m)
+                        if (cn.st[m] >= 0) acc += cn.w[m] * FB[cn.st[m] * Q + q];
+                    v[q] = acc;
+                }
+            }
+            for (int q = 0; q < Q; ++q)
+                if (cn.mask >> q & 1u) FB[cn.n * Q + q] = v[q];
+        }
+    }
+
+    // F2C: fine state at t+1 onto the coarse coupling nodes (NOFI: the
+    // coincident node; LAG: arithmetic average of the non-equilibria of the
+    // 3x3x3 fine neighbourhood; TOU: the separable (1/4, 1/2, 1/4) filter)
+    void fineToCoarse(int fcur, int cnew) {
+        Level& C = lev[0];
+        Level& F = lev[1];
+        const double* FA = F.f[fcur].data();
+        double* CB = C.f[cnew].data();
+        const double w1[3] = {0.25, 0.5, 0.25};
+#pragma omp parallel for num_threads(threads) schedule(static)
+        for (long t = 0; t < (long)f2c.size(); ++t) {
+            const F2CNode& fn = f2c[t];
+            double eq[Q], rho, u[3], neq[Q];
+            splitEq(&FA[fn.partner * Q], eq, rho, u, F.dt);
+            if (desc.f2c_filter == ACP_F2C_NOFI) {
+                for (int q = 0; q < Q; ++q) neq[q] = FA[fn.partner * Q + q] - eq[q];
+            } else {
+                for (int q = 0; q < Q; ++q) neq[q] = 0.;
+                int m = 0;
+                for (int dz = 0; dz < 3; ++dz)
+                    for (int dy = 0; dy < 3; ++dy)
+                        for (int dx = 0; dx < 3; ++dx) {
+                            const long nn = fn.cube[m++];
+                            const double w = desc.f2c_filter == ACP_F2C_LAG ? 1. / 27. : w1[dx] * w1[dy] * w1[dz];
+                            double e2[Q], r2, u2[3];
+                            splitEq(&FA[nn * Q], e2, r2, u2, F.dt);
+                            for (int q = 0; q < Q; ++q) neq[q] += w * (FA[nn * Q + q] - e2[q]);
+                        }
+            }
+            double sc[Q];
+            rescale(neq, sc, false);
+            for (int q = 0; q < Q; ++q)
+                if (fn.mask >> q & 1u) CB[fn.n * Q + q] = eq[q] + sc[q];
+        }
+    }
+
+    void stepTwoLevel() {
+        Level& C = lev[0];
+        // coarse populations at t of the coincident coupling sources
+        long ic = 0;
+        for (const C2FNode& cn : c2f)
+            if (cn.kind == 0) {
+                for (int q = 0; q < Q; ++q) pre[ic * Q + q] = C.f[alt][cn.src * Q + q];
+                ++ic;
+            }
+        const int cnew = 1 - alt;
+        stepLevel(0, alt);                 // coarse step t -> t+1
+        stepLevel(1, altf);                // fine sub-step t -> t+1/2
+        coarseToFine(cnew, 1 - altf, 0.5);  // C2F at t+1/2 (linear in time)
+        stepLevel(1, 1 - altf);            // fine sub-step t+1/2 -> t+1
+        fineToCoarse(altf, cnew);          // F2C at t+1
+        coarseToFine(cnew, altf, 1.0);     // C2F at t+1
+        alt = cnew;
         ++steps;
     }
 };
@@ -507,7 +946,10 @@ int orc_init(void* h) {
 
 int orc_step(void* h, int n) {
     Oracle* o = static_cast<Oracle*>(h);
-    for (int s = 0; s < n; ++s) o->stepSingle();
+    for (int s = 0; s < n; ++s) {
+        if (o->lev.size() == 2) o->stepTwoLevel();
+        else o->stepSingle();
+    }
     return 0;
 }
 
@@ -523,7 +965,7 @@ int orc_read_populations(void* h, int level, double* out) {
     Oracle* o = static_cast<Oracle*>(h);
     if (level < 0 || level >= (int)o->lev.size()) return -1;
     const orc::Level& L = o->lev[level];
-    const double* f = L.f[o->alt].data();
+    const double* f = L.f[level == 0 ? o->alt : o->altf].data();
     for (long n = 0; n < L.N; ++n)
         for (int q = 0; q < orc::Q; ++q) out[(long)q * L.N + n] = f[n * orc::Q + q];
     return 0;
