@@ -1,16 +1,18 @@
 """Benchmark of the acPulse_vcLBM hot path on B200.
 
-Workload (default): the operator/scheme sweep configuration's lattice -- a
-quasi-2D Gaussian pulse on 1024 x 512 x 3 coarse nodes, periodic in y and z,
-LODI non-reflecting faces in x, HRR collision (sigma = 0.98, order 3),
-nu = 1e-4 lattice units, eps = 1e-3, b = 24 cells.  Inputs are synthetic
-(seeded pulse parameters); there is no dataset.
+Workload (default): the operator/scheme sweep configuration -- a quasi-2D
+Gaussian pulse on 1024 x 512 x 3 coarse nodes, periodic in y and z, LODI
+non-reflecting faces in x, the right half (x >= 512) refined 2:1 with the
+standard overlap scheme and arithmetic-average (LAG) restriction, HRR
+collision (sigma = 0.98, order 3), nu = 1e-4 lattice units, eps = 1e-3,
+b = 24 coarse cells.  Inputs are synthetic (seeded pulse parameters); there
+is no dataset.
 
-A step is one coarse time step of the whole lattice.  `value` is the
-FP32-deviation form's throughput in MLUPS (node updates per second / 1e6)
-with the state resident in HBM; the FP64 form runs the same steps and its
-MLUPS, the FP32/FP64 ratio and the FP32 form's pressure error against FP64
-are reported beside it.  Timing: CUDA events on the stream the engine
+A step is one coarse time step (a coarse step and two fine sub-steps with the
+couplings).  MLUPS = (live coarse nodes + 2 x fine nodes) x steps / s / 1e6.
+`value` is the FP32-deviation form's MLUPS with the state resident in HBM;
+the FP64 form runs the same steps and its MLUPS, the FP32/FP64 ratio and the
+FP32 form's pressure error against FP64 are reported beside it.  Timing: CUDA events on the stream the engine
 launches on, W warm-up steps, K timed steps, max over ranks.  The working set
 (populations, two arrays) is larger than the 126 MB L2, so no flush is needed.
 
@@ -46,6 +48,8 @@ def parse():
     ap.add_argument("--ny", type=int, default=512)
     ap.add_argument("--nz", type=int, default=3)
     ap.add_argument("--nu", type=float, default=1e-4)
+    ap.add_argument("--levels", type=int, default=2, choices=[1, 2])
+    ap.add_argument("--filter", default="LAG")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -57,13 +61,32 @@ def workload(args, storage):
                            center=(args.nx / 4.0, args.ny / 2.0, 1.0), storage=storage)
     d.hybrid_sigma = 0.98
     d.mrt_writeback = 1
+    if args.levels == 2:
+        from acpulse_vclbm_b200.capi import F2C_FILTER, LAYOUT_BOX
+        d.max_level = 1
+        d.layout = LAYOUT_BOX
+        d.box_lo[:] = [args.nx // 2, 0, 0]
+        d.box_hi[:] = [args.nx - 1, args.ny - 1, args.nz - 1]
+        d.f2c_filter = F2C_FILTER[args.filter]
     return d
 
 
+def updates_per_step(desc):
+    """live coarse nodes + 2 x fine nodes of one coarse step"""
+    if desc.max_level == 0:
+        return desc.nx * desc.ny * desc.nz
+    nx, ny, nz = desc.nx, desc.ny, desc.nz
+    coarse = (desc.box_lo[0] + 2) * ny * nz
+    fine = (2 * (desc.box_hi[0] - desc.box_lo[0]) + 1) * 2 * ny * 2 * nz
+    return coarse + 2 * fine
+
+
 def config_of(args):
-    return {"workload": f"quasi-2D Gaussian pulse, {args.nx}x{args.ny}x{args.nz} coarse nodes, single level, "
+    lv = (f"right half (x >= {args.nx // 2}) refined 2:1, overlap 1, {args.filter} restriction"
+          if args.levels == 2 else "single level")
+    return {"workload": f"quasi-2D Gaussian pulse, {args.nx}x{args.ny}x{args.nz} coarse nodes, {lv}, "
                         f"periodic y/z, LODI x faces, {args.op} order 3, nu={args.nu:g} lu, eps=1e-3, b=24",
-            "nodes": args.nx * args.ny * args.nz, "op": args.op, "levels": 1,
+            "updates_per_step": updates_per_step(workload(args, "FP64")), "op": args.op, "levels": args.levels,
             "l2_flush": "not needed: population arrays exceed the 126 MB L2",
             "parallelism": f"replicas x{args.gpus}"}
 
@@ -160,8 +183,7 @@ def cpu_oracle_mlups(desc, budget_s=12.0, max_steps=40, threads=0):
         o.step(1)
         n += 1
     dt = time.perf_counter() - t0
-    nodes = desc.nx * desc.ny * desc.nz
-    return nodes * n / dt / 1e6, n, dt
+    return updates_per_step(desc) * n / dt / 1e6, n, dt
 
 
 def run_reference(args):
@@ -174,17 +196,21 @@ def run_reference(args):
     o = OracleLattice(d, threads=threads)
     o.init()
     o.step(min(args.warmup, 1))
+    # each step is a bounded sample: stop after K steps or 120 s of CPU work
+    n = 0
     t0 = time.perf_counter()
-    o.step(args.steps)
+    while n < args.steps and time.perf_counter() - t0 < 120.0:
+        o.step(1)
+        n += 1
     dt = time.perf_counter() - t0
-    nodes = d.nx * d.ny * d.nz
-    v = nodes * args.steps / dt / 1e6
+    v = updates_per_step(d) * n / dt / 1e6
     line = {"impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": "MLUPS", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
+            "steps": n, "warmup": args.warmup, "ms_per_step": dt * 1e3 / n,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "config": config_of(args),
             "cpu_baseline": {"value": round(v, 3), "unit": "MLUPS", "cores": threads, "kind": "port",
-                             "sample": f"{args.steps} coarse steps of the full workload, FP64 oracle"},
+                             "sample": f"{n} coarse steps of the full workload in {dt:.1f} s, FP64 CPU oracle "
+                                       f"(restated reference, OpenMP)"},
             "e2e": {"value": round(v, 3), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -201,7 +227,7 @@ def run_engine(args):
 
     d32 = workload(args, "FP32-DEV")
     d64 = workload(args, "FP64")
-    nodes = d32.nx * d32.ny * d32.nz
+    nodes = updates_per_step(d32)
 
     L32 = engine.Lattice(d32, device=local)
     engine.lib().acp_set_stream(L32._h, stream)
@@ -224,9 +250,11 @@ def run_engine(args):
 
     # accuracy of the FP32 deviation form against FP64 after the same steps
     cs2 = d64.speed_of_sound ** 2
-    p32 = L32.field(4)
-    p64 = L64.field(4)
-    rel_err = float(np.abs(p32 - p64).max() / (d64.ic_eps * d64.density * cs2))
+    amp = d64.ic_eps * d64.density * cs2
+    live_x = slice(0, d64.box_lo[0] + 2) if d64.max_level == 1 else slice(None)
+    rel_err = float(np.abs(L32.field(4)[..., live_x] - L64.field(4)[..., live_x]).max() / amp)
+    if d64.max_level == 1:
+        rel_err = max(rel_err, float(np.abs(L32.field(4, 1) - L64.field(4, 1)).max() / amp))
 
     # per-kernel device time (events between launches) for the roofline
     import ctypes as C
@@ -239,8 +267,8 @@ def run_engine(args):
     lps = C.c_int()
     engine.lib().acp_launches_per_step(L32._h, C.byref(lps))
     peak, peak_kind = peaks()
-    alg_bytes = nodes * 2 * 19 * 4  # FP32 deviation storage: read 19 + write 19 per node
-    achieved = alg_bytes / (collide_ms32 * 1e-3) / 1e9
+    alg_bytes = nodes * 2 * 19 * 4  # FP32 deviation storage: read 19 + write 19 per node update
+    achieved = alg_bytes / (collide_ms32 * 1e-3) / 1e9  # collide launches of one coarse step
     L32.close()
     L64.close()
 
@@ -252,9 +280,13 @@ def run_engine(args):
     Le.step(args.steps)
     Le.sync()
     pe = Le.field(4)
+    if d32.max_level == 1:
+        pe = Le.field(4, 1)
     t1 = time.perf_counter()
-    h2d = nodes + 2 * (d32.ny * d32.nz) * 80  # node classes + LODI wiring records
-    d2h = nodes * 19 * 8  # populations read back for the pressure field
+    dims = [Le.dims(l) for l in range(d32.max_level + 1)]
+    stored = sum(a * b * c for a, b, c in dims)
+    h2d = stored + 2 * (d32.ny * d32.nz) * 80  # node classes + LODI wiring records
+    d2h = stored * 19 * 8  # populations read back for the pressure fields
     Le.close()
     e2e = nodes * args.steps / (t1 - t0) / 1e6
 
@@ -276,7 +308,7 @@ def run_engine(args):
                 "fp32_pressure_err_rel_amplitude": rel_err,
                 "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                              "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
-                             "kernel": "k_collide_push (FP32 deviation)",
+                             "kernel": "collide+push kernels of one coarse step (FP32 deviation)",
                              "algorithmic_bytes_per_node": 152, "traffic": ncu_traffic("collide_fp32"),
                              "kernel_ms": {"moments": km[0], "collide": km[1], "lodi": km[2], "probes": km[4]}},
                 "cpu_baseline": cpu,
