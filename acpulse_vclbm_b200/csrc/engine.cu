@@ -875,6 +875,37 @@ size_t estimateBytes(const acp_case_desc& d) {
 
 }  // namespace
 
+// Device scratch of acp_read_populations_window: the FP64 copy of one window
+// of nodes lives in this fixed array instead of a per-call allocation.
+static __device__ __align__(256) double g_windowScratch[(size_t)ACP_WINDOW_MAX_NODES * Q];
+
+namespace {
+std::mutex g_windowMutex;
+double* g_windowPtr[64] = {nullptr};
+
+// device address of g_windowScratch on `device` (current), looked up once per device
+int windowScratch(acp_handle* h, int device, double** out) {
+    if (device < 0 || device >= 64) return fail(h, ACP_ERR_UNSUPPORTED, "device index %d beyond 63", device);
+    std::lock_guard<std::mutex> lock(g_windowMutex);
+    if (!g_windowPtr[device]) {
+        double* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress((void**)&p, g_windowScratch);
+        if (e != cudaSuccess) return fail(h, ACP_ERR_CUDA, "cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+        g_windowPtr[device] = p;
+    }
+    *out = g_windowPtr[device];
+    return ACP_OK;
+}
+
+template <typename S>
+void launchWindow(acp_handle* h, int l, int arr, long long begin, int count, double* dst) {
+    LevelArgs<S> a = levelArgs<S>(h, l, 0);
+    const long long total = (long long)count * Q;
+    k_to_f64_window<S><<<(unsigned)((total + 255) / 256), 256, 0, h->stream>>>((const S*)h->dev[l].f[arr], dst,
+                                                                                h->host[l].N, begin, count, h->shift, a);
+}
+}  // namespace
+
 extern "C" {
 
 void acp_default_case(acp_case_desc* d) {
@@ -1058,6 +1089,31 @@ int acp_read_populations(acp_handle* h, int level, double* out) {
     cudaError_t e = cudaMemcpyAsync(out, tmp, (size_t)L.N * Q * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
     cudaFreeAsync(tmp, h->stream);
     if (e != cudaSuccess) return fail(h, ACP_ERR_CUDA, "copy: %s", cudaGetErrorString(e));
+    CU(h, cudaStreamSynchronize(h->stream));
+    return ACP_OK;
+}
+
+int acp_read_populations_window(acp_handle* h, int level, long long begin, int count, double* out) {
+    if (!h || !out || level < 0 || level >= (int)h->host.size()) return ACP_ERR_INVALID;
+    const LevelHost& L = h->host[level];
+    if (count < 0 || count > ACP_WINDOW_MAX_NODES)
+        return fail(h, ACP_ERR_INVALID, "window of %d nodes: at most %d (ACP_WINDOW_MAX_NODES) per call", count,
+                    ACP_WINDOW_MAX_NODES);
+    if (begin < 0 || begin + count > L.N)
+        return fail(h, ACP_ERR_INVALID, "window [%lld, %lld) outside the level's %lld nodes", begin, begin + count, L.N);
+    if (count == 0) return ACP_OK;
+    CU(h, cudaSetDevice(h->device));
+    double* scratch = nullptr;
+    int s = windowScratch(h, h->device, &scratch);
+    if (s) return s;
+    const int arr = level == 0 ? h->cur : 0;
+    switch (h->d.storage) {
+        case ACP_STORE_F64: launchWindow<double>(h, level, arr, begin, count, scratch); break;
+        case ACP_STORE_F32_DEV: launchWindow<float>(h, level, arr, begin, count, scratch); break;
+        default: launchWindow<__half>(h, level, arr, begin, count, scratch); break;
+    }
+    CU(h, cudaGetLastError());
+    CU(h, cudaMemcpyAsync(out, scratch, (size_t)count * Q * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     CU(h, cudaStreamSynchronize(h->stream));
     return ACP_OK;
 }

@@ -669,6 +669,16 @@ __global__ void k_to_f64(const S* __restrict__ src, double* dst, long long N, do
     const int q = (int)(t / N);
     dst[t] = (double)Store<S>::load(src + t, la.hscale[q]) + wq(q) * shift;
 }
+// storage -> absolute FP64 populations of the node window [begin, begin+count)
+template <typename S>
+__global__ void k_to_f64_window(const S* __restrict__ src, double* dst, long long N, long long begin, int count,
+                                double shift, LevelArgs<S> la) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)count * Q) return;
+    const int q = (int)(t / count);
+    const long long m = t - (long long)q * count;
+    dst[t] = (double)Store<S>::load(src + (long long)q * N + begin + m, la.hscale[q]) + wq(q) * shift;
+}
 template <typename S>
 __global__ void k_from_f64(const double* __restrict__ src, S* dst0, S* dst1, long long N, double shift, LevelArgs<S> la) {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;

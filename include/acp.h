@@ -181,6 +181,27 @@ int acp_launches_per_step(acp_handle* h, int* launches);
  * (Lattice::setConnectivity, Lattice.cpp:500-1394).  rows may be NULL to
  * query *count. */
 int acp_boundary_wiring(const acp_case_desc* d, long long* rows, long long max_rows, long long* count);
+/* Largest window, in nodes, that acp_read_populations_window accepts. */
+#define ACP_WINDOW_MAX_NODES 32768
+/* Read the populations of the nodes [node_begin, node_begin + node_count) of
+ * a level as FP64 f_i into host_out[q * node_count + m] -- the same values
+ * acp_read_populations gives for those nodes -- without allocating any device
+ * memory.  It has no counterpart in the reference (whose populations live in
+ * host memory).  It is for callers that cannot allocate on the device: a
+ * serving process that has handed its whole HBM budget to resident lattices,
+ * where the temporary FP64 copy of a level that acp_read_populations makes
+ * could fail or eat into another solve's share, and applications whose own
+ * allocator owns all device memory and forbids cudaMalloc from libraries.
+ * The FP64 conversion goes through one fixed device array of
+ * ACP_WINDOW_MAX_NODES x 19 doubles (about 5 MB) built into the library; every
+ * device that loads the library holds it until the process exits.  Larger
+ * windows are rejected (ACP_ERR_INVALID): read a large level window by window.
+ * The first call on a device looks up that array's device address (once per
+ * device), so make the first call before any stream capture on the device.
+ * All calls share the array: calls that overlap on the GPU (other threads or
+ * streams) race and must be serialised by the caller.  Nothing in it needs to
+ * start at zero; each call overwrites the part it reads back. */
+int acp_read_populations_window(acp_handle* h, int level, long long node_begin, int node_count, double* host_out);
 int acp_destroy(acp_handle* h);
 const char* acp_last_error(const acp_handle* h);
 const char* acp_status_string(int status);
