@@ -21,10 +21,20 @@ def main():
     ap.add_argument("--nz", type=int, default=3)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--timed", type=int, default=0, help="also run N steps kernel by kernel with events")
+    ap.add_argument("--levels", type=int, default=1, choices=[1, 2],
+                    help="2: refine the right half 2:1 (the sweep configuration's layout)")
+    ap.add_argument("--filter", default="LAG")
     a = ap.parse_args()
     d = lattice_units_case(a.nx, a.ny, a.nz, op=a.op, nu_lu=1e-4, order=a.order, periodic=(False, True, True),
                            eps=1e-3, b=24.0, center=(a.nx / 4.0, a.ny / 2.0, 1.0), storage=a.storage)
     d.mrt_writeback = 1
+    if a.levels == 2:
+        from .capi import F2C_FILTER, LAYOUT_BOX
+        d.max_level = 1
+        d.layout = LAYOUT_BOX
+        d.box_lo[:] = [a.nx // 2, 0, 0]
+        d.box_hi[:] = [a.nx - 1, a.ny - 1, a.nz - 1]
+        d.f2c_filter = F2C_FILTER[a.filter]
     L = engine.Lattice(d).init()
     L.step(a.steps)
     L.sync()
@@ -32,11 +42,12 @@ def main():
         km = (C.c_double * 5)()
         engine.lib().acp_step_timed.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
         engine.lib().acp_step_timed(L._h, a.timed, C.cast(km, C.c_void_p))
-        nodes = a.nx * a.ny * a.nz
+        c, f = L.active_updates()
+        nodes = c + 2 * f
         b = {"FP64": 8, "FP32-DEV": 4, "FP16-DEV": 2}[a.storage] * 38
-        print(f"{a.op} {a.storage} order {a.order} {a.nx}x{a.ny}x{a.nz}: moments {km[0]*1e3:.1f} us, "
+        print(f"{a.op} {a.storage} order {a.order} {a.nx}x{a.ny}x{a.nz} levels {a.levels}: "
               f"collide {km[1]*1e3:.1f} us ({nodes * b / (km[1] * 1e-3) / 1e9:.0f} GB/s algorithmic), "
-              f"lodi {km[2]*1e3:.1f} us")
+              f"lodi {km[2]*1e3:.1f} us, coupling {km[3]*1e3:.1f} us, updates/step {nodes}")
     L.close()
 
 
