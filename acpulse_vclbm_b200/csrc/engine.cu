@@ -713,9 +713,10 @@ void enqueueC2F(acp_handle* h, int cnew, int fdst, R th) {
         else k_c2f_coincident<S, R, 4><<<g, 128, 0, h->stream>>>(Bc, Ff, h->dC2F, h->nCoinc, pre, th, c, la);
     }
     if (h->nMid)
-        k_c2f_interp<S, R><<<(h->nMid + 127) / 128, 128, 0, h->stream>>>(Ff, h->dC2F + h->nCoinc, h->nMid, c, la);
+        k_c2f_interp<S, R><<<(h->nMid * Q + 255) / 256, 256, 0, h->stream>>>(Ff, h->dC2F + h->nCoinc, h->nMid, c, la);
     if (h->nCen)
-        k_c2f_interp<S, R><<<(h->nCen + 127) / 128, 128, 0, h->stream>>>(Ff, h->dC2F + h->nCoinc + h->nMid, h->nCen, c, la);
+        k_c2f_interp<S, R><<<(h->nCen * Q + 255) / 256, 256, 0, h->stream>>>(Ff, h->dC2F + h->nCoinc + h->nMid,
+                                                                                h->nCen, c, la);
 }
 
 // one coarse step: single level, or the two-level sequence of
@@ -740,7 +741,7 @@ int enqueueStepT(acp_handle* h, int src, PhaseTimer* tm) {
         if (tm) tm->mark(-1);
         if (!h->f2cHost.empty()) {
             LevelArgs<S> lf = levelArgs<S>(h, 1, 0);
-            const unsigned g = ((unsigned)h->f2cHost.size() + 127) / 128;
+            const unsigned g = ((unsigned)h->f2cHost.size() * 32 + 127) / 128;  // a warp per coarse node
             const S* Ff = (const S*)h->dev[1].f[0];
             S* Bc = (S*)h->dev[0].f[1 - src];
             const int n = (int)h->f2cHost.size();

@@ -824,52 +824,57 @@ __global__ void k_c2f_coincident(const S* __restrict__ Bc, S* Ff, const C2FDev* 
 
 // C2F on the other fine coupling nodes: interpolation along the face from
 // the nodes written before (mid nodes from coincident ones, centre nodes from
-// mid nodes)
+// mid nodes); one thread per (node, population)
 template <typename S, typename R>
 __global__ void k_c2f_interp(S* Ff, const C2FDev* __restrict__ nodes, int count, CouplingArgs c, LevelArgs<S> la) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= count) return;
-    const C2FDev nd = nodes[t];
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)count * Q) return;
+    const int q = (int)(t / count);
+    const int m = (int)(t - (long long)q * count);
+    const C2FDev& nd = nodes[m];
+    if (!(nd.mask >> q & 1u)) return;
+    R acc = 0;
 #pragma unroll
-    for (int q = 0; q < Q; ++q) {
-        if (!(nd.mask >> q & 1u)) continue;
-        R acc = 0;
-#pragma unroll
-        for (int m = 0; m < 4; ++m)
-            if (nd.st[m] >= 0) acc += R(nd.w[m]) * R(Store<S>::load(Ff + (long long)q * c.Nf + nd.st[m], la.hscale[q]));
-        Store<S>::store(Ff + (long long)q * c.Nf + nd.n, acc, la.hscale[q]);
-    }
+    for (int k = 0; k < 4; ++k)
+        if (nd.st[k] >= 0) acc += R(nd.w[k]) * R(Store<S>::load(Ff + (long long)q * c.Nf + nd.st[k], la.hscale[q]));
+    Store<S>::store(Ff + (long long)q * c.Nf + nd.n, acc, la.hscale[q]);
 }
 
-// F2C on the coarse nodes one cell inside the fine box
+// F2C on the coarse nodes one cell inside the fine box: one warp per coarse
+// node, lane m < 27 forms the weighted non-equilibrium of fine neighbour m
 template <typename S, typename R, int ORDER>
 __global__ void k_f2c(const S* __restrict__ Ff, S* Bc, const F2CDev* __restrict__ nodes, int count, CouplingArgs c,
                       LevelArgs<S> la) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= count) return;
-    const F2CDev& nd = nodes[t];
-    R g[Q], geq[Q], neq[Q];
+    const int warp = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (warp >= count) return;  // uniform per warp
+    const F2CDev& nd = nodes[warp];
+    R neq[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) neq[q] = 0;
+    const bool filtered = c.filter != 0;
+    const int member = filtered ? lane : (lane == 0 ? 13 : -1);  // NOFI: the coincident node only
+    if (member >= 0 && member < 27) {
+        const int dx = member % 3, dy = (member / 3) % 3, dz = member / 9;
+        const R wgt = !filtered ? R(1)
+                                : (c.filter == 1 ? R(1.0 / 27.0)
+                                                 : R((dx == 1 ? 0.5 : 0.25) * (dy == 1 ? 0.5 : 0.25) * (dz == 1 ? 0.5 : 0.25)));
+        R h[Q], heq[Q];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) h[q] = R(Store<S>::load(Ff + (long long)q * c.Nf + nd.cube[member], la.hscale[q]));
+        eqSplit<R, ORDER>(h, R(c.shiftC), R(c.kappa), heq);
+#pragma unroll
+        for (int q = 0; q < Q; ++q) neq[q] = wgt * (h[q] - heq[q]);
+    }
+#pragma unroll
+    for (int q = 0; q < Q; ++q)
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) neq[q] += __shfl_down_sync(0xffffffffu, neq[q], off);
+    if (lane != 0) return;
+    R g[Q], geq[Q];
 #pragma unroll
     for (int q = 0; q < Q; ++q) g[q] = R(Store<S>::load(Ff + (long long)q * c.Nf + nd.partner, la.hscale[q]));
     eqSplit<R, ORDER>(g, R(c.shiftC), R(c.kappa), geq);
-    if (c.filter == 0) {
-#pragma unroll
-        for (int q = 0; q < Q; ++q) neq[q] = g[q] - geq[q];
-    } else {
-#pragma unroll
-        for (int q = 0; q < Q; ++q) neq[q] = 0;
-        for (int m = 0; m < 27; ++m) {
-            const int dx = m % 3, dy = (m / 3) % 3, dz = m / 9;
-            const R wgt = c.filter == 1 ? R(1.0 / 27.0)
-                                        : R((dx == 1 ? 0.5 : 0.25) * (dy == 1 ? 0.5 : 0.25) * (dz == 1 ? 0.5 : 0.25));
-            R h[Q], heq[Q];
-#pragma unroll
-            for (int q = 0; q < Q; ++q) h[q] = R(Store<S>::load(Ff + (long long)q * c.Nf + nd.cube[m], la.hscale[q]));
-            eqSplit<R, ORDER>(h, R(c.shiftC), R(c.kappa), heq);
-#pragma unroll
-            for (int q = 0; q < Q; ++q) neq[q] += wgt * (h[q] - heq[q]);
-        }
-    }
     rescaleNeq<R>(neq, c, false);
 #pragma unroll
     for (int q = 0; q < Q; ++q)
