@@ -73,6 +73,7 @@ struct acp_handle {
     std::string err;
     double c = 0, kappa = 0, shift = 0;
     float hscale[Q];
+    double m4[18] = {0};  // sum_q w_q H2_q (x) H4_q(kappa) (fourth-order equilibria)
 };
 
 namespace {
@@ -554,6 +555,7 @@ LevelArgs<S> levelArgs(acp_handle* h, int l, int src) {
     a.kappa = h->kappa;
     a.sigma = h->d.hybrid_sigma;
     for (int q = 0; q < Q; ++q) a.hscale[q] = h->hscale[q];
+    for (int c = 0; c < 18; ++c) a.m4[c] = h->m4[c];
     return a;
 }
 
@@ -963,6 +965,20 @@ int acp_create(const acp_case_desc* d, int device, acp_handle** out) {
     h->c = d->speed_of_sound * std::sqrt(3.0);
     h->kappa = 1.0 / (6.0 * h->c * h->c);
     h->shift = d->storage == ACP_STORE_F64 ? 0.0 : d->density;
+    if (d->eq_order == 4) {
+        // projection of the orthogonalised fourth-order Hermite terms on H2,
+        // nonzero when kappa differs from the lattice-unit value 1/6
+        for (int q = 0; q < Q; ++q) {
+            const double hxx = ex(q) * ex(q) - 1.0 / 3.0, hyy = ey(q) * ey(q) - 1.0 / 3.0, hzz = ez(q) * ez(q) - 1.0 / 3.0;
+            const double h2[6] = {hxx, hyy, hzz, (double)(ex(q) * ey(q)), (double)(ex(q) * ez(q)), (double)(ey(q) * ez(q))};
+            double f0 = hxx * hyy + h->kappa * hzz;
+            double f1 = hxx * hzz + h->kappa * hyy + 2.0 / 7.0 * f0;
+            double f2 = hyy * hzz + h->kappa * hxx + 2.0 / 7.0 * f0 + 2.0 / 5.0 * f1;
+            const double h4[3] = {8.0 / 7.0 * f0, 56.0 / 45.0 * f1, 40.0 / 27.0 * f2};
+            for (int ab = 0; ab < 6; ++ab)
+                for (int k = 0; k < 3; ++k) h->m4[ab * 3 + k] += wq(q) * h2[ab] * h4[k];
+        }
+    }
     for (int q = 0; q < Q; ++q) h->hscale[q] = 1.0f;
     if (d->storage == ACP_STORE_F16_DEV) {
         // power-of-two scale per population: the deviation w_q * drho of a

@@ -59,6 +59,7 @@ struct LevelArgs {
     double kappa;   // 1/(6 c^2): fourth-order orthogonalisation constant
     double sigma;   // HRR hybrid parameter
     float hscale[Q];  // FP16 per-population scales (1 otherwise)
+    double m4[18];    // sum_q w_q H2_q,ab H4_q,k(kappa), ab in {xx,yy,zz,xy,xz,yz}, k in 0..2
 };
 
 __device__ __forceinline__ int wrapc(int c, int n, int per) {
@@ -207,15 +208,18 @@ struct Collider {
 
         EqCoef<R, ORDER> ec;
         ec.set(u, kappa);
-        auto geq = [&](int q) -> R { return R(wq(q)) * (drho + rho * ec.poly(q, kappa)); };
 
         if (OP == OP_SRT) {
 #pragma unroll
-            for (int q = 0; q < Q; ++q) emit(q, g[q] + omega * (geq(q) - g[q]));
+            for (int q = 0; q < Q; ++q) {
+                const R geq = R(wq(q)) * (drho + rho * ec.poly(q, kappa));
+                emit(q, g[q] + omega * (geq - g[q]));
+            }
             return;
         }
 
-        // RR / HRR: strain rate S and cubic-Mach gradient G from the six axis neighbours
+        // RR / HRR.  Strain rate S and cubic-Mach gradient G from the
+        // neighbours (null for coupling nodes).
         R S[6] = {0, 0, 0, 0, 0, 0};
         R G[6] = {0, 0, 0, 0, 0, 0};
         if ((OP == OP_HRR || CUBIC) && nb) {
@@ -225,19 +229,41 @@ struct Collider {
                 G[c] = nb[6 + c];
             }
         }
-        // half time step times the cubic-Mach correction of direction q
-        auto hpsi = [&](int q) -> R { return R(2.25) * R(wq(q)) * h2dot<R>(q, G); };
-        R P[6] = {0, 0, 0, 0, 0, 0};
+        // Pi1 = sum_q H2_q (g_q - geq_q [+ dt/2 psi_q]) (Node.cpp:2493-2558), with
+        // the equilibrium and correction parts summed in closed form by the
+        // fourth-order isotropy of D3Q19 (sum_q w_q H2_q,ab H2_q,cd =
+        // (d_ac d_bd + d_ad d_bc) / 9, odd moments vanish): sum_q H2_q geq_q =
+        // rho (u u + 20.25 M a4), M = sum_q w_q H2_q (x) H4_q(kappa) per case
+        // (zero unless ORDER == 4), and sum_q H2_q dt/2 psi_q = G / 2.
+        R P[6];
+        {
+            R sxx = 0, syy = 0, szz = 0, sxy = 0, sxz = 0, syz = 0;
 #pragma unroll
-        for (int q = 0; q < Q; ++q) {
-            R gn = g[q] - geq(q);
-            if (CUBIC) gn += hpsi(q);
-            P[0] += h2xx<R>(q) * gn;
-            P[1] += h2yy<R>(q) * gn;
-            P[2] += h2zz<R>(q) * gn;
-            P[3] += R(ex(q) * ey(q)) * gn;
-            P[4] += R(ex(q) * ez(q)) * gn;
-            P[5] += R(ey(q) * ez(q)) * gn;
+            for (int q = 0; q < Q; ++q) {
+                if (ex(q)) sxx += g[q];
+                if (ey(q)) syy += g[q];
+                if (ez(q)) szz += g[q];
+                if (ex(q) * ey(q)) sxy += R(ex(q) * ey(q)) * g[q];
+                if (ex(q) * ez(q)) sxz += R(ex(q) * ez(q)) * g[q];
+                if (ey(q) * ez(q)) syz += R(ey(q) * ez(q)) * g[q];
+            }
+            const R third = drho / R(3);
+            P[0] = sxx - third - rho * ec.uu[0];
+            P[1] = syy - third - rho * ec.uu[1];
+            P[2] = szz - third - rho * ec.uu[2];
+            P[3] = sxy - rho * ec.uu[3];
+            P[4] = sxz - rho * ec.uu[4];
+            P[5] = syz - rho * ec.uu[5];
+            if (ORDER == 4) {
+#pragma unroll
+                for (int c = 0; c < 6; ++c)
+                    P[c] -= rho * R(20.25) *
+                            (R(a.m4[c * 3 + 0]) * ec.a4[0] + R(a.m4[c * 3 + 1]) * ec.a4[1] + R(a.m4[c * 3 + 2]) * ec.a4[2]);
+            }
+            if (CUBIC) {
+#pragma unroll
+                for (int c = 0; c < 6; ++c) P[c] += R(0.5) * G[c];
+            }
         }
         R A2[6];
         if (OP == OP_HRR) {
@@ -251,13 +277,26 @@ struct Collider {
         }
         NeqCoef<R, ORDER> nc;
         nc.set(A2, u, kappa);
+        // post-collision f_q = feq_q + (1 - omega) neq_q [+ dt/2 psi_q]: one
+        // Hermite polynomial per direction with the merged coefficients
+        // rho * (equilibrium) + (1 - omega) * (recursive non-equilibrium)
+        // [+ G / 2 in the second order for the cubic-Mach correction]
         const R om1 = R(1) - omega;
+        EqCoef<R, ORDER> mc;
 #pragma unroll
-        for (int q = 0; q < Q; ++q) {
-            R v = geq(q) + om1 * R(wq(q)) * nc.poly(q, kappa);
-            if (CUBIC) v += hpsi(q);
-            emit(q, v);
+        for (int c = 0; c < 3; ++c) mc.u[c] = rho * u[c];
+#pragma unroll
+        for (int c = 0; c < 6; ++c) mc.uu[c] = rho * ec.uu[c] + om1 * nc.A[c] + (CUBIC ? R(0.5) * G[c] : R(0));
+        if (ORDER >= 3) {
+#pragma unroll
+            for (int c = 0; c < 6; ++c) mc.a3[c] = rho * ec.a3[c] + om1 * nc.a3[c];
         }
+        if (ORDER == 4) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) mc.a4[c] = rho * ec.a4[c] + om1 * nc.a4[c];
+        }
+#pragma unroll
+        for (int q = 0; q < Q; ++q) emit(q, R(wq(q)) * (drho + mc.poly(q, kappa)));
     }
 };
 
