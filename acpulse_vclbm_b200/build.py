@@ -13,6 +13,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libacp_cuda.so")
+MAIN = os.path.join(HERE, "acp_main")
+HOSTCXX = os.environ.get("ACP_HOSTCXX", "/usr/bin/g++")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 SOURCES = ["engine.cu", "caseparse.cpp"]
@@ -26,10 +28,20 @@ def _deps():
 
 
 def up_to_date():
-    if not os.path.exists(OUT):
+    if not os.path.exists(OUT) or not os.path.exists(MAIN):
         return False
-    t = os.path.getmtime(OUT)
-    return all(os.path.getmtime(f) <= t for f in _deps())
+    t = min(os.path.getmtime(OUT), os.path.getmtime(MAIN))
+    host = [os.path.join(HERE, "host", f) for f in os.listdir(os.path.join(HERE, "host"))]
+    return all(os.path.getmtime(f) <= t for f in _deps() + host)
+
+
+def build_host():
+    """The drop-in C++ Control/Lattice and the reference-style driver, linked to libacp_cuda.so."""
+    host = os.path.join(HERE, "host")
+    srcs = [os.path.join(host, f) for f in ("Control.cpp", "Lattice.cpp", "acp_main.cpp")]
+    subprocess.run([HOSTCXX, "-O2", "-std=c++17", "-o", MAIN, *srcs, "-L" + HERE, "-lacp_cuda",
+                    "-Wl,-rpath,$ORIGIN"], check=True)
+    return MAIN
 
 
 def build(force=False, verbose_ptxas=False):
@@ -52,6 +64,7 @@ def build(force=False, verbose_ptxas=False):
     tmp = OUT + ".tmp"
     subprocess.run([NVCC, *ARCH, "-shared", "-cudart", "static", "-o", tmp, *objs], check=True)
     os.replace(tmp, OUT)
+    build_host()
     return OUT
 
 

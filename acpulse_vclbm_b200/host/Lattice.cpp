@@ -1,0 +1,99 @@
+// Lattice over the C ABI (see Lattice.h).
+#include "Lattice.h"
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <fstream>
+#include <iomanip>
+#include <iostream>
+#include <limits>
+
+void Lattice::check(int status, const char* what) {
+    if (status != ACP_OK) {
+        std::cerr << what << ": " << acp_status_string(status) << ": " << acp_last_error(h_) << std::endl;
+        std::exit(1);
+    }
+}
+
+Lattice::Lattice(Control& bc) : bc_(bc) {
+    check(acp_create(&bc.caseDescription(), -1, &h_), "Lattice");
+    const acp_case_desc& d = bc.caseDescription();
+    for (int l = 0; l <= d.max_level; ++l) {
+        check(acp_level_dims(h_, l, dims_[l]), "Lattice");
+        if (l == 1)
+            for (int a = 0; a < 3; ++a) origin_[1][a] = 2 * d.box_lo[a];
+    }
+}
+
+Lattice::~Lattice() {
+    if (h_) acp_destroy(h_);
+}
+
+void Lattice::initialization(Control&) {
+    check(acp_init(h_), "initialization");
+    // main.cpp:55-57: both flags start true and the state is in both arrays
+    currentFlag_ = true;
+    stepsSeen_[0] = stepsSeen_[1] = -1;
+}
+
+void Lattice::solve(bool& alternating) {
+    check(acp_step(h_, 1), "solve");
+    // the reference collides in array `alternating` and streams into the other,
+    // which the caller then selects by toggling its flag (main.cpp:155)
+    currentFlag_ = !alternating;
+}
+
+void Lattice::solve(bool& alternatingL0, bool&) {
+    check(acp_step(h_, 1), "solve");
+    currentFlag_ = !alternatingL0;
+}
+
+void Lattice::refresh(int level) {
+    long long steps = 0;
+    acp_steps_done(h_, &steps);
+    if (stepsSeen_[level] == steps) return;
+    check(acp_sync(h_), "sync");
+    const size_t n = (size_t)dims_[level][0] * dims_[level][1] * dims_[level][2];
+    cache_[level].resize(n * 19);
+    check(acp_read_populations(h_, level, cache_[level].data()), "getDistribution");
+    stepsSeen_[level] = steps;
+}
+
+double Lattice::getDistribution(bool& alternating, int& dir, int& level, int& i, int& j, int& k) {
+    if (dir >= 19 || level < 0 || level > bc_.caseDescription().max_level) return 0.;
+    if (alternating != currentFlag_) return std::numeric_limits<double>::quiet_NaN();  // only the current array is kept
+    refresh(level);
+    const int li = i - origin_[level][0], lj = j - origin_[level][1], lk = k - origin_[level][2];
+    const int* n = dims_[level];
+    if (li < 0 || lj < 0 || lk < 0 || li >= n[0] || lj >= n[1] || lk >= n[2]) return 0.;
+    const size_t N = (size_t)n[0] * n[1] * n[2];
+    return cache_[level][(size_t)dir * N + ((size_t)lk * n[1] + lj) * n[0] + li];
+}
+
+void Lattice::writeResultsVTK(std::string filename, bool&, bool&) {
+    const acp_case_desc& d = bc_.caseDescription();
+    for (int l = 0; l <= d.max_level; ++l) {
+        const int* n = dims_[l];
+        const size_t N = (size_t)n[0] * n[1] * n[2];
+        std::vector<double> rho(N), ux(N), uy(N), uz(N);
+        check(acp_read_field(h_, l, ACP_FIELD_RHO, rho.data()), "writeResultsVTK");
+        check(acp_read_field(h_, l, ACP_FIELD_UX, ux.data()), "writeResultsVTK");
+        check(acp_read_field(h_, l, ACP_FIELD_UY, uy.data()), "writeResultsVTK");
+        check(acp_read_field(h_, l, ACP_FIELD_UZ, uz.data()), "writeResultsVTK");
+        const double sp = d.spacing / std::pow(2., l);
+        std::ofstream out(filename + (d.max_level ? "_level" + std::to_string(l) : std::string()) + ".vtk");
+        out << "# vtk DataFile Version 3.0\nacPulse_vcLBM level " << l << "\nASCII\nDATASET STRUCTURED_POINTS\n";
+        out << "DIMENSIONS " << n[0] << " " << n[1] << " " << n[2] << "\n";
+        out << "ORIGIN " << origin_[l][0] * sp << " " << origin_[l][1] * sp << " " << origin_[l][2] * sp << "\n";
+        out << "SPACING " << sp << " " << sp << " " << sp << "\nPOINT_DATA " << N << "\n";
+        out << std::setprecision(8);
+        const double cs2 = d.speed_of_sound * d.speed_of_sound;
+        out << "SCALARS Pressure double 1\nLOOKUP_TABLE default\n";
+        for (size_t m = 0; m < N; ++m) out << rho[m] * cs2 << "\n";
+        out << "SCALARS Density double 1\nLOOKUP_TABLE default\n";
+        for (size_t m = 0; m < N; ++m) out << rho[m] << "\n";
+        out << "VECTORS Velocity double\n";
+        for (size_t m = 0; m < N; ++m) out << ux[m] << " " << uy[m] << " " << uz[m] << "\n";
+    }
+}
