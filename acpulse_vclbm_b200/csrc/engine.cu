@@ -546,6 +546,7 @@ LevelArgs<S> levelArgs(acp_handle* h, int l, int src) {
     LevelArgs<S> a;
     a.nx = L.nx; a.ny = L.ny; a.nz = L.nz;
     a.N = L.N;
+    a.Ni = (int)L.N;
     for (int ax = 0; ax < 3; ++ax) a.per[ax] = L.per[ax];
     a.A = (const S*)D.f[src];
     a.B = (S*)D.f[1 - src];

@@ -40,16 +40,17 @@ __constant__ double c_rmTinv2[Q][5];
 __constant__ float c_gsMinvF[Q][Q];
 __constant__ float c_rmTinv2F[Q][5];
 
-// pre-collision density (absolute) and lattice velocity of a node
+// pre-collision moments of a node
 template <typename R>
 struct MomR {
-    R rho, ux, uy, uz;
+    R drho, ux, uy, uz;  // deviation density and lattice velocity
 };
 
 template <typename S>
 struct LevelArgs {
     int nx, ny, nz;
     long long N;
+    int Ni;      // N as int: 19 * N < 2^31, so population element indices are 32-bit
     int per[3];  // periodic axes
     const S* A;  // array read this step
     S* B;        // array written this step
@@ -96,12 +97,111 @@ struct RT<float> {
     __device__ __forceinline__ static float rmTinv(int q, int m) { return c_rmTinv2F[q][m]; }
 };
 
+// second-order sums {xx, yy, zz, xy, xz, yz} of a node's deviations g:
+// sum over the directions with a nonzero component (diagonal) or of the
+// signed products (off-diagonal)
+template <typename R>
+__device__ __forceinline__ void secondSums(const R* g, R* s2) {
+    R sxx = 0, syy = 0, szz = 0, sxy = 0, sxz = 0, syz = 0;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        if (ex(q)) sxx += g[q];
+        if (ey(q)) syy += g[q];
+        if (ez(q)) szz += g[q];
+        if (ex(q) * ey(q)) sxy += R(ex(q) * ey(q)) * g[q];
+        if (ex(q) * ez(q)) sxz += R(ex(q) * ez(q)) * g[q];
+        if (ey(q) * ez(q)) syz += R(ey(q) * ez(q)) * g[q];
+    }
+    s2[0] = sxx; s2[1] = syy; s2[2] = szz; s2[3] = sxy; s2[4] = sxz; s2[5] = syz;
+}
+
+// Regularised collision (RR, Node.cpp:560-650; HRR, Node.cpp:653-736) of one
+// node from its moments: drho, lattice velocity u and the second-order sums
+// s2 of its deviations.  nb: strain S and cubic-Mach gradient G of the node
+// (12 values), or null for a coupling node, whose neighbours are not all on
+// its level: there the hybrid operator falls back to the population-based Pi1
+// (sigma = 1) and the cubic-Mach correction is dropped.
+template <typename R, int OP, int ORDER, bool CUBIC, typename ST, typename Emit>
+__device__ __forceinline__ void regularisedEmit(R drho, const R* u, const R* s2, const LevelArgs<ST>& a, const R* nb,
+                                                Emit& emit) {
+    const R rho = R(a.shift) + drho;
+    const R omega = R(a.omega);
+    const R kappa = R(a.kappa);
+    EqCoef<R, ORDER> ec;
+    ec.set(u, kappa);
+    R S[6] = {0, 0, 0, 0, 0, 0};
+    R G[6] = {0, 0, 0, 0, 0, 0};
+    if ((OP == OP_HRR || CUBIC) && nb) {
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+            S[c] = nb[c];
+            G[c] = nb[6 + c];
+        }
+    }
+    // Pi1 = sum_q H2_q (g_q - geq_q [+ dt/2 psi_q]) (Node.cpp:2493-2558), with
+    // the equilibrium and correction parts summed in closed form by the
+    // fourth-order isotropy of D3Q19 (sum_q w_q H2_q,ab H2_q,cd =
+    // (d_ac d_bd + d_ad d_bc) / 9, odd moments vanish): sum_q H2_q geq_q =
+    // rho (u u + 20.25 M a4), M = sum_q w_q H2_q (x) H4_q(kappa) per case
+    // (zero unless ORDER == 4), and sum_q H2_q dt/2 psi_q = G / 2.
+    R P[6];
+    {
+        const R sxx = s2[0], syy = s2[1], szz = s2[2], sxy = s2[3], sxz = s2[4], syz = s2[5];
+        const R third = drho / R(3);
+        P[0] = sxx - third - rho * ec.uu[0];
+        P[1] = syy - third - rho * ec.uu[1];
+        P[2] = szz - third - rho * ec.uu[2];
+        P[3] = sxy - rho * ec.uu[3];
+        P[4] = sxz - rho * ec.uu[4];
+        P[5] = syz - rho * ec.uu[5];
+        if (ORDER == 4) {
+#pragma unroll
+            for (int c = 0; c < 6; ++c)
+                P[c] -= rho * R(20.25) *
+                        (R(a.m4[c * 3 + 0]) * ec.a4[0] + R(a.m4[c * 3 + 1]) * ec.a4[1] + R(a.m4[c * 3 + 2]) * ec.a4[2]);
+        }
+        if (CUBIC) {
+#pragma unroll
+            for (int c = 0; c < 6; ++c) P[c] += R(0.5) * G[c];
+        }
+    }
+    R A2[6];
+    if (OP == OP_HRR) {
+        const R sg = nb ? R(a.sigma) : R(1);
+        const R fd = (R(1) - sg) * (R(-2) * rho / (R(3) * omega));
+#pragma unroll
+        for (int c = 0; c < 6; ++c) A2[c] = sg * P[c] + fd * S[c];
+    } else {
+#pragma unroll
+        for (int c = 0; c < 6; ++c) A2[c] = P[c];
+    }
+    NeqCoef<R, ORDER> nc;
+    nc.set(A2, u, kappa);
+    // post-collision f_q = feq_q + (1 - omega) neq_q [+ dt/2 psi_q]: one
+    // Hermite polynomial per direction with the merged coefficients
+    // rho * (equilibrium) + (1 - omega) * (recursive non-equilibrium)
+    // [+ G / 2 in the second order for the cubic-Mach correction]
+    const R om1 = R(1) - omega;
+    EqCoef<R, ORDER> mc;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) mc.u[c] = rho * u[c];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) mc.uu[c] = rho * ec.uu[c] + om1 * nc.A[c] + (CUBIC ? R(0.5) * G[c] : R(0));
+    if (ORDER >= 3) {
+#pragma unroll
+        for (int c = 0; c < 6; ++c) mc.a3[c] = rho * ec.a3[c] + om1 * nc.a3[c];
+    }
+    if (ORDER == 4) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) mc.a4[c] = rho * ec.a4[c] + om1 * nc.a4[c];
+    }
+#pragma unroll
+    for (int q = 0; q < Q; ++q) emit(q, R(wq(q)) * (drho + mc.poly(q, kappa)));
+}
+
 template <typename R, int OP, int ORDER, bool CUBIC, bool MRTWB>
 struct Collider {
-    // nb: strain S and cubic-Mach gradient G of the node (12 values), or null
-    // for a coupling node, whose neighbours are not all on its level: there the
-    // hybrid operator falls back to the population-based Pi1 (sigma = 1) and
-    // the cubic-Mach correction is dropped
+    // nb: as for regularisedEmit
     template <typename ST, typename Emit>
     __device__ __forceinline__ static void run(R* g, const LevelArgs<ST>& a, const R* nb, Emit& emit) {
         if ((OP == OP_MRT_GS || OP == OP_MRT_RM) && !MRTWB) {
@@ -206,10 +306,9 @@ struct Collider {
             return;
         }
 
-        EqCoef<R, ORDER> ec;
-        ec.set(u, kappa);
-
         if (OP == OP_SRT) {
+            EqCoef<R, ORDER> ec;
+            ec.set(u, kappa);
 #pragma unroll
             for (int q = 0; q < Q; ++q) {
                 const R geq = R(wq(q)) * (drho + rho * ec.poly(q, kappa));
@@ -218,85 +317,11 @@ struct Collider {
             return;
         }
 
-        // RR / HRR.  Strain rate S and cubic-Mach gradient G from the
-        // neighbours (null for coupling nodes).
-        R S[6] = {0, 0, 0, 0, 0, 0};
-        R G[6] = {0, 0, 0, 0, 0, 0};
-        if ((OP == OP_HRR || CUBIC) && nb) {
-#pragma unroll
-            for (int c = 0; c < 6; ++c) {
-                S[c] = nb[c];
-                G[c] = nb[6 + c];
-            }
-        }
-        // Pi1 = sum_q H2_q (g_q - geq_q [+ dt/2 psi_q]) (Node.cpp:2493-2558), with
-        // the equilibrium and correction parts summed in closed form by the
-        // fourth-order isotropy of D3Q19 (sum_q w_q H2_q,ab H2_q,cd =
-        // (d_ac d_bd + d_ad d_bc) / 9, odd moments vanish): sum_q H2_q geq_q =
-        // rho (u u + 20.25 M a4), M = sum_q w_q H2_q (x) H4_q(kappa) per case
-        // (zero unless ORDER == 4), and sum_q H2_q dt/2 psi_q = G / 2.
-        R P[6];
-        {
-            R sxx = 0, syy = 0, szz = 0, sxy = 0, sxz = 0, syz = 0;
-#pragma unroll
-            for (int q = 0; q < Q; ++q) {
-                if (ex(q)) sxx += g[q];
-                if (ey(q)) syy += g[q];
-                if (ez(q)) szz += g[q];
-                if (ex(q) * ey(q)) sxy += R(ex(q) * ey(q)) * g[q];
-                if (ex(q) * ez(q)) sxz += R(ex(q) * ez(q)) * g[q];
-                if (ey(q) * ez(q)) syz += R(ey(q) * ez(q)) * g[q];
-            }
-            const R third = drho / R(3);
-            P[0] = sxx - third - rho * ec.uu[0];
-            P[1] = syy - third - rho * ec.uu[1];
-            P[2] = szz - third - rho * ec.uu[2];
-            P[3] = sxy - rho * ec.uu[3];
-            P[4] = sxz - rho * ec.uu[4];
-            P[5] = syz - rho * ec.uu[5];
-            if (ORDER == 4) {
-#pragma unroll
-                for (int c = 0; c < 6; ++c)
-                    P[c] -= rho * R(20.25) *
-                            (R(a.m4[c * 3 + 0]) * ec.a4[0] + R(a.m4[c * 3 + 1]) * ec.a4[1] + R(a.m4[c * 3 + 2]) * ec.a4[2]);
-            }
-            if (CUBIC) {
-#pragma unroll
-                for (int c = 0; c < 6; ++c) P[c] += R(0.5) * G[c];
-            }
-        }
-        R A2[6];
-        if (OP == OP_HRR) {
-            const R sg = nb ? R(a.sigma) : R(1);
-            const R fd = (R(1) - sg) * (R(-2) * rho / (R(3) * omega));
-#pragma unroll
-            for (int c = 0; c < 6; ++c) A2[c] = sg * P[c] + fd * S[c];
-        } else {
-#pragma unroll
-            for (int c = 0; c < 6; ++c) A2[c] = P[c];
-        }
-        NeqCoef<R, ORDER> nc;
-        nc.set(A2, u, kappa);
-        // post-collision f_q = feq_q + (1 - omega) neq_q [+ dt/2 psi_q]: one
-        // Hermite polynomial per direction with the merged coefficients
-        // rho * (equilibrium) + (1 - omega) * (recursive non-equilibrium)
-        // [+ G / 2 in the second order for the cubic-Mach correction]
-        const R om1 = R(1) - omega;
-        EqCoef<R, ORDER> mc;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) mc.u[c] = rho * u[c];
-#pragma unroll
-        for (int c = 0; c < 6; ++c) mc.uu[c] = rho * ec.uu[c] + om1 * nc.A[c] + (CUBIC ? R(0.5) * G[c] : R(0));
-        if (ORDER >= 3) {
-#pragma unroll
-            for (int c = 0; c < 6; ++c) mc.a3[c] = rho * ec.a3[c] + om1 * nc.a3[c];
-        }
-        if (ORDER == 4) {
-#pragma unroll
-            for (int c = 0; c < 3; ++c) mc.a4[c] = rho * ec.a4[c] + om1 * nc.a4[c];
-        }
-#pragma unroll
-        for (int q = 0; q < Q; ++q) emit(q, R(wq(q)) * (drho + mc.poly(q, kappa)));
+        // RR / HRR: the post-collision state depends on the populations only
+        // through drho, u and the six second-order sums
+        R s2[6];
+        secondSums<R>(g, s2);
+        regularisedEmit<R, OP, ORDER, CUBIC>(drho, u, s2, a, nb, emit);
     }
 };
 
@@ -335,10 +360,10 @@ struct Pusher {
     template <typename V>
     __device__ __forceinline__ void operator()(int q, V v) const {
         if (q == 18) {
-            Store<S>::store(a.B + 18LL * a.N + n, v, scaleOf(a, 18));
+            Store<S>::store(a.B + (18 * a.Ni + n), v, scaleOf(a, 18));
         } else if (mask >> q & 1u) {
             const int t = n + o.dx[ex(q) + 1] + o.dy[ey(q) + 1] + o.dz[ez(q) + 1];
-            Store<S>::store(a.B + (long long)q * a.N + t, v, scaleOf(a, q));
+            Store<S>::store(a.B + (q * a.Ni + t), v, scaleOf(a, q));
         }
     }
 };
@@ -355,7 +380,7 @@ __global__ void __launch_bounds__(128) k_collide_push(LevelArgs<S> a) {
     if (code == CODE_DEAD) return;
     R g[Q];
 #pragma unroll
-    for (int q = 0; q < Q; ++q) g[q] = R(Store<S>::load(a.A + (long long)q * a.N + n, scaleOf(a, q)));
+    for (int q = 0; q < Q; ++q) g[q] = R(Store<S>::load(a.A + (q * a.Ni + n), scaleOf(a, q)));
     if (collides(code)) {
         Pusher<S> emit{a, n, c_pushMask[code], nbOffsets(a, i, j, k)};
         Collider<R, OP, ORDER, CUBIC, MRTWB>::run(g, a, (const R*)nullptr, emit);
@@ -370,34 +395,44 @@ __global__ void __launch_bounds__(128) k_collide_push(LevelArgs<S> a) {
 // collide + push for the operators that read the six axis neighbours'
 // pre-collision (rho, u): HRR (finite-difference strain rate, Node.cpp:1750-1889)
 // and RR with the cubic-Mach correction.  A block owns a TX x TY column of
-// nodes and marches through z; the moments of the planes z-1, z, z+1 of the
-// column and of its one-node ring are formed from the populations in shared
-// memory, so no moment array travels through HBM.  Planes of a periodic z axis
-// of at most three nodes are all resident at once.
-constexpr int TX = 32, TY = 8;
+// nodes and marches through z.  One pass over a plane loads each node's 19
+// populations once and forms everything the regularised collision needs:
+// drho and u of the tile and of its one-node ring go to shared memory (the
+// neighbours' strain stencil), the six second-order sums of the thread's own
+// node stay in registers until that plane collides.  The populations are not
+// loaded a second time: the post-collision state of RR / HRR depends on them
+// only through these ten moments.  Planes of a periodic z axis of at most
+// three nodes are all resident at once.
+#ifndef ACP_TILE_Y
+#define ACP_TILE_Y 8
+#endif
+constexpr int TX = 32, TY = ACP_TILE_Y;
 
+// drho, jx, jy, jz of a node's deviations
 template <typename S, typename R>
 __device__ __forceinline__ MomR<R> nodeMoments(const LevelArgs<S>& a, int n) {
     R d = 0, jx = 0, jy = 0, jz = 0;
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
-        const R g = R(Store<S>::load(a.A + (long long)q * a.N + n, scaleOf(a, q)));
+        const R g = R(Store<S>::load(a.A + (q * a.Ni + n), scaleOf(a, q)));
         d += g;
         jx += R(ex(q)) * g;
         jy += R(ey(q)) * g;
         jz += R(ez(q)) * g;
     }
     MomR<R> m;
-    m.rho = R(a.shift) + d;
-    const R inv = R(1) / m.rho;
+    m.drho = d;
+    const R inv = R(1) / (R(a.shift) + d);
     m.ux = jx * inv;
     m.uy = jy * inv;
     m.uz = jz * inv;
     return m;
 }
 
+// one plane of the tile: moments of the own node (with its second-order
+// sums into s2) and of the one-node ring into `slot`
 template <typename S, typename R>
-__device__ __forceinline__ void loadPlaneMoments(const LevelArgs<S>& a, MomR<R> (*slot)[TX + 2], int x0, int y0, int z) {
+__device__ __forceinline__ void planePass(const LevelArgs<S>& a, MomR<R> (*slot)[TX + 2], int x0, int y0, int z, R* s2) {
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
     // own node (on a periodic axis a thread past the end holds the wrapped
     // node, which is the neighbour of the last node of a partial tile)
@@ -405,7 +440,27 @@ __device__ __forceinline__ void loadPlaneMoments(const LevelArgs<S>& a, MomR<R> 
         const int i = wrapm(x0 + tx, a.nx, a.per[0]), j = wrapm(y0 + ty, a.ny, a.per[1]);
         if (i >= 0 && j >= 0) {
             const int n = (z * a.ny + j) * a.nx + i;
-            if (a.code[n] != CODE_DEAD) slot[ty + 1][tx + 1] = nodeMoments<S, R>(a, n);
+            if (a.code[n] != CODE_DEAD) {
+                R g[Q];
+#pragma unroll
+                for (int q = 0; q < Q; ++q) g[q] = R(Store<S>::load(a.A + (q * a.Ni + n), scaleOf(a, q)));
+                R d = 0, jx = 0, jy = 0, jz = 0;
+#pragma unroll
+                for (int q = 0; q < Q; ++q) {
+                    d += g[q];
+                    jx += R(ex(q)) * g[q];
+                    jy += R(ey(q)) * g[q];
+                    jz += R(ez(q)) * g[q];
+                }
+                secondSums<R>(g, s2);
+                MomR<R> m;
+                m.drho = d;
+                const R inv = R(1) / (R(a.shift) + d);
+                m.ux = jx * inv;
+                m.uy = jy * inv;
+                m.uz = jz * inv;
+                slot[ty + 1][tx + 1] = m;
+            }
         }
     }
     // one-node ring (axis neighbours only): bottom row, top row, left column, right column
@@ -430,7 +485,8 @@ __device__ __forceinline__ void loadPlaneMoments(const LevelArgs<S>& a, MomR<R> 
 // six axis neighbours' moments (+x, -x, +y, -y, +z, -z)
 template <typename R, bool STRAIN, bool CUBIC>
 __device__ __forceinline__ void neighbourTerms(const MomR<R>& mxp, const MomR<R>& mxm, const MomR<R>& myp,
-                                               const MomR<R>& mym, const MomR<R>& mzp, const MomR<R>& mzm, R* SG) {
+                                               const MomR<R>& mym, const MomR<R>& mzp, const MomR<R>& mzm, R shift,
+                                               R* SG) {
 #pragma unroll
     for (int c = 0; c < 12; ++c) SG[c] = 0;
     if (STRAIN) {
@@ -442,8 +498,8 @@ __device__ __forceinline__ void neighbourTerms(const MomR<R>& mxp, const MomR<R>
         SG[5] = R(0.25) * ((myp.uz - mym.uz) + (mzp.uy - mzm.uy));
     }
     if (CUBIC) {
-        auto psiT = [](const MomR<R>& m, R* P) {
-            const R r = m.rho, x = m.ux, y = m.uy, z = m.uz;
+        auto psiT = [shift](const MomR<R>& m, R* P) {
+            const R r = shift + m.drho, x = m.ux, y = m.uy, z = m.uz;
             P[0] = r * x * x * x;           // XXX
             P[1] = R(0.5) * r * y * z * z;  // XXY
             P[2] = R(0.5) * r * z * y * y;  // XXZ
@@ -470,74 +526,140 @@ __device__ __forceinline__ void neighbourTerms(const MomR<R>& mxp, const MomR<R>
 }
 
 // Register cap of the tiled kernel: blocks of 256 threads per SM for FP64 /
-// FP32 compute.  Measured on the 1024x512x3 HRR pulse, this per-plane form
-// (moments of planes z-1..z+1 in shared memory, own populations re-read from
-// L2 for the collision) beat both staging every plane's populations in shared
-// memory behind one barrier and a two-plane-deep software pipeline.
+// FP32 compute.
 #ifndef ACP_TILED_MINB_F64
 #define ACP_TILED_MINB_F64 2
 #endif
 #ifndef ACP_TILED_MINB_F32
-#define ACP_TILED_MINB_F32 3
+#define ACP_TILED_MINB_F32 4
 #endif
 template <typename R>
 struct TiledMinBlocks {
     static constexpr int value = sizeof(R) == 8 ? ACP_TILED_MINB_F64 : ACP_TILED_MINB_F32;
 };
 
+// collide + push of the thread's node of plane z: slots sc / sp / sn hold the
+// moments of planes z, z+1, z-1; s2 the node's second-order sums (null: form
+// them from the populations again)
+template <typename S, typename R, int OP, int ORDER, bool CUBIC>
+__device__ __forceinline__ void tiledNode(const LevelArgs<S>& a, MomR<R> (*sm)[TY + 2][TX + 2], int i, int j, int z,
+                                          int sc, int sp, int sn, const R* s2own) {
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int n = (z * a.ny + j) * a.nx + i;
+    const uint8_t code = a.code[n];
+    if (code == CODE_DEAD) return;
+    if (collides(code)) {
+        R s2buf[6];
+        const R* s2 = s2own;
+        if (!s2) {
+            R g[Q];
+#pragma unroll
+            for (int q = 0; q < Q; ++q) g[q] = R(Store<S>::load(a.A + (q * a.Ni + n), scaleOf(a, q)));
+            secondSums<R>(g, s2buf);
+            s2 = s2buf;
+        }
+        const MomR<R> me = sm[sc][ty + 1][tx + 1];
+        const R u[3] = {me.ux, me.uy, me.uz};
+        if (code >= CODE_IFACE0) {
+            Pusher<S> emit{a, n, c_pushMask[code], nbOffsets(a, i, j, z)};
+            regularisedEmit<R, OP, ORDER, CUBIC>(me.drho, u, s2, a, (const R*)nullptr, emit);
+        } else {
+            // fluid nodes are interior or on periodic axes: every axis neighbour exists
+            R SG[12];
+            neighbourTerms<R, OP == OP_HRR, CUBIC>(sm[sc][ty + 1][tx + 2], sm[sc][ty + 1][tx], sm[sc][ty + 2][tx + 1],
+                                                   sm[sc][ty][tx + 1], sm[sp][ty + 1][tx + 1], sm[sn][ty + 1][tx + 1],
+                                                   R(a.shift), SG);
+            Pusher<S> emit{a, n, 0x3FFFFu, nbOffsets(a, i, j, z)};
+            regularisedEmit<R, OP, ORDER, CUBIC>(me.drho, u, s2, a, SG, emit);
+        }
+    } else {
+        // LODI boundary node: pushes its uncollided populations inward
+        Pusher<S> emit{a, n, c_pushMask[code], nbOffsets(a, i, j, z)};
+#pragma unroll
+        for (int q = 0; q < Q; ++q) emit(q, R(Store<S>::load(a.A + (q * a.Ni + n), scaleOf(a, q))));
+    }
+}
+
+// plane slots of the tiled kernel: four rolling ones (the pass over plane
+// z+2 never overwrites a plane that a slower warp still reads for plane z,
+// so one barrier per plane suffices), plus (FP32 compute) two that keep the
+// first and last plane of a periodic column resident, so a block that owns a
+// whole periodic z column passes over each plane once
+template <typename R>
+struct TiledSlots {
+    static constexpr int value = sizeof(R) == 4 ? 6 : 4;
+};
+
 template <typename S, typename R, int OP, int ORDER, bool CUBIC>
 __global__ void __launch_bounds__(TX * TY, TiledMinBlocks<R>::value) k_collide_push_tiled(LevelArgs<S> a, int zChunk) {
-    __shared__ MomR<R> sm[3][TY + 2][TX + 2];
-    const int tx = threadIdx.x, ty = threadIdx.y;
+    __shared__ MomR<R> sm[TiledSlots<R>::value][TY + 2][TX + 2];
     const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
-    const int i = x0 + tx, j = y0 + ty;
-    const int zBeg = blockIdx.z * zChunk;
-    const int zEnd = min(a.nz, zBeg + zChunk);
-    const bool allResident = a.per[2] && a.nz <= 3;
-    // rolling planes: slot of the unwrapped plane u in [zBeg-1, zEnd] is (u - zBeg + 1) mod 3
-    auto key = [&](int u) { return (u - zBeg + 1) % 3; };
-    if (allResident) {
-        for (int z = 0; z < a.nz; ++z) loadPlaneMoments<S, R>(a, sm[z], x0, y0, z);
-    } else {
-        const int zm = wrapc(zBeg - 1, a.nz, a.per[2]);
-        if (zm >= 0) loadPlaneMoments<S, R>(a, sm[key(zBeg - 1)], x0, y0, zm);
-        loadPlaneMoments<S, R>(a, sm[key(zBeg)], x0, y0, zBeg);
-    }
-    for (int z = zBeg; z < zEnd; ++z) {
-        if (!allResident) {
-            const int zp = wrapc(z + 1, a.nz, a.per[2]);
-            if (zp >= 0) loadPlaneMoments<S, R>(a, sm[key(z + 1)], x0, y0, zp);
-        }
+    const int i = x0 + threadIdx.x, j = y0 + threadIdx.y;
+    const bool mine = i < a.nx && j < a.ny;
+    if (a.per[2] && a.nz <= 3) {
+        // every plane resident: one pass per plane, then the collisions; the
+        // second-order sums of all planes stay in registers in the FP32 form,
+        // the FP64 form forms them again at the collision (register budget)
+        constexpr bool keep = sizeof(R) == 4;
+        R s2[3][6];
+#pragma unroll
+        for (int z = 0; z < 3; ++z)
+            if (z < a.nz) planePass<S, R>(a, sm[z], x0, y0, z, s2[z]);
         __syncthreads();
-        if (i < a.nx && j < a.ny) {
-            const int n = (z * a.ny + j) * a.nx + i;
-            const uint8_t code = a.code[n];
-            if (code != CODE_DEAD) {
-                R g[Q];
+        if (mine) {
 #pragma unroll
-                for (int q = 0; q < Q; ++q) g[q] = R(Store<S>::load(a.A + (long long)q * a.N + n, scaleOf(a, q)));
-                if (code >= CODE_IFACE0) {
-                    Pusher<S> emit{a, n, c_pushMask[code], nbOffsets(a, i, j, z)};
-                    Collider<R, OP, ORDER, CUBIC, false>::run(g, a, (const R*)nullptr, emit);
-                } else if (code == CODE_FLUID) {
-                    // fluid nodes are interior or on periodic axes: every axis neighbour exists
-                    const int sc = allResident ? z : key(z);
-                    const int sp = allResident ? wrapm(z + 1, a.nz, 1) : key(z + 1);
-                    const int sn = allResident ? wrapm(z - 1, a.nz, 1) : key(z - 1);
-                    R SG[12];
-                    neighbourTerms<R, OP == OP_HRR, CUBIC>(sm[sc][ty + 1][tx + 2], sm[sc][ty + 1][tx],
-                                                           sm[sc][ty + 2][tx + 1], sm[sc][ty][tx + 1],
-                                                           sm[sp][ty + 1][tx + 1], sm[sn][ty + 1][tx + 1], SG);
-                    Pusher<S> emit{a, n, 0x3FFFFu, nbOffsets(a, i, j, z)};
-                    Collider<R, OP, ORDER, CUBIC, false>::run(g, a, SG, emit);
-                } else {
-                    Pusher<S> emit{a, n, c_pushMask[code], nbOffsets(a, i, j, z)};
+            for (int z = 0; z < 3; ++z)
+                if (z < a.nz)
+                    tiledNode<S, R, OP, ORDER, CUBIC>(a, sm, i, j, z, z, wrapm(z + 1, a.nz, 1), wrapm(z - 1, a.nz, 1),
+                                                      keep ? s2[z] : (const R*)nullptr);
+        }
+        return;
+    }
+    R cur[6], nxt[6];
+    if (TiledSlots<R>::value == 6 && a.per[2] && zChunk >= a.nz) {
+        // whole periodic column: planes 0 and nz-1 in slots 4 and 5, planes
+        // 1..nz-2 rolling through slots p mod 4; the last plane's own sums
+        // wait in shared memory
+        __shared__ R lastS2[6][TY][TX];
+        const int nz = a.nz;
+        const int tx = threadIdx.x, ty = threadIdx.y;
+        auto slot = [nz](int p) { return p == 0 ? 4 : (p == nz - 1 ? 5 : (p & 3)); };
+        planePass<S, R>(a, sm[5], x0, y0, nz - 1, nxt);
 #pragma unroll
-                    for (int q = 0; q < Q; ++q) emit(q, g[q]);
-                }
+        for (int c = 0; c < 6; ++c) lastS2[c][ty][tx] = nxt[c];
+        planePass<S, R>(a, sm[4], x0, y0, 0, cur);
+        for (int z = 0; z < nz; ++z) {
+            if (z + 1 <= nz - 2) planePass<S, R>(a, sm[slot(z + 1)], x0, y0, z + 1, nxt);
+            __syncthreads();
+            if (mine)
+                tiledNode<S, R, OP, ORDER, CUBIC>(a, sm, i, j, z, slot(z), slot(z + 1 == nz ? 0 : z + 1),
+                                                  slot(z == 0 ? nz - 1 : z - 1), cur);
+            if (z + 1 == nz - 1) {
+#pragma unroll
+                for (int c = 0; c < 6; ++c) cur[c] = lastS2[c][ty][tx];
+            } else {
+#pragma unroll
+                for (int c = 0; c < 6; ++c) cur[c] = nxt[c];
             }
         }
-        __syncthreads();  // the slot of z-1 is refilled with z+2 next
+        return;
+    }
+    const int zBeg = blockIdx.z * zChunk;
+    const int zEnd = min(a.nz, zBeg + zChunk);
+    // rolling planes: slot of the unwrapped plane u in [zBeg-1, zEnd] is (u - zBeg + 1) mod 4
+    auto key = [&](int u) { return (u - zBeg + 1) & 3; };
+    {
+        const int zm = wrapc(zBeg - 1, a.nz, a.per[2]);
+        if (zm >= 0) planePass<S, R>(a, sm[key(zBeg - 1)], x0, y0, zm, nxt);  // ring and moments only
+        planePass<S, R>(a, sm[key(zBeg)], x0, y0, zBeg, cur);
+    }
+    for (int z = zBeg; z < zEnd; ++z) {
+        const int zp = wrapc(z + 1, a.nz, a.per[2]);
+        if (zp >= 0) planePass<S, R>(a, sm[key(z + 1)], x0, y0, zp, nxt);
+        __syncthreads();
+        if (mine) tiledNode<S, R, OP, ORDER, CUBIC>(a, sm, i, j, z, key(z), key(z + 1), key(z - 1), cur);
+#pragma unroll
+        for (int c = 0; c < 6; ++c) cur[c] = nxt[c];
     }
 }
 
