@@ -57,6 +57,8 @@ struct acp_handle {
     // two-level coupling (fine state always in array 0 between coarse steps)
     std::vector<C2FDev> c2fHost;
     std::vector<F2CDev> f2cHost;
+    std::vector<DCDev> dcHost;  // direct coupling: the shared nodes
+    DCDev* dDC = nullptr;
     int nCoinc = 0, nMid = 0, nCen = 0;
     C2FDev* dC2F = nullptr;
     F2CDev* dF2C = nullptr;
@@ -212,9 +214,10 @@ int validate(const acp_case_desc* d, std::string& why) {
             why = "two-level cases use the box layout (Refinement-Layout BOX)";
             return ACP_ERR_UNSUPPORTED;
         }
-        if (d->coupling != ACP_COUPLING_STD || d->overlap != 1) {
-            why = "the direct-coupling schemes (Overlap 0) are not built; use STD with Overlap 1";
-            return ACP_ERR_UNSUPPORTED;
+        if (d->coupling < ACP_COUPLING_STD || d->coupling > ACP_COUPLING_DC2) { why = "unknown coupling approach"; return ACP_ERR_INVALID; }
+        if ((d->coupling == ACP_COUPLING_STD) != (d->overlap == 1)) {
+            why = "Coupling-Approach STD needs Overlap 1, DC1 and DC2 need Overlap 0";
+            return ACP_ERR_INVALID;
         }
         bool spans[3];
         for (int a = 0; a < 3; ++a) {
@@ -328,6 +331,8 @@ uint32_t replaceMask(int mode, const int* f) {
 int buildTwoLevel(acp_handle* h) {
     const acp_case_desc& d = h->d;
     const int dom[3] = {d.nx, d.ny, d.nz};
+    const bool direct = d.coupling != ACP_COUPLING_STD;
+    const int ov = direct ? 0 : 1;
     int lo[3], hi[3], loIf[3], hiIf[3], spans[3];
     for (int a = 0; a < 3; ++a) {
         lo[a] = d.box_lo[a];
@@ -349,8 +354,9 @@ int buildTwoLevel(acp_handle* h) {
                 const int c[3] = {i, j, k};
                 bool dead = true, inner = true;
                 for (int a = 0; a < 3; ++a) {
-                    const int dlo = loIf[a] ? lo[a] + 2 : lo[a], dhi = hiIf[a] ? hi[a] - 2 : hi[a];
-                    const int ilo = loIf[a] ? lo[a] + 1 : lo[a], ihi = hiIf[a] ? hi[a] - 1 : hi[a];
+                    // coupling nodes one cell inside the box (STD, Overlap 1) or on its faces (DC, Overlap 0)
+                    const int dlo = loIf[a] ? lo[a] + 1 + ov : lo[a], dhi = hiIf[a] ? hi[a] - 1 - ov : hi[a];
+                    const int ilo = loIf[a] ? lo[a] + ov : lo[a], ihi = hiIf[a] ? hi[a] - ov : hi[a];
                     if (c[a] < dlo || c[a] > dhi) dead = false;
                     if (c[a] < ilo || c[a] > ihi) inner = false;
                 }
@@ -413,7 +419,8 @@ int buildTwoLevel(acp_handle* h) {
                 C2FDev cn;
                 cn.n = (int)n;
                 cn.src = -1;
-                cn.mask = replaceMask(d.c2f_replace, f);
+                // the direct coupling never overwrites the fine populations that only the fine level has
+                cn.mask = replaceMask(direct && d.c2f_replace == ACP_C2F_FALL ? ACP_C2F_MFP : d.c2f_replace, f);
                 for (int m = 0; m < 4; ++m) { cn.st[m] = -1; cn.w[m] = 0.f; }
                 if (nodd == 0) {
                     int cc[3];
@@ -451,7 +458,68 @@ int buildTwoLevel(acp_handle* h) {
     h->c2fHost.insert(h->c2fHost.end(), mid.begin(), mid.end());
     h->c2fHost.insert(h->c2fHost.end(), cen.begin(), cen.end());
     h->f2cHost.clear();
-    for (int k = 0; k < C.nz; ++k)
+    h->dcHost.clear();
+    if (direct) {
+        // the shared nodes, in the order of the coincident C2F nodes
+        auto liveIn = [](const LevelHost& L, const int* c) {
+            int cc[3];
+            const int dd[3] = {L.nx, L.ny, L.nz};
+            for (int a = 0; a < 3; ++a) {
+                cc[a] = c[a];
+                if (cc[a] < 0 || cc[a] >= dd[a]) {
+                    if (!L.per[a]) return -1LL;
+                    cc[a] = (cc[a] % dd[a] + dd[a]) % dd[a];
+                }
+            }
+            const long long n = ((long long)cc[2] * L.ny + cc[1]) * L.nx + cc[0];
+            return L.code[n] == CODE_DEAD ? -1LL : n;
+        };
+        const uint32_t all = (1u << Q) - 1u;
+        const double w1[3] = {0.25, 0.5, 0.25};
+        for (const C2FDev& cn : coinc) {
+            DCDev dn;
+            dn.nf = cn.n;
+            dn.nc = cn.src;
+            const int cf[3] = {(int)(cn.n % F.nx), (int)((cn.n / F.nx) % F.ny), (int)(cn.n / ((long long)F.nx * F.ny))};
+            const int cc[3] = {(int)(cn.src % C.nx), (int)((cn.src / C.nx) % C.ny),
+                               (int)(cn.src / ((long long)C.nx * C.ny))};
+            dn.vc = dn.vf = 0;
+            for (int q = 0; q < Q; ++q) {
+                const int sc[3] = {cc[0] - ex(q), cc[1] - ey(q), cc[2] - ez(q)};
+                const int sf[3] = {cf[0] - ex(q), cf[1] - ey(q), cf[2] - ez(q)};
+                if (liveIn(C, sc) >= 0) dn.vc |= 1u << q;
+                if (liveIn(F, sf) >= 0) dn.vf |= 1u << q;
+            }
+            const uint32_t both = dn.vc & dn.vf;
+            dn.rc = (~dn.vc & all) | (d.f2c_replace != ACP_F2C_MC ? both : 0u);
+            dn.rf = (~dn.vf & all) | (d.c2f_replace != ACP_C2F_MF ? both : 0u);
+            int fa = 0;
+            for (int a = 0; a < 3; ++a)
+                if ((loIf[a] && cf[a] == 0) || (hiIf[a] && cf[a] == fd[a] - 1)) { fa = a; break; }
+            const int b1 = fa == 0 ? 1 : 0, b2 = fa == 2 ? 1 : 2;
+            double wsum = 0;
+            for (int m = 0; m < 9; ++m) {
+                const int d1 = m % 3 - 1, d2 = m / 3 - 1;
+                int c2[3] = {cf[0], cf[1], cf[2]};
+                c2[b1] += d1;
+                c2[b2] += d2;
+                const long long t = liveIn(F, c2);
+                const bool ok = t >= 0 && F.code[t] >= CODE_IFACE0;
+                double w = 0;
+                if (ok) {
+                    if (d.f2c_filter == ACP_F2C_NOFI) w = m == 4 ? 1. : 0.;
+                    else if (d.f2c_filter == ACP_F2C_LAG) w = 1.;
+                    else w = w1[d1 + 1] * w1[d2 + 1];
+                }
+                dn.plane[m] = ok && w > 0 ? (int)t : -1;
+                dn.w[m] = dn.plane[m] >= 0 ? w : 0.;
+                wsum += dn.w[m];
+            }
+            for (int m = 0; m < 9; ++m) dn.w[m] /= wsum;
+            h->dcHost.push_back(dn);
+        }
+    }
+    for (int k = 0; k < C.nz && !direct; ++k)
         for (int j = 0; j < C.ny; ++j)
             for (int i = 0; i < C.nx; ++i) {
                 const long long n = ((long long)k * C.ny + j) * C.nx + i;
@@ -700,7 +768,8 @@ CouplingArgs couplingArgs(const acp_handle* h) {
 }
 
 // C2F onto the fine array `fdst` from the coarse array `cnew` (blended with
-// the saved coarse state by weight 1 - th)
+// the saved coarse state by weight 1 - th); with the direct coupling the
+// shared nodes are coupled both ways (th == 1) or towards the fine level
 template <typename S, typename R>
 void enqueueC2F(acp_handle* h, int cnew, int fdst, R th) {
     LevelArgs<S> la = levelArgs<S>(h, 1, 0);
@@ -709,7 +778,14 @@ void enqueueC2F(acp_handle* h, int cnew, int fdst, R th) {
     S* Ff = (S*)h->dev[1].f[fdst];
     const R* pre = (const R*)h->dPre;
     const int o = h->d.eq_order;
-    if (h->nCoinc) {
+    if (h->nCoinc && !h->dcHost.empty()) {
+        const unsigned g = (h->nCoinc + 127) / 128;
+        S* Bw = (S*)h->dev[0].f[cnew];
+        const int dc2 = h->d.coupling == ACP_COUPLING_DC2;
+        if (o == 2) k_dc_couple<S, R, 2><<<g, 128, 0, h->stream>>>(Bw, Ff, h->dDC, h->nCoinc, pre, th, dc2, c, la);
+        else if (o == 3) k_dc_couple<S, R, 3><<<g, 128, 0, h->stream>>>(Bw, Ff, h->dDC, h->nCoinc, pre, th, dc2, c, la);
+        else k_dc_couple<S, R, 4><<<g, 128, 0, h->stream>>>(Bw, Ff, h->dDC, h->nCoinc, pre, th, dc2, c, la);
+    } else if (h->nCoinc) {
         const unsigned g = (h->nCoinc + 127) / 128;
         if (o == 2) k_c2f_coincident<S, R, 2><<<g, 128, 0, h->stream>>>(Bc, Ff, h->dC2F, h->nCoinc, pre, th, c, la);
         else if (o == 3) k_c2f_coincident<S, R, 3><<<g, 128, 0, h->stream>>>(Bc, Ff, h->dC2F, h->nCoinc, pre, th, c, la);
@@ -742,7 +818,7 @@ int enqueueStepT(acp_handle* h, int src, PhaseTimer* tm) {
         if (tm) tm->mark(ACP_K_COUPLING);
         enqueueLevelStep<S, R>(h, 1, 1, tm);    // fine t+1/2 -> t+1
         if (tm) tm->mark(-1);
-        if (!h->f2cHost.empty()) {
+        if (!h->f2cHost.empty()) {  // STD only: the direct coupling does F2C in its t+1 pass
             LevelArgs<S> lf = levelArgs<S>(h, 1, 0);
             const unsigned g = ((unsigned)h->f2cHost.size() * 32 + 127) / 128;  // a warp per coarse node
             const S* Ff = (const S*)h->dev[1].f[0];
@@ -872,7 +948,7 @@ size_t estimateBytes(const acp_case_desc& d) {
         // coupling lists and the saved coarse populations
         const size_t rb = d.storage == ACP_STORE_F64 ? 8 : 4;
         return (size_t)nodes * per + (size_t)surf * sizeof(BNodeDev) +
-               (size_t)fsurf * (sizeof(C2FDev) + sizeof(F2CDev) / 4 + Q * rb);
+               (size_t)fsurf * (sizeof(C2FDev) + sizeof(F2CDev) / 4 + sizeof(DCDev) / 4 + Q * rb);
     }
     return (size_t)nodes * per + (size_t)surf * sizeof(BNodeDev);
 }
@@ -1026,6 +1102,11 @@ int acp_create(const acp_case_desc* d, int device, acp_handle** out) {
                                   cudaMemcpyHostToDevice, h->stream));
         }
         if (h->nCoinc && (s = devAlloc(h, &h->dPre, (size_t)h->nCoinc * Q * rb))) return s;
+        if (!h->dcHost.empty()) {
+            if ((s = devAlloc(h, (void**)&h->dDC, h->dcHost.size() * sizeof(DCDev)))) return s;
+            CU(h, cudaMemcpyAsync(h->dDC, h->dcHost.data(), h->dcHost.size() * sizeof(DCDev), cudaMemcpyHostToDevice,
+                                  h->stream));
+        }
         if (!h->f2cHost.empty()) {
             if ((s = devAlloc(h, (void**)&h->dF2C, h->f2cHost.size() * sizeof(F2CDev)))) return s;
             CU(h, cudaMemcpyAsync(h->dF2C, h->f2cHost.data(), h->f2cHost.size() * sizeof(F2CDev),
@@ -1343,6 +1424,7 @@ int acp_destroy(acp_handle* h) {
     cudaFree(h->dErr);
     cudaFree(h->dC2F);
     cudaFree(h->dF2C);
+    cudaFree(h->dDC);
     cudaFree(h->dPre);
     cudaFree(h->dProbeNodes);
     cudaFree(h->dSeries);

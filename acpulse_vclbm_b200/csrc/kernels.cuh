@@ -1042,4 +1042,129 @@ __global__ void k_f2c(const S* __restrict__ Ff, S* Bc, const F2CDev* __restrict_
         if (nd.mask >> q & 1u) Store<S>::store(Bc + (long long)q * c.Nc + nd.n, geq[q] + neq[q], la.hscale[q]);
 }
 
+// ---------------------------------------------------------------------------
+// direct coupling (Coupling-Approach DC1 / DC2, Overlap 0).  The reference
+// declares interpolTimeDirectCoupling / directCoupling (GridCoupling.h:28-29,
+// called at Lattice.cpp:14018-14058 and 14699-14739) without bodies.  Here the
+// coarse nodes on the box faces and the fine nodes at coarse positions there
+// are the same points; every population is taken from the level on which its
+// source node is live, the equilibrium is that of this merged set, and each
+// level's replaced populations get it plus the other level's rescaled
+// non-equilibrium: population-wise (DC1) or regularised onto the
+// second-order Hermite tensor (DC2).
+struct DCDev {
+    int nf, nc;                 // the shared node on the fine and the coarse level
+    uint32_t vc, vf;            // populations whose source node is live on the coarse / fine level
+    uint32_t rc, rf;            // populations replaced on the coarse / fine level
+    int plane[9];               // 3x3 fine stencil in the interface plane (-1: none)
+    double w[9];                // F2C filter weights over the stencil (normalised)
+};
+
+// 4.5 w_q H2_q : Pi, Pi = sum_q H2_q neq_q (lattice units)
+template <typename R>
+__device__ __forceinline__ void regulariseNeq(const R* neq, R* out) {
+    R P[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        P[0] += h2xx<R>(q) * neq[q];
+        P[1] += h2yy<R>(q) * neq[q];
+        P[2] += h2zz<R>(q) * neq[q];
+        P[3] += R(ex(q) * ey(q)) * neq[q];
+        P[4] += R(ex(q) * ez(q)) * neq[q];
+        P[5] += R(ey(q) * ez(q)) * neq[q];
+    }
+#pragma unroll
+    for (int q = 0; q < Q; ++q) out[q] = R(4.5) * R(wq(q)) * h2dot<R>(q, P);
+}
+
+// th < 1: the fine side at t+1/2 (coarse state blended in time with the
+// saved pre-step state); th == 1: both sides at t+1.  One thread per shared node.
+template <typename S, typename R, int ORDER>
+__global__ void k_dc_couple(S* Bc, S* Ff, const DCDev* __restrict__ nodes, int count, const R* __restrict__ pre,
+                            R th, int dc2, CouplingArgs c, LevelArgs<S> la) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    const DCDev& nd = nodes[t];
+    const bool full = th == R(1);
+    R cp[Q], X[Q], eq[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) cp[q] = R(Store<S>::load(Bc + (long long)q * c.Nc + nd.nc, la.hscale[q]));
+    // populations whose source node is live on neither level keep the coarse
+    // state of t (complete after the previous exchange): no population that a
+    // level leaves unwritten is ever read
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        if (nd.vc >> q & 1u) {
+            X[q] = (R(1) - th) * pre[(long long)q * count + t] + th * cp[q];
+        } else if (full && (nd.vf >> q & 1u)) {
+            X[q] = R(Store<S>::load(Ff + (long long)q * c.Nf + nd.nf, la.hscale[q]));
+        } else {
+            X[q] = pre[(long long)q * count + t];
+        }
+    }
+    eqSplit<R, ORDER>(X, R(c.shiftC), R(c.kappa), eq);
+    const R aF2C = R(c.alphaF2C), aC2F = R(c.alphaC2F);
+    // t+1: the fine populations filtered over the interface plane, gathered
+    // before this thread overwrites the shared node's fine populations (the
+    // stencil's other nodes are hanging fine nodes, which this kernel does
+    // not write)
+    R ff[Q];
+    if (full) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            R acc = 0;
+            for (int m = 0; m < 9; ++m)
+                if (nd.plane[m] >= 0)
+                    acc += R(nd.w[m]) * R(Store<S>::load(Ff + (long long)q * c.Nf + nd.plane[m], la.hscale[q]));
+            ff[q] = acc;
+        }
+    }
+    // fine side
+    {
+        R neq[Q], sc[Q];
+        if (dc2) {
+#pragma unroll
+            for (int q = 0; q < Q; ++q) {
+                const bool fineScaled = full && !(nd.vc >> q & 1u) && (nd.vf >> q & 1u);
+                neq[q] = (fineScaled ? aF2C : R(1)) * (X[q] - eq[q]);
+            }
+            regulariseNeq<R>(neq, sc);
+#pragma unroll
+            for (int q = 0; q < Q; ++q)
+                if (nd.rf >> q & 1u) Store<S>::store(Ff + (long long)q * c.Nf + nd.nf, eq[q] + aC2F * sc[q], la.hscale[q]);
+        } else {
+#pragma unroll
+            for (int q = 0; q < Q; ++q) neq[q] = X[q] - eq[q];
+            rescaleNeq<R>(neq, c, true);
+#pragma unroll
+            for (int q = 0; q < Q; ++q)
+                if (nd.rf >> q & 1u)
+                    Store<S>::store(Ff + (long long)q * c.Nf + nd.nf, (nd.vc >> q & 1u) ? eq[q] + neq[q] : eq[q],
+                                    la.hscale[q]);
+        }
+    }
+    if (!full) return;
+    // coarse side: fine non-equilibrium; the fine-missing populations take the
+    // coarse one brought to the fine scale
+    R neq[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) neq[q] = (nd.vf >> q & 1u) ? ff[q] - eq[q] : aC2F * (X[q] - eq[q]);
+    if (dc2) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) neq[q] *= aF2C;
+        R sc[Q];
+        regulariseNeq<R>(neq, sc);
+#pragma unroll
+        for (int q = 0; q < Q; ++q)
+            if (nd.rc >> q & 1u) Store<S>::store(Bc + (long long)q * c.Nc + nd.nc, eq[q] + sc[q], la.hscale[q]);
+    } else {
+        rescaleNeq<R>(neq, c, false);
+#pragma unroll
+        for (int q = 0; q < Q; ++q)
+            if (nd.rc >> q & 1u)
+                Store<S>::store(Bc + (long long)q * c.Nc + nd.nc, (nd.vf >> q & 1u) ? eq[q] + neq[q] : eq[q],
+                                la.hscale[q]);
+    }
+}
+
 }  // namespace acp

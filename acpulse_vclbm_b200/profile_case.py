@@ -24,6 +24,7 @@ def main():
     ap.add_argument("--levels", type=int, default=1, choices=[1, 2],
                     help="2: refine the right half 2:1 (the sweep configuration's layout)")
     ap.add_argument("--filter", default="LAG")
+    ap.add_argument("--coupling", default="STD", choices=["STD", "DC1", "DC2"])
     a = ap.parse_args()
     d = lattice_units_case(a.nx, a.ny, a.nz, op=a.op, nu_lu=1e-4, order=a.order, periodic=(False, True, True),
                            eps=1e-3, b=24.0, center=(a.nx / 4.0, a.ny / 2.0, 1.0), storage=a.storage)
@@ -35,6 +36,12 @@ def main():
         d.box_lo[:] = [a.nx // 2, 0, 0]
         d.box_hi[:] = [a.nx - 1, a.ny - 1, a.nz - 1]
         d.f2c_filter = F2C_FILTER[a.filter]
+        if a.coupling != "STD":
+            from .capi import C2F_REPLACE, COUPLING, F2C_REPLACE
+            d.coupling = COUPLING[a.coupling]
+            d.overlap = 0
+            d.c2f_replace = C2F_REPLACE["Mf"]
+            d.f2c_replace = F2C_REPLACE["Mc"]
     L = engine.Lattice(d).init()
     L.step(a.steps)
     L.sync()

@@ -50,6 +50,7 @@ def parse():
     ap.add_argument("--nu", type=float, default=1e-4)
     ap.add_argument("--levels", type=int, default=2, choices=[1, 2])
     ap.add_argument("--filter", default="LAG")
+    ap.add_argument("--coupling", default="STD", choices=["STD", "DC1", "DC2"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -68,6 +69,12 @@ def workload(args, storage):
         d.box_lo[:] = [args.nx // 2, 0, 0]
         d.box_hi[:] = [args.nx - 1, args.ny - 1, args.nz - 1]
         d.f2c_filter = F2C_FILTER[args.filter]
+        if args.coupling != "STD":
+            from acpulse_vclbm_b200.capi import C2F_REPLACE, COUPLING, F2C_REPLACE
+            d.coupling = COUPLING[args.coupling]
+            d.overlap = 0
+            d.c2f_replace = C2F_REPLACE["Mf"]
+            d.f2c_replace = F2C_REPLACE["Mc"]
     return d
 
 
@@ -76,13 +83,14 @@ def updates_per_step(desc):
     if desc.max_level == 0:
         return desc.nx * desc.ny * desc.nz
     nx, ny, nz = desc.nx, desc.ny, desc.nz
-    coarse = (desc.box_lo[0] + 2) * ny * nz
+    coarse = (desc.box_lo[0] + 1 + desc.overlap) * ny * nz
     fine = (2 * (desc.box_hi[0] - desc.box_lo[0]) + 1) * 2 * ny * 2 * nz
     return coarse + 2 * fine
 
 
 def config_of(args):
-    lv = (f"right half (x >= {args.nx // 2}) refined 2:1, overlap 1, {args.filter} restriction"
+    scheme = "overlap 1" if args.coupling == "STD" else f"direct coupling {args.coupling}"
+    lv = (f"right half (x >= {args.nx // 2}) refined 2:1, {scheme}, {args.filter} restriction"
           if args.levels == 2 else "single level")
     return {"workload": f"quasi-2D Gaussian pulse, {args.nx}x{args.ny}x{args.nz} coarse nodes, {lv}, "
                         f"periodic y/z, LODI x faces, {args.op} order 3, nu={args.nu:g} lu, eps=1e-3, b=24",

@@ -192,6 +192,19 @@ struct Oracle {
     };
     std::vector<C2FNode> c2f;   // ordered: coincident, mid, centre
     std::vector<F2CNode> f2c;
+    // direct coupling (Coupling-Approach DC1 / DC2, Overlap 0): the coarse
+    // nodes on the box faces and the fine nodes at coarse positions there
+    // are the same points; each population is taken from the level on which
+    // its source node is live
+    struct DCNode {
+        long nf, nc;            // the shared node on the fine and the coarse level
+        unsigned vc, vf;        // populations whose source node is live on the coarse / fine level
+        unsigned rc, rf;        // populations replaced on the coarse / fine level
+        long plane[9];          // 3x3 fine stencil in the interface plane (-1: none), [4] = nf
+        double w[9];            // F2C filter weights over the stencil (normalised)
+    };
+    std::vector<DCNode> dc;     // one per coincident C2F node, same order
+    bool isDC() const { return desc.coupling != ACP_COUPLING_STD; }
     std::vector<double> pre;    // coarse populations before the coarse step, per coincident C2F node
     int boxLo[3], boxHi[3], loIf[3], hiIf[3], spans[3];
 
@@ -539,6 +552,7 @@ struct Oracle {
         rmBasis(rmM);
         if (!invert19(gsM, gsMinv) || !invert19(rmM, rmMinv)) { err = "moment basis not invertible"; return false; }
         if (d.layout != ACP_LAYOUT_BOX) { err = "two-level oracle: box layout only"; return false; }
+        if ((d.coupling == ACP_COUPLING_STD) != (d.overlap == 1)) { err = "STD needs Overlap 1, DC1/DC2 Overlap 0"; return false; }
         const int dims[3] = {d.nx, d.ny, d.nz};
         for (int a = 0; a < 3; ++a) {
             boxLo[a] = d.box_lo[a];
@@ -569,8 +583,11 @@ struct Oracle {
                         const int c[3] = {i, j, kk};
                         bool dead = true, inner = true;
                         for (int a = 0; a < 3; ++a) {
-                            const int dlo = loIf[a] ? boxLo[a] + 2 : boxLo[a], dhi = hiIf[a] ? boxHi[a] - 2 : boxHi[a];
-                            const int ilo = loIf[a] ? boxLo[a] + 1 : boxLo[a], ihi = hiIf[a] ? boxHi[a] - 1 : boxHi[a];
+                            // STD: the coupling nodes lie one cell inside the box (Overlap 1);
+                            // DC: on the box faces (Overlap 0); the nodes inside them are dead
+                            const int ov = isDC() ? 0 : 1;
+                            const int dlo = loIf[a] ? boxLo[a] + 1 + ov : boxLo[a], dhi = hiIf[a] ? boxHi[a] - 1 - ov : boxHi[a];
+                            const int ilo = loIf[a] ? boxLo[a] + ov : boxLo[a], ihi = hiIf[a] ? boxHi[a] - ov : boxHi[a];
                             if (c[a] < dlo || c[a] > dhi) dead = false;
                             if (c[a] < ilo || c[a] > ihi) inner = false;
                         }
@@ -734,7 +751,8 @@ struct Oracle {
                     }
                     C2FNode cn;
                     cn.n = n;
-                    cn.mask = replaceMask(desc.c2f_replace, face);
+                    // the direct coupling never overwrites the fine populations that only the fine level has
+                    cn.mask = replaceMask(isDC() && desc.c2f_replace == ACP_C2F_FALL ? ACP_C2F_MFP : desc.c2f_replace, face);
                     for (int m = 0; m < 4; ++m) { cn.st[m] = -1; cn.w[m] = 0; }
                     cn.src = -1;
                     if (nodd == 0) {
@@ -802,6 +820,193 @@ struct Oracle {
                     fn.mask = replaceMask(desc.f2c_replace, face);
                     f2c.push_back(fn);
                 }
+        if (isDC()) {
+            f2c.clear();
+            buildDirectCoupling();
+        }
+    }
+
+    // the shared nodes of the direct coupling, in the order of the coincident C2F nodes
+    void buildDirectCoupling() {
+        Level& C = lev[0];
+        Level& F = lev[1];
+        const int dims[3] = {C.nx, C.ny, C.nz}, fd[3] = {F.nx, F.ny, F.nz};
+        auto live = [&](Level& L, const int* dd, const int* c, long& out) {
+            int cc[3];
+            for (int a = 0; a < 3; ++a) {
+                cc[a] = c[a];
+                if (cc[a] < 0 || cc[a] >= dd[a]) {
+                    if (!L.per[a]) return false;
+                    cc[a] = (cc[a] % dd[a] + dd[a]) % dd[a];
+                }
+            }
+            out = L.idx(cc[0], cc[1], cc[2]);
+            return L.type[out] != NT_DEAD;
+        };
+        const unsigned all = (1u << Q) - 1u;
+        const double w1[3] = {0.25, 0.5, 0.25};
+        dc.clear();
+        for (const C2FNode& cn : c2f) {
+            if (cn.kind != 0) continue;
+            DCNode dn;
+            dn.nf = cn.n;
+            dn.nc = cn.src;
+            const int cf[3] = {(int)(cn.n % F.nx), (int)((cn.n / F.nx) % F.ny), (int)(cn.n / ((long)F.nx * F.ny))};
+            const int cc[3] = {(int)(cn.src % C.nx), (int)((cn.src / C.nx) % C.ny), (int)(cn.src / ((long)C.nx * C.ny))};
+            dn.vc = dn.vf = 0;
+            for (int q = 0; q < Q; ++q) {
+                const int e[3] = {EX[q], EY[q], EZ[q]};
+                int sc[3], sf[3];
+                long t;
+                for (int a = 0; a < 3; ++a) { sc[a] = cc[a] - e[a]; sf[a] = cf[a] - e[a]; }
+                if (live(C, dims, sc, t)) dn.vc |= 1u << q;
+                if (live(F, fd, sf, t)) dn.vf |= 1u << q;
+            }
+            const unsigned both = dn.vc & dn.vf;
+            dn.rc = (~dn.vc & all) | (desc.f2c_replace != ACP_F2C_MC ? both : 0u);
+            dn.rf = (~dn.vf & all) | (desc.c2f_replace != ACP_C2F_MF ? both : 0u);
+            // interface plane: spanned by the axes other than the first face axis
+            int fa = 0;
+            for (int a = 0; a < 3; ++a)
+                if ((loIf[a] && cf[a] == 0) || (hiIf[a] && cf[a] == fd[a] - 1)) { fa = a; break; }
+            const int b1 = fa == 0 ? 1 : 0, b2 = fa == 2 ? 1 : 2;
+            double wsum = 0;
+            for (int m = 0; m < 9; ++m) {
+                const int d1 = m % 3 - 1, d2 = m / 3 - 1;
+                int c2[3] = {cf[0], cf[1], cf[2]};
+                c2[b1] += d1;
+                c2[b2] += d2;
+                long t;
+                const bool ok = live(F, fd, c2, t) && F.type[t] == NT_IFACE;
+                double w = 0;
+                if (ok) {
+                    if (desc.f2c_filter == ACP_F2C_NOFI) w = m == 4 ? 1. : 0.;
+                    else if (desc.f2c_filter == ACP_F2C_LAG) w = 1.;
+                    else w = w1[d1 + 1] * w1[d2 + 1];
+                }
+                dn.plane[m] = ok && w > 0 ? t : -1;
+                dn.w[m] = dn.plane[m] >= 0 ? w : 0.;
+                wsum += dn.w[m];
+            }
+            for (int m = 0; m < 9; ++m) dn.w[m] /= wsum;
+            dc.push_back(dn);
+        }
+    }
+
+    // second-order regularised non-equilibrium: 4.5 w_q H2_q : Pi with Pi =
+    // sum_q H2_q neq_q, H2 in lattice units (e_a e_b - delta_ab / 3)
+    void regularise(const double* neq, double* out) {
+        double P[6] = {0, 0, 0, 0, 0, 0};
+        for (int q = 0; q < Q; ++q) {
+            P[0] += (EX[q] * EX[q] - 1. / 3.) * neq[q];
+            P[1] += (EY[q] * EY[q] - 1. / 3.) * neq[q];
+            P[2] += (EZ[q] * EZ[q] - 1. / 3.) * neq[q];
+            P[3] += EX[q] * EY[q] * neq[q];
+            P[4] += EX[q] * EZ[q] * neq[q];
+            P[5] += EY[q] * EZ[q] * neq[q];
+        }
+        for (int q = 0; q < Q; ++q) {
+            const double h = (EX[q] * EX[q] - 1. / 3.) * P[0] + (EY[q] * EY[q] - 1. / 3.) * P[1] +
+                             (EZ[q] * EZ[q] - 1. / 3.) * P[2] +
+                             2. * (EX[q] * EY[q] * P[3] + EX[q] * EZ[q] * P[4] + EY[q] * EZ[q] * P[5]);
+            out[q] = 4.5 * k.w[q] * h;
+        }
+    }
+
+    // direct coupling at the shared nodes (GridCoupling::interpolTimeDirectCoupling
+    // and directCoupling, declared GridCoupling.h:28-29, called at
+    // Lattice.cpp:14018-14058 and 14699-14739; bodies absent).  th < 1: the
+    // fine side at t+1/2 from the coarse state blended in time; th == 1: both
+    // sides at t+1.  The equilibrium is that of the merged population set
+    // (each population from the level on which it is valid); the replaced
+    // populations get that equilibrium plus the other level's rescaled
+    // non-equilibrium -- population-wise (DC1) or regularised onto H2 (DC2).
+    void directCouple(int cnew, int fnew, double th) {
+        Level& C = lev[0];
+        Level& F = lev[1];
+        double* CB = C.f[cnew].data();
+        double* FB = F.f[fnew].data();
+        const bool dc2 = desc.coupling == ACP_COUPLING_DC2;
+        const double aF2C = 2. * F.omega / C.omega;
+#pragma omp parallel for num_threads(threads) schedule(static)
+        for (long t = 0; t < (long)dc.size(); ++t) {
+            const DCNode& dn = dc[t];
+            const double* cp = &CB[dn.nc * Q];
+            const double* fp = &FB[dn.nf * Q];
+            double X[Q], eq[Q], rho, u[3];
+            // populations whose source node is live on neither level keep the
+            // coarse state of t (complete after the previous exchange); no
+            // population that a level leaves unwritten is ever read
+            for (int q = 0; q < Q; ++q) {
+                if (dn.vc >> q & 1u) X[q] = (1. - th) * pre[t * Q + q] + th * cp[q];
+                else if (th == 1. && (dn.vf >> q & 1u)) X[q] = fp[q];
+                else X[q] = pre[t * Q + q];
+            }
+            splitEq(X, eq, rho, u, C.dt);
+            double fnew_[Q], cnew_[Q];
+            // fine side
+            {
+                double neq[Q], sc[Q];
+                if (dc2) {
+                    for (int q = 0; q < Q; ++q) {
+                        const bool fineScaled = th == 1. && !(dn.vc >> q & 1u) && (dn.vf >> q & 1u);
+                        neq[q] = (fineScaled ? aF2C : 1.) * (X[q] - eq[q]);
+                    }
+                    double r[Q];
+                    regularise(neq, r);
+                    const double aC2F = C.omega / (2. * F.omega);
+                    for (int q = 0; q < Q; ++q) fnew_[q] = eq[q] + aC2F * r[q];
+                } else {
+                    for (int q = 0; q < Q; ++q) neq[q] = X[q] - eq[q];
+                    rescale(neq, sc, true);
+                    for (int q = 0; q < Q; ++q) fnew_[q] = (dn.vc >> q & 1u) ? eq[q] + sc[q] : eq[q];
+                }
+            }
+            // coarse side (t+1): filtered fine populations in the interface plane
+            if (th == 1.) {
+                double ff[Q], neq[Q], sc[Q];
+                for (int q = 0; q < Q; ++q) {
+                    double acc = 0;
+                    for (int m = 0; m < 9; ++m)
+                        if (dn.plane[m] >= 0) acc += dn.w[m] * FB[dn.plane[m] * Q + q];
+                    ff[q] = acc;
+                }
+                // fine non-equilibrium; the fine-missing populations take the
+                // coarse one brought to the fine scale
+                const double aC2F = C.omega / (2. * F.omega);
+                for (int q = 0; q < Q; ++q) neq[q] = (dn.vf >> q & 1u) ? ff[q] - eq[q] : aC2F * (X[q] - eq[q]);
+                if (dc2) {
+                    for (int q = 0; q < Q; ++q) neq[q] *= aF2C;
+                    regularise(neq, sc);
+                    for (int q = 0; q < Q; ++q) cnew_[q] = eq[q] + sc[q];
+                } else {
+                    rescale(neq, sc, false);
+                    for (int q = 0; q < Q; ++q) cnew_[q] = (dn.vf >> q & 1u) ? eq[q] + sc[q] : eq[q];
+                }
+            }
+            for (int q = 0; q < Q; ++q)
+                if (dn.rf >> q & 1u) FB[dn.nf * Q + q] = fnew_[q];
+            if (th == 1.)
+                for (int q = 0; q < Q; ++q)
+                    if (dn.rc >> q & 1u) CB[dn.nc * Q + q] = cnew_[q];
+        }
+    }
+
+    // the fine coupling nodes between coarse positions (mid, then centre)
+    void interpolateHanging(int fnew) {
+        double* FB = lev[1].f[fnew].data();
+        for (const C2FNode& cn : c2f) {
+            if (cn.kind == 0) continue;
+            double v[Q];
+            for (int q = 0; q < Q; ++q) {
+                double acc = 0;
+                for (int m = 0; m < 4; ++m)
+                    if (cn.st[m] >= 0) acc += cn.w[m] * FB[cn.st[m] * Q + q];
+                v[q] = acc;
+            }
+            for (int q = 0; q < Q; ++q)
+                if (cn.mask >> q & 1u) FB[cn.n * Q + q] = v[q];
+        }
     }
 
     // equilibrium of a population array's own moments and the non-equilibrium part
@@ -910,6 +1115,18 @@ struct Oracle {
                 ++ic;
             }
         const int cnew = 1 - alt;
+        if (isDC()) {
+            stepLevel(0, alt);                  // coarse step t -> t+1
+            stepLevel(1, altf);                 // fine sub-step t -> t+1/2
+            directCouple(cnew, 1 - altf, 0.5);  // shared nodes, fine side, t+1/2
+            interpolateHanging(1 - altf);
+            stepLevel(1, 1 - altf);             // fine sub-step t+1/2 -> t+1
+            directCouple(cnew, altf, 1.0);      // shared nodes, both sides, t+1
+            interpolateHanging(altf);
+            alt = cnew;
+            ++steps;
+            return;
+        }
         stepLevel(0, alt);                 // coarse step t -> t+1
         stepLevel(1, altf);                // fine sub-step t -> t+1/2
         coarseToFine(cnew, 1 - altf, 0.5);  // C2F at t+1/2 (linear in time)

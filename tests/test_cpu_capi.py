@@ -114,3 +114,20 @@ def test_invalid_cases_rejected_before_device_use():
     assert L.acp_estimate_bytes(C.byref(default_case()), C.byref(size)) == ACP_OK
     n = 151 * 151 * 21
     assert size.value >= n * 2 * 19 * 8
+
+
+def test_coupling_needs_matching_overlap():
+    """STD couples with one coarse cell of overlap, DC1/DC2 with none
+    (BoundaryConditions.txt: Overlap 0 for the direct coupling)."""
+    from acpulse_vclbm_b200.capi import COUPLING, LAYOUT_BOX, lattice_units_case
+    L = engine.lib()
+    for coupling, overlap in [("STD", 0), ("DC1", 1), ("DC2", 1)]:
+        d = lattice_units_case(32, 16, 3, op="HRR", periodic=(False, True, True))
+        d.max_level, d.layout = 1, LAYOUT_BOX
+        d.box_lo[:] = [16, 0, 0]
+        d.box_hi[:] = [31, 15, 2]
+        d.coupling, d.overlap = COUPLING[coupling], overlap
+        h = C.c_void_p()
+        assert L.acp_create(C.byref(d), -1, C.byref(h)) == ACP_ERR_INVALID
+        assert b"Overlap" in L.acp_last_error(h)
+        L.acp_destroy(h)

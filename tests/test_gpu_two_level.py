@@ -11,13 +11,14 @@ import numpy as np
 import pytest
 
 from acpulse_vclbm_b200 import engine
-from acpulse_vclbm_b200.capi import (C2F_REPLACE, F2C_FILTER, F2C_REPLACE, LAYOUT_BOX, SCALING, lattice_units_case)
+from acpulse_vclbm_b200.capi import (C2F_REPLACE, COUPLING, F2C_FILTER, F2C_REPLACE, LAYOUT_BOX, SCALING,
+                                     lattice_units_case)
 
 pytestmark = pytest.mark.gpu
 
 
 def half_box(op, filt="NOFI", style="SRTSTYLE", storage="FP64", nx=48, ny=20, nz=3, order=3, c2f="fAll",
-             f2c="cAll", cubic=0):
+             f2c="cAll", cubic=0, coupling="STD"):
     d = lattice_units_case(nx, ny, nz, op=op, nu_lu=1e-3, order=order, periodic=(False, True, True), eps=1e-3,
                            b=4.0, center=(nx / 4.0, ny / 2.0, 1.0), storage=storage)
     d.max_level = 1
@@ -30,10 +31,12 @@ def half_box(op, filt="NOFI", style="SRTSTYLE", storage="FP64", nx=48, ny=20, nz
     d.f2c_replace = F2C_REPLACE[f2c]
     d.mrt_writeback = 1
     d.cubic_mach = cubic
+    d.coupling = COUPLING[coupling]
+    d.overlap = 1 if coupling == "STD" else 0
     return d
 
 
-def patch_3d(op, filt="LAG", storage="FP64"):
+def patch_3d(op, filt="LAG", storage="FP64", coupling="STD"):
     d = lattice_units_case(24, 22, 20, op=op, nu_lu=1e-3, order=3, periodic=(True, True, True), eps=2e-3, b=3.0,
                            center=(7.0, 11.0, 10.0), storage=storage, ic_dims=3)
     d.max_level = 1
@@ -42,6 +45,8 @@ def patch_3d(op, filt="LAG", storage="FP64"):
     d.box_hi[:] = [18, 16, 13]
     d.f2c_filter = F2C_FILTER[filt]
     d.mrt_writeback = 1
+    d.coupling = COUPLING[coupling]
+    d.overlap = 1 if coupling == "STD" else 0
     return d
 
 
@@ -140,3 +145,62 @@ def test_update_count_and_probe_on_fine_level():
     s = L.probes()
     assert s.shape == (3, 1) and np.all(np.isfinite(s))
     L.close()
+
+
+# direct coupling (Overlap 0): the coarse nodes on the box faces are shared
+# with the fine level; coarse nodes strictly inside the box carry no state
+@pytest.mark.parametrize("op", ["SRT", "MRT-GS", "MRT-RM", "RR", "HRR"])
+@pytest.mark.parametrize("coupling", ["DC1", "DC2"])
+@pytest.mark.parametrize("filt", ["NOFI", "LAG", "TOU"])
+def test_direct_coupling_matches_oracle(op, coupling, filt):
+    d = half_box(op, filt, coupling=coupling, c2f="Mf", f2c="Mc")
+    g, r = run_both(d, 60)
+    live_x = slice(0, d.nx // 2 + 1)
+    err_c = np.abs(g[0][..., live_x] - r[0][..., live_x]).max() / d.ic_eps
+    err_f = np.abs(g[1] - r[1]).max() / d.ic_eps
+    assert err_c < 1e-9 and err_f < 1e-9, (err_c, err_f)
+
+
+@pytest.mark.parametrize("variant", ["MfP-Mc", "Mf-McP", "MRTSTYLE", "order4"])
+@pytest.mark.parametrize("coupling", ["DC1", "DC2"])
+def test_direct_coupling_variants(variant, coupling):
+    kw = {"MfP-Mc": dict(c2f="MfP", f2c="Mc"), "Mf-McP": dict(c2f="Mf", f2c="McP"),
+          "MRTSTYLE": dict(style="MRTSTYLE", c2f="Mf", f2c="Mc"), "order4": dict(order=4, c2f="Mf", f2c="Mc")}[variant]
+    d = half_box("HRR", "TOU", coupling=coupling, **kw)
+    g, r = run_both(d, 50)
+    live_x = slice(0, d.nx // 2 + 1)
+    assert np.abs(g[0][..., live_x] - r[0][..., live_x]).max() / d.ic_eps < 1e-9
+    assert np.abs(g[1] - r[1]).max() / d.ic_eps < 1e-9
+
+
+@pytest.mark.parametrize("coupling", ["DC1", "DC2"])
+def test_direct_coupling_3d_patch(coupling):
+    d = patch_3d("HRR", coupling=coupling)
+    d.c2f_replace = C2F_REPLACE["Mf"]
+    d.f2c_replace = F2C_REPLACE["Mc"]
+    g, r = run_both(d, 40)
+    c = np.ones(g[0].shape[1:], dtype=bool)
+    c[7:13, 6:16, 11:18] = False  # z, y, x: lo+1..hi-1 carry no state
+    err_c = np.abs(g[0][:, c] - r[0][:, c]).max() / d.ic_eps
+    err_f = np.abs(g[1] - r[1]).max() / d.ic_eps
+    assert err_c < 1e-9 and err_f < 1e-9, (err_c, err_f)
+
+
+def test_direct_coupling_fp32_within_1e5():
+    d64 = half_box("HRR", "LAG", coupling="DC1", c2f="Mf", f2c="Mc")
+    d32 = half_box("HRR", "LAG", coupling="DC1", c2f="Mf", f2c="Mc", storage="FP32-DEV")
+    steps = 150
+    from oracle.pyoracle import OracleLattice
+    o = OracleLattice(d64, threads=8)
+    o.init()
+    o.step(steps)
+    L = engine.Lattice(d32).init()
+    L.step(steps)
+    L.sync()
+    cs2 = d64.speed_of_sound ** 2
+    amp = d64.ic_eps * d64.density * cs2
+    live_x = slice(0, d64.nx // 2 + 1)
+    pc = np.abs(L.populations(0).sum(0)[..., live_x] - o.populations(0).sum(0)[..., live_x]).max() * cs2 / amp
+    pf = np.abs(L.populations(1).sum(0) - o.populations(1).sum(0)).max() * cs2 / amp
+    L.close()
+    assert pc < 1e-5 and pf < 1e-5, (pc, pf)
