@@ -17,7 +17,7 @@ MAIN = os.path.join(HERE, "acp_main")
 HOSTCXX = os.environ.get("ACP_HOSTCXX", "/usr/bin/g++")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["engine.cu", "caseparse.cpp"]
+SOURCES = ["engine.cu", "batch.cu", "caseparse.cpp"]
 
 
 def _deps():
@@ -49,7 +49,7 @@ def build(force=False, verbose_ptxas=False):
         return OUT
     objdir = os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
-    objs = []
+    objs, cmds = [], []
     for src in SOURCES:
         obj = os.path.join(objdir, src + ".o")
         cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
@@ -59,8 +59,17 @@ def build(force=False, verbose_ptxas=False):
             cmd.insert(2, "cu")
         if verbose_ptxas:
             cmd += ["-Xptxas", "-v"]
-        subprocess.run(cmd, check=True)
+        cmds.append(cmd)
         objs.append(obj)
+    # the translation units compile side by side
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(len(cmds)) as pool:
+        for r in pool.map(lambda c: subprocess.run(c, capture_output=True, text=True), cmds):
+            if r.returncode != 0:
+                sys.stderr.write(r.stdout + r.stderr)
+                raise subprocess.CalledProcessError(r.returncode, r.args)
+            if verbose_ptxas:
+                sys.stderr.write(r.stderr)
     tmp = OUT + ".tmp"
     subprocess.run([NVCC, *ARCH, "-shared", "-cudart", "static", "-o", tmp, *objs], check=True)
     os.replace(tmp, OUT)

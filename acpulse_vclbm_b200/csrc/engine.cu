@@ -4,6 +4,7 @@
 #include "../../include/acp.h"
 #include "kernels.cuh"
 #include "topology.h"
+#include "handle.h"
 
 #include <cuda_runtime.h>
 
@@ -20,86 +21,21 @@ using namespace acp;
 
 namespace {
 
-struct LevelHost {
-    int nx = 0, ny = 0, nz = 0;
-    long long N = 0;
-    int off[3] = {0, 0, 0};  // box origin in this level's global node index
-    int per[3] = {0, 0, 0};  // periodic axes of this level
-    std::vector<uint8_t> code;
-    std::vector<BNodeDev> lodiX, lodiZY;
-    long long active = 0;
-    double omega = 0, dt = 0, spacing = 0;
-};
+std::mutex g_constMutex;
+bool g_constUploaded[64] = {false};
 
-struct LevelDev {
-    void* f[2] = {nullptr, nullptr};
-    uint8_t* code = nullptr;
-    BNodeDev* lodiX = nullptr;
-    BNodeDev* lodiZY = nullptr;
-    int nLodiX = 0, nLodiZY = 0;
-};
-
-size_t storageBytes(int storage) { return storage == ACP_STORE_F64 ? 8 : (storage == ACP_STORE_F32_DEV ? 4 : 2); }
-
-}  // namespace
-
-struct acp_handle {
-    acp_case_desc d;
-    int device = 0;
-    std::vector<LevelHost> host;
-    std::vector<LevelDev> dev;
-    int cur = 0;  // array holding the current state (0 or 1) of every level
-    bool inited = false;
-    long long steps = 0;
-    cudaStream_t stream = nullptr;
-    bool ownStream = false;
-    cudaGraphExec_t graph[2] = {nullptr, nullptr};  // one step starting from cur == 0 / cur == 1
-    // two-level coupling (fine state always in array 0 between coarse steps)
-    std::vector<C2FDev> c2fHost;
-    std::vector<F2CDev> f2cHost;
-    std::vector<DCDev> dcHost;  // direct coupling: the shared nodes
-    DCDev* dDC = nullptr;
-    int nCoinc = 0, nMid = 0, nCen = 0;
-    C2FDev* dC2F = nullptr;
-    F2CDev* dF2C = nullptr;
-    void* dPre = nullptr;  // coarse populations before the coarse step, [Q][nCoinc]
-    int* dErr = nullptr;
-    // probes
-    long long* dProbeNodes = nullptr;
-    int nProbes = 0;
-    double* dSeries = nullptr;
-    int* dCounter = nullptr;
-    int probeCapacity = 0;
-    int probeLevel = 0;
-    size_t devBytes = 0;
-    std::string err;
-    double c = 0, kappa = 0, shift = 0;
-    float hscale[Q];
-    double m4[18] = {0};  // sum_q w_q H2_q (x) H4_q(kappa) (fourth-order equilibria)
-};
-
-namespace {
-
-int fail(acp_handle* h, int code, const char* fmt, ...) {
-    if (h) {
-        char buf[512];
-        va_list ap;
-        va_start(ap, fmt);
-        std::vsnprintf(buf, sizeof buf, fmt, ap);
-        va_end(ap);
-        h->err = buf;
-    }
-    return code;
+// this translation unit's copies of the constant tables, once per device
+int uploadConstants(int device) {
+    if (device < 0 || device >= 64) return ACP_ERR_UNSUPPORTED;
+    std::lock_guard<std::mutex> lock(g_constMutex);
+    if (g_constUploaded[device]) return ACP_OK;
+    ConstTables t;
+    int s = makeConstTables(t);
+    if (s) return s;
+    if ((s = uploadTables(t))) return s;
+    g_constUploaded[device] = true;
+    return ACP_OK;
 }
-
-#define CU(h, call)                                                                                       \
-    do {                                                                                                  \
-        cudaError_t e_ = (call);                                                                          \
-        if (e_ != cudaSuccess) return fail((h), ACP_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
-    } while (0)
-
-std::once_flag g_constOnce;
-int g_constStatus = 0;
 
 // MRT bases on the host: inverse of the Gram-Schmidt basis and the
 // raw-moment back transform, uploaded once per process.
@@ -138,8 +74,13 @@ int rmRowFull(int m, int q) {
     return v[m];
 }
 
-int uploadConstants() {
-    uint32_t masks[54];
+}  // namespace
+
+namespace acp {
+
+// the lattice constant tables (push masks, MRT bases)
+int makeConstTables(ConstTables& t) {
+    uint32_t* masks = t.masks;
     for (int c = 0; c < 54; ++c) masks[c] = 0;
     // coupling nodes: every direction except those leaving the level across its box faces
     for (int c = 0; c < 27; ++c) {
@@ -160,7 +101,10 @@ int uploadConstants() {
         masks[faceCode(b.fx, b.fy, b.fz)] = m;
     }
     masks[CODE_FLUID] = 0x3FFFFu;
-    double gs[Q * Q], gsi[Q * Q], rm[Q * Q], rmi[Q * Q], mw[Q], rm2[Q][5];
+    double gs[Q * Q], rm[Q * Q], rmi[Q * Q];
+    double* gsi = t.gsi;
+    double* mw = t.mw;
+    double(*rm2)[5] = t.rm2;
     for (int m = 0; m < Q; ++m)
         for (int q = 0; q < Q; ++q) {
             gs[m * Q + q] = gsRow(m, q);
@@ -173,18 +117,15 @@ int uploadConstants() {
     }
     for (int q = 0; q < Q; ++q)
         for (int m = 0; m < 5; ++m) rm2[q][m] = rmi[q * Q + 5 + m];
-    if (cudaMemcpyToSymbol(c_pushMask, masks, sizeof masks) != cudaSuccess) return ACP_ERR_CUDA;
-    if (cudaMemcpyToSymbol(c_gsMinv, gsi, sizeof gsi) != cudaSuccess) return ACP_ERR_CUDA;
-    if (cudaMemcpyToSymbol(c_gsMw, mw, sizeof mw) != cudaSuccess) return ACP_ERR_CUDA;
-    if (cudaMemcpyToSymbol(c_rmTinv2, rm2, sizeof rm2) != cudaSuccess) return ACP_ERR_CUDA;
-    float gsif[Q * Q], rm2f[Q][5];
-    for (int k = 0; k < Q * Q; ++k) gsif[k] = (float)gsi[k];
+    for (int k = 0; k < Q * Q; ++k) t.gsiF[k] = (float)gsi[k];
     for (int q = 0; q < Q; ++q)
-        for (int m = 0; m < 5; ++m) rm2f[q][m] = (float)rm2[q][m];
-    if (cudaMemcpyToSymbol(c_gsMinvF, gsif, sizeof gsif) != cudaSuccess) return ACP_ERR_CUDA;
-    if (cudaMemcpyToSymbol(c_rmTinv2F, rm2f, sizeof rm2f) != cudaSuccess) return ACP_ERR_CUDA;
+        for (int m = 0; m < 5; ++m) t.rm2F[q][m] = (float)rm2[q][m];
     return ACP_OK;
 }
+
+}  // namespace acp
+
+namespace {
 
 int validate(const acp_case_desc* d, std::string& why) {
     if (!d) { why = "null case"; return ACP_ERR_INVALID; }
@@ -608,27 +549,6 @@ int buildSingleLevel(acp_handle* h) {
 }
 
 template <typename S>
-LevelArgs<S> levelArgs(acp_handle* h, int l, int src) {
-    const LevelHost& L = h->host[l];
-    const LevelDev& D = h->dev[l];
-    LevelArgs<S> a;
-    a.nx = L.nx; a.ny = L.ny; a.nz = L.nz;
-    a.N = L.N;
-    a.Ni = (int)L.N;
-    for (int ax = 0; ax < 3; ++ax) a.per[ax] = L.per[ax];
-    a.A = (const S*)D.f[src];
-    a.B = (S*)D.f[1 - src];
-    a.code = D.code;
-    a.shift = h->shift;
-    a.omega = L.omega;
-    a.kappa = h->kappa;
-    a.sigma = h->d.hybrid_sigma;
-    for (int q = 0; q < Q; ++q) a.hscale[q] = h->hscale[q];
-    for (int c = 0; c < 18; ++c) a.m4[c] = h->m4[c];
-    return a;
-}
-
-template <typename S>
 using CollideFn = void (*)(LevelArgs<S>);
 
 template <typename S, typename R, int OP>
@@ -688,7 +608,6 @@ LodiFn<S> pickLodi(int order) {
     return order == 2 ? k_lodi<S, 2> : (order == 3 ? k_lodi<S, 3> : k_lodi<S, 4>);
 }
 
-bool needsMoments(const acp_case_desc& d) { return d.op == OP_HRR || (d.op == OP_RR && d.cubic_mach); }
 
 // events recorded between the kernels of a step, for acp_step_timed
 struct PhaseTimer {
@@ -716,55 +635,19 @@ int enqueueLevelStep(acp_handle* h, int l, int src, PhaseTimer* tm = nullptr) {
     const int bx = 128;
     if (tm) tm->mark(-1);
     if (needsMoments(h->d)) {
-        // z-marching tiles; a periodic z axis of <= 3 planes is resident at once
-        const int bxy = ((L.nx + TX - 1) / TX) * ((L.ny + TY - 1) / TY);
-        int chunk = L.nz;
-        if (!(L.per[2] && L.nz <= 3)) {
-            const int want = (4 * 148 + bxy - 1) / bxy;  // z chunks for >= 4 blocks per SM
-            chunk = std::max(8, (L.nz + want - 1) / want);
-        }
+        const int chunk = tiledChunk(L);
         dim3 grid((L.nx + TX - 1) / TX, (L.ny + TY - 1) / TY, (L.nz + chunk - 1) / chunk);
         pickTiled<S, R>(h->d)<<<grid, dim3(TX, TY), 0, h->stream>>>(a, chunk);
     } else {
         pickCollide<S, R>(h->d)<<<gridOf(L, bx), bx, 0, h->stream>>>(a);
     }
     if (tm) tm->mark(ACP_K_COLLIDE);
-    LodiArgs p;
-    p.N = L.N;
-    p.shift = h->shift;
-    p.cs = h->d.speed_of_sound;
-    p.c = h->c;
-    p.mach = h->d.mach;
-    p.k1 = h->d.k1;
-    p.rho0 = h->d.density;
-    p.dt = L.dt;
-    p.localSpacing = h->d.spacing * std::pow(2.0, -(double)l);
-    p.kappa = h->kappa;
-    p.domainLength[0] = h->d.nx * h->d.spacing;
-    p.domainLength[1] = h->d.ny * h->d.spacing;
-    p.domainLength[2] = h->d.nz * h->d.spacing;
-    p.order = h->d.eq_order;
-    p.errorFlag = h->dErr;
+    const LodiArgs p = lodiArgsOf(h, l);
     LodiFn<S> lf = pickLodi<S>(h->d.eq_order);
     if (D.nLodiX) lf<<<(D.nLodiX + 127) / 128, 128, 0, h->stream>>>(a.A, a.B, D.lodiX, D.nLodiX, p, a);
     if (D.nLodiZY) lf<<<(D.nLodiZY + 127) / 128, 128, 0, h->stream>>>(a.A, a.B, D.lodiZY, D.nLodiZY, p, a);
     if (tm && (D.nLodiX || D.nLodiZY)) tm->mark(ACP_K_LODI);
     return ACP_OK;
-}
-
-CouplingArgs couplingArgs(const acp_handle* h) {
-    CouplingArgs c;
-    c.Nc = h->host[0].N;
-    c.Nf = h->host[1].N;
-    c.shiftC = h->shift;
-    c.kappa = h->kappa;
-    c.omegaC = h->host[0].omega;
-    c.omegaF = h->host[1].omega;
-    c.alphaC2F = c.omegaC / (2.0 * c.omegaF);
-    c.alphaF2C = 2.0 * c.omegaF / c.omegaC;
-    c.mrtStyle = h->d.scaling_style == ACP_SCALING_MRT;
-    c.filter = h->d.f2c_filter;
-    return c;
 }
 
 // C2F onto the fine array `fdst` from the coarse array `cnew` (blended with
@@ -1037,8 +920,7 @@ int acp_create(const acp_case_desc* d, int device, acp_handle** out) {
     }
     *out = h;
     CU(h, cudaSetDevice(h->device));
-    std::call_once(g_constOnce, [] { g_constStatus = uploadConstants(); });
-    if (g_constStatus) return fail(h, g_constStatus, "uploading lattice constants failed");
+    if ((s = uploadConstants(h->device))) return fail(h, s, "uploading lattice constants failed");
     h->c = d->speed_of_sound * std::sqrt(3.0);
     h->kappa = 1.0 / (6.0 * h->c * h->c);
     h->shift = d->storage == ACP_STORE_F64 ? 0.0 : d->density;
@@ -1140,6 +1022,7 @@ int acp_init(acp_handle* h) {
 
 int acp_step(acp_handle* h, int n) {
     if (!h || !h->inited) return ACP_ERR_STATE;
+    if (h->batch) return fail(h, ACP_ERR_STATE, "the case is stepped by its batch (acp_batch_step)");
     if (n < 0) return fail(h, ACP_ERR_INVALID, "negative step count");
     CU(h, cudaSetDevice(h->device));
     for (int s = 0; s < n; ++s) {
@@ -1154,6 +1037,7 @@ int acp_sync(acp_handle* h) {
     if (!h) return ACP_ERR_INVALID;
     if (h->dev.empty()) return ACP_ERR_STATE;
     CU(h, cudaSetDevice(h->device));
+    joinBatch(h);
     int flag = 0;
     CU(h, cudaMemcpyAsync(&flag, h->dErr, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     CU(h, cudaStreamSynchronize(h->stream));
@@ -1177,6 +1061,7 @@ int acp_active_updates(acp_handle* h, long long* coarse, long long* fine) {
 int acp_read_populations(acp_handle* h, int level, double* out) {
     if (!h || !out || level < 0 || level >= (int)h->host.size()) return ACP_ERR_INVALID;
     CU(h, cudaSetDevice(h->device));
+    joinBatch(h);
     const LevelHost& L = h->host[level];
     double* tmp = nullptr;
     CU(h, cudaMallocAsync((void**)&tmp, (size_t)L.N * Q * sizeof(double), h->stream));
@@ -1202,6 +1087,7 @@ int acp_read_populations_window(acp_handle* h, int level, long long begin, int c
         return fail(h, ACP_ERR_INVALID, "window [%lld, %lld) outside the level's %lld nodes", begin, begin + count, L.N);
     if (count == 0) return ACP_OK;
     CU(h, cudaSetDevice(h->device));
+    joinBatch(h);
     double* scratch = nullptr;
     int s = windowScratch(h, h->device, &scratch);
     if (s) return s;
@@ -1220,6 +1106,7 @@ int acp_read_populations_window(acp_handle* h, int level, long long begin, int c
 int acp_write_populations(acp_handle* h, int level, const double* in) {
     if (!h || !in || level < 0 || level >= (int)h->host.size()) return ACP_ERR_INVALID;
     CU(h, cudaSetDevice(h->device));
+    joinBatch(h);
     const LevelHost& L = h->host[level];
     double* tmp = nullptr;
     CU(h, cudaMallocAsync((void**)&tmp, (size_t)L.N * Q * sizeof(double), h->stream));
@@ -1304,6 +1191,7 @@ int acp_set_probes(acp_handle* h, int n, const int* lijk) {
 int acp_read_probes(acp_handle* h, double* out, int max_samples, int* n_samples) {
     if (!h || !n_samples) return ACP_ERR_INVALID;
     CU(h, cudaSetDevice(h->device));
+    joinBatch(h);
     int cnt = 0;
     if (h->dCounter) CU(h, cudaMemcpyAsync(&cnt, h->dCounter, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     CU(h, cudaStreamSynchronize(h->stream));
@@ -1323,6 +1211,7 @@ int acp_steps_done(acp_handle* h, long long* steps) {
 
 int acp_set_stream(acp_handle* h, void* stream) {
     if (!h) return ACP_ERR_INVALID;
+    if (h->batch) return fail(h, ACP_ERR_STATE, "the case belongs to a batch");
     CU(h, cudaSetDevice(h->device));
     CU(h, cudaStreamSynchronize(h->stream));
     if (h->ownStream && stream) {
@@ -1347,6 +1236,7 @@ int acp_device_bytes(acp_handle* h, size_t* bytes) {
 
 int acp_step_timed(acp_handle* h, int n, double* kernel_ms) {
     if (!h || !h->inited || !kernel_ms || n < 0) return ACP_ERR_INVALID;
+    if (h->batch) return fail(h, ACP_ERR_STATE, "the case is stepped by its batch (acp_batch_step)");
     CU(h, cudaSetDevice(h->device));
     double acc[ACP_K_COUNT] = {0, 0, 0, 0, 0};
     PhaseTimer tm;
@@ -1411,6 +1301,7 @@ int acp_boundary_wiring(const acp_case_desc* d, long long* rows, long long max_r
 
 int acp_destroy(acp_handle* h) {
     if (!h) return ACP_OK;
+    if (h->batch) return fail(h, ACP_ERR_STATE, "destroy the batch before its cases");
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     destroyGraphs(h);

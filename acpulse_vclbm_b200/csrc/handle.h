@@ -1,0 +1,181 @@
+// The engine's handle (the state behind acp_handle of include/acp.h) and the
+// helpers that build kernel arguments from it; shared by the single-case
+// engine (engine.cu) and the batched engine (batch.cu).
+#pragma once
+#include "../../include/acp.h"
+#include "kernels.cuh"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+struct acp_batch;
+
+namespace acp {
+
+struct LevelHost {
+    int nx = 0, ny = 0, nz = 0;
+    long long N = 0;
+    int off[3] = {0, 0, 0};  // box origin in this level's global node index
+    int per[3] = {0, 0, 0};  // periodic axes of this level
+    std::vector<uint8_t> code;
+    std::vector<BNodeDev> lodiX, lodiZY;
+    long long active = 0;
+    double omega = 0, dt = 0, spacing = 0;
+};
+
+struct LevelDev {
+    void* f[2] = {nullptr, nullptr};
+    uint8_t* code = nullptr;
+    BNodeDev* lodiX = nullptr;
+    BNodeDev* lodiZY = nullptr;
+    int nLodiX = 0, nLodiZY = 0;
+};
+
+inline size_t storageBytes(int storage) {
+    return storage == ACP_STORE_F64 ? 8 : (storage == ACP_STORE_F32_DEV ? 4 : 2);
+}
+
+}  // namespace acp
+
+struct acp_handle {
+    acp_case_desc d;
+    int device = 0;
+    std::vector<acp::LevelHost> host;
+    std::vector<acp::LevelDev> dev;
+    int cur = 0;  // array holding the current state (0 or 1) of the coarse level
+    bool inited = false;
+    long long steps = 0;
+    cudaStream_t stream = nullptr;
+    bool ownStream = false;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};  // one step starting from cur == 0 / cur == 1
+    // two-level coupling (fine state always in array 0 between coarse steps)
+    std::vector<acp::C2FDev> c2fHost;
+    std::vector<acp::F2CDev> f2cHost;
+    std::vector<acp::DCDev> dcHost;  // direct coupling: the shared nodes
+    acp::DCDev* dDC = nullptr;
+    int nCoinc = 0, nMid = 0, nCen = 0;
+    acp::C2FDev* dC2F = nullptr;
+    acp::F2CDev* dF2C = nullptr;
+    void* dPre = nullptr;  // coarse populations before the coarse step, [Q][nCoinc]
+    int* dErr = nullptr;
+    // probes
+    long long* dProbeNodes = nullptr;
+    int nProbes = 0;
+    double* dSeries = nullptr;
+    int* dCounter = nullptr;
+    int probeCapacity = 0;
+    int probeLevel = 0;
+    size_t devBytes = 0;
+    std::string err;
+    double c = 0, kappa = 0, shift = 0;
+    float hscale[acp::Q];
+    double m4[18] = {0};  // sum_q w_q H2_q (x) H4_q(kappa) (fourth-order equilibria)
+    acp_batch* batch = nullptr;  // the batch this case belongs to (stepped only through it)
+};
+
+namespace acp {
+
+inline int fail(acp_handle* h, int code, const char* fmt, ...) {
+    if (h) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        std::vsnprintf(buf, sizeof buf, fmt, ap);
+        va_end(ap);
+        h->err = buf;
+    }
+    return code;
+}
+
+#define CU(h, call)                                                                                       \
+    do {                                                                                                  \
+        cudaError_t e_ = (call);                                                                          \
+        if (e_ != cudaSuccess) return fail((h), ACP_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+// kernel arguments of level l of a case, reading array src
+template <typename S>
+LevelArgs<S> levelArgs(const acp_handle* h, int l, int src) {
+    const LevelHost& L = h->host[l];
+    const LevelDev& D = h->dev[l];
+    LevelArgs<S> a;
+    a.nx = L.nx; a.ny = L.ny; a.nz = L.nz;
+    a.N = L.N;
+    a.Ni = (int)L.N;
+    for (int ax = 0; ax < 3; ++ax) a.per[ax] = L.per[ax];
+    a.A = (const S*)D.f[src];
+    a.B = (S*)D.f[1 - src];
+    a.code = D.code;
+    a.shift = h->shift;
+    a.omega = L.omega;
+    a.kappa = h->kappa;
+    a.sigma = h->d.hybrid_sigma;
+    for (int q = 0; q < Q; ++q) a.hscale[q] = h->hscale[q];
+    for (int c = 0; c < 18; ++c) a.m4[c] = h->m4[c];
+    return a;
+}
+
+inline CouplingArgs couplingArgs(const acp_handle* h) {
+    CouplingArgs c;
+    c.Nc = h->host[0].N;
+    c.Nf = h->host[1].N;
+    c.shiftC = h->shift;
+    c.kappa = h->kappa;
+    c.omegaC = h->host[0].omega;
+    c.omegaF = h->host[1].omega;
+    c.alphaC2F = c.omegaC / (2.0 * c.omegaF);
+    c.alphaF2C = 2.0 * c.omegaF / c.omegaC;
+    c.mrtStyle = h->d.scaling_style == ACP_SCALING_MRT;
+    c.filter = h->d.f2c_filter;
+    return c;
+}
+
+// LODI arguments of level l (Node::LODIpressureOutlet's constants: L is the
+// node count times the coarse spacing on every level, Node.cpp:311)
+inline LodiArgs lodiArgsOf(const acp_handle* h, int l) {
+    const LevelHost& L = h->host[l];
+    LodiArgs p;
+    p.N = L.N;
+    p.shift = h->shift;
+    p.cs = h->d.speed_of_sound;
+    p.c = h->c;
+    p.mach = h->d.mach;
+    p.k1 = h->d.k1;
+    p.rho0 = h->d.density;
+    p.dt = L.dt;
+    p.localSpacing = h->d.spacing * std::pow(2.0, -(double)l);
+    p.kappa = h->kappa;
+    p.domainLength[0] = h->d.nx * h->d.spacing;
+    p.domainLength[1] = h->d.ny * h->d.spacing;
+    p.domainLength[2] = h->d.nz * h->d.spacing;
+    p.order = h->d.eq_order;
+    p.errorFlag = h->dErr;
+    return p;
+}
+
+// event recorded after a batch's last enqueued step (defined with the batch)
+cudaEvent_t batchDoneEvent(acp_batch* b);
+
+// a case stepped by a batch: order the case's own stream after the batch's work
+inline void joinBatch(acp_handle* h) {
+    if (h && h->batch) cudaStreamWaitEvent(h->stream, batchDoneEvent(h->batch), 0);
+}
+
+inline bool needsMoments(const acp_case_desc& d) { return d.op == OP_HRR || (d.op == OP_RR && d.cubic_mach); }
+
+// z chunk of the tiled kernel: a periodic z axis of at most three planes is
+// resident at once; otherwise chunks give >= 4 blocks per SM
+inline int tiledChunk(const LevelHost& L) {
+    if (L.per[2] && L.nz <= 3) return L.nz;
+    const int bxy = ((L.nx + TX - 1) / TX) * ((L.ny + TY - 1) / TY);
+    const int want = (4 * 148 + bxy - 1) / bxy;
+    return std::max(8, (L.nz + want - 1) / want);
+}
+
+}  // namespace acp

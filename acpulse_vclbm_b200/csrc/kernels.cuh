@@ -40,6 +40,26 @@ __constant__ double c_rmTinv2[Q][5];
 __constant__ float c_gsMinvF[Q][Q];
 __constant__ float c_rmTinv2F[Q][5];
 
+// host copies of those tables.  Without relocatable device code every
+// translation unit that includes this header owns its own __constant__
+// copies, so each one uploads them (uploadTables is static per unit), once
+// per device.
+struct ConstTables {
+    uint32_t masks[54];
+    double gsi[Q * Q], mw[Q], rm2[Q][5];
+    float gsiF[Q * Q], rm2F[Q][5];
+};
+int makeConstTables(ConstTables& t);
+static inline int uploadTables(const ConstTables& t) {
+    if (cudaMemcpyToSymbol(c_pushMask, t.masks, sizeof t.masks) != cudaSuccess) return -2;
+    if (cudaMemcpyToSymbol(c_gsMinv, t.gsi, sizeof t.gsi) != cudaSuccess) return -2;
+    if (cudaMemcpyToSymbol(c_gsMw, t.mw, sizeof t.mw) != cudaSuccess) return -2;
+    if (cudaMemcpyToSymbol(c_rmTinv2, t.rm2, sizeof t.rm2) != cudaSuccess) return -2;
+    if (cudaMemcpyToSymbol(c_gsMinvF, t.gsiF, sizeof t.gsiF) != cudaSuccess) return -2;
+    if (cudaMemcpyToSymbol(c_rmTinv2F, t.rm2F, sizeof t.rm2F) != cudaSuccess) return -2;
+    return 0;
+}
+
 // pre-collision moments of a node
 template <typename R>
 struct MomR {
@@ -371,9 +391,9 @@ struct Pusher {
 // collide + push for operators without neighbour data (SRT, RR, MRT): one
 // thread per node, x fastest so each direction's loads and stores coalesce
 template <typename S, typename R, int OP, int ORDER, bool CUBIC, bool MRTWB>
-__global__ void __launch_bounds__(128) k_collide_push(LevelArgs<S> a) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y, k = blockIdx.z;
+__device__ __forceinline__ void collidePushBody(const LevelArgs<S>& a, int bx, int by, int bz) {
+    const int i = bx * blockDim.x + threadIdx.x;
+    const int j = by, k = bz;
     if (i >= a.nx) return;
     const int n = (k * a.ny + j) * a.nx + i;
     const uint8_t code = a.code[n];
@@ -390,6 +410,11 @@ __global__ void __launch_bounds__(128) k_collide_push(LevelArgs<S> a) {
         for (int q = 0; q < Q; ++q) emit(q, g[q]);
     }
 }
+template <typename S, typename R, int OP, int ORDER, bool CUBIC, bool MRTWB>
+__global__ void __launch_bounds__(128) k_collide_push(LevelArgs<S> a) {
+    collidePushBody<S, R, OP, ORDER, CUBIC, MRTWB>(a, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
 
 // ---------------------------------------------------------------------------
 // collide + push for the operators that read the six axis neighbours'
@@ -591,9 +616,9 @@ struct TiledSlots {
 };
 
 template <typename S, typename R, int OP, int ORDER, bool CUBIC>
-__global__ void __launch_bounds__(TX * TY, TiledMinBlocks<R>::value) k_collide_push_tiled(LevelArgs<S> a, int zChunk) {
+__device__ __forceinline__ void tiledBody(const LevelArgs<S>& a, int zChunk, int bx, int by, int bz) {
     __shared__ MomR<R> sm[TiledSlots<R>::value][TY + 2][TX + 2];
-    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+    const int x0 = bx * TX, y0 = by * TY;
     const int i = x0 + threadIdx.x, j = y0 + threadIdx.y;
     const bool mine = i < a.nx && j < a.ny;
     if (a.per[2] && a.nz <= 3) {
@@ -644,7 +669,7 @@ __global__ void __launch_bounds__(TX * TY, TiledMinBlocks<R>::value) k_collide_p
         }
         return;
     }
-    const int zBeg = blockIdx.z * zChunk;
+    const int zBeg = bz * zChunk;
     const int zEnd = min(a.nz, zBeg + zChunk);
     // rolling planes: slot of the unwrapped plane u in [zBeg-1, zEnd] is (u - zBeg + 1) mod 4
     auto key = [&](int u) { return (u - zBeg + 1) & 3; };
@@ -662,6 +687,11 @@ __global__ void __launch_bounds__(TX * TY, TiledMinBlocks<R>::value) k_collide_p
         for (int c = 0; c < 6; ++c) cur[c] = nxt[c];
     }
 }
+template <typename S, typename R, int OP, int ORDER, bool CUBIC>
+__global__ void __launch_bounds__(TX * TY, TiledMinBlocks<R>::value) k_collide_push_tiled(LevelArgs<S> a, int zChunk) {
+    tiledBody<S, R, OP, ORDER, CUBIC>(a, zChunk, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
 
 // ---------------------------------------------------------------------------
 // LODI characteristic pressure boundary (Node::LODIpressureOutlet and
@@ -700,9 +730,9 @@ __device__ __forceinline__ void absMoments(const S* arr, long long N, long long 
 }
 
 template <typename S, int ORDER>
-__global__ void k_lodi(const S* __restrict__ A, S* B, const BNodeDev* __restrict__ nodes, int count, LodiArgs p,
-                       LevelArgs<S> la) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void lodiBody(const S* __restrict__ A, S* B, const BNodeDev* __restrict__ nodes, int count,
+                                         const LodiArgs& p, const LevelArgs<S>& la, int bx) {
+    const int t = bx * blockDim.x + threadIdx.x;
     if (t >= count) return;
     const BNodeDev b = nodes[t];
     const float* hs = la.hscale;
@@ -779,6 +809,12 @@ __global__ void k_lodi(const S* __restrict__ A, S* B, const BNodeDev* __restrict
         Store<S>::store(B + q * p.N + b.n, (decltype(Store<S>::load(B, 1.f)))geq, hs[q]);
     }
 }
+template <typename S, int ORDER>
+__global__ void k_lodi(const S* __restrict__ A, S* B, const BNodeDev* __restrict__ nodes, int count, LodiArgs p,
+                       LevelArgs<S> la) {
+    lodiBody<S, ORDER>(A, B, nodes, count, p, la, blockIdx.x);
+}
+
 
 // ---------------------------------------------------------------------------
 // initial condition (Lattice::initialization, Lattice.cpp:1397-1493): f is
@@ -952,20 +988,27 @@ __device__ __forceinline__ void rescaleNeq(R* neq, const CouplingArgs& c, bool t
 
 // populations of the coincident coupling sources before the coarse step
 template <typename S, typename R>
-__global__ void k_c2f_save(const S* __restrict__ Ac, const C2FDev* __restrict__ nodes, int count, R* pre,
-                           LevelArgs<S> la) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void c2fSaveBody(const S* __restrict__ Ac, const C2FDev* __restrict__ nodes, int count, R* pre,
+                                            const LevelArgs<S>& la, int bx) {
+    const int t = bx * blockDim.x + threadIdx.x;
     if (t >= count) return;
     const int src = nodes[t].src;
 #pragma unroll
     for (int q = 0; q < Q; ++q) pre[(long long)q * count + t] = R(Store<S>::load(Ac + (long long)q * la.N + src, la.hscale[q]));
 }
+template <typename S, typename R>
+__global__ void k_c2f_save(const S* __restrict__ Ac, const C2FDev* __restrict__ nodes, int count, R* pre,
+                           LevelArgs<S> la) {
+    c2fSaveBody<S, R>(Ac, nodes, count, pre, la, blockIdx.x);
+}
+
 
 // C2F on the fine nodes at coarse positions: coarse state at (1-th)*t + th*(t+1)
 template <typename S, typename R, int ORDER>
-__global__ void k_c2f_coincident(const S* __restrict__ Bc, S* Ff, const C2FDev* __restrict__ nodes, int count,
-                                 const R* __restrict__ pre, R th, CouplingArgs c, LevelArgs<S> la) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void c2fCoincidentBody(const S* __restrict__ Bc, S* Ff, const C2FDev* __restrict__ nodes, int count,
+                                                  const R* __restrict__ pre, R th, const CouplingArgs& c,
+                                                  const LevelArgs<S>& la, int bx) {
+    const int t = bx * blockDim.x + threadIdx.x;
     if (t >= count) return;
     const C2FDev nd = nodes[t];
     R g[Q], geq[Q];
@@ -982,13 +1025,20 @@ __global__ void k_c2f_coincident(const S* __restrict__ Bc, S* Ff, const C2FDev* 
     for (int q = 0; q < Q; ++q)
         if (nd.mask >> q & 1u) Store<S>::store(Ff + (long long)q * c.Nf + nd.n, geq[q] + g[q], la.hscale[q]);
 }
+template <typename S, typename R, int ORDER>
+__global__ void k_c2f_coincident(const S* __restrict__ Bc, S* Ff, const C2FDev* __restrict__ nodes, int count,
+                                 const R* __restrict__ pre, R th, CouplingArgs c, LevelArgs<S> la) {
+    c2fCoincidentBody<S, R, ORDER>(Bc, Ff, nodes, count, pre, th, c, la, blockIdx.x);
+}
+
 
 // C2F on the other fine coupling nodes: interpolation along the face from
 // the nodes written before (mid nodes from coincident ones, centre nodes from
 // mid nodes); one thread per (node, population)
 template <typename S, typename R>
-__global__ void k_c2f_interp(S* Ff, const C2FDev* __restrict__ nodes, int count, CouplingArgs c, LevelArgs<S> la) {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void c2fInterpBody(S* Ff, const C2FDev* __restrict__ nodes, int count, const CouplingArgs& c,
+                                              const LevelArgs<S>& la, int bx) {
+    const long long t = (long long)bx * blockDim.x + threadIdx.x;
     if (t >= (long long)count * Q) return;
     const int q = (int)(t / count);
     const int m = (int)(t - (long long)q * count);
@@ -1000,13 +1050,18 @@ __global__ void k_c2f_interp(S* Ff, const C2FDev* __restrict__ nodes, int count,
         if (nd.st[k] >= 0) acc += R(nd.w[k]) * R(Store<S>::load(Ff + (long long)q * c.Nf + nd.st[k], la.hscale[q]));
     Store<S>::store(Ff + (long long)q * c.Nf + nd.n, acc, la.hscale[q]);
 }
+template <typename S, typename R>
+__global__ void k_c2f_interp(S* Ff, const C2FDev* __restrict__ nodes, int count, CouplingArgs c, LevelArgs<S> la) {
+    c2fInterpBody<S, R>(Ff, nodes, count, c, la, blockIdx.x);
+}
+
 
 // F2C on the coarse nodes one cell inside the fine box: one warp per coarse
 // node, lane m < 27 forms the weighted non-equilibrium of fine neighbour m
 template <typename S, typename R, int ORDER>
-__global__ void k_f2c(const S* __restrict__ Ff, S* Bc, const F2CDev* __restrict__ nodes, int count, CouplingArgs c,
-                      LevelArgs<S> la) {
-    const int warp = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+__device__ __forceinline__ void f2cBody(const S* __restrict__ Ff, S* Bc, const F2CDev* __restrict__ nodes, int count,
+                                        const CouplingArgs& c, const LevelArgs<S>& la, int bx) {
+    const int warp = (int)(((long long)bx * blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
     if (warp >= count) return;  // uniform per warp
     const F2CDev& nd = nodes[warp];
@@ -1041,6 +1096,12 @@ __global__ void k_f2c(const S* __restrict__ Ff, S* Bc, const F2CDev* __restrict_
     for (int q = 0; q < Q; ++q)
         if (nd.mask >> q & 1u) Store<S>::store(Bc + (long long)q * c.Nc + nd.n, geq[q] + neq[q], la.hscale[q]);
 }
+template <typename S, typename R, int ORDER>
+__global__ void k_f2c(const S* __restrict__ Ff, S* Bc, const F2CDev* __restrict__ nodes, int count, CouplingArgs c,
+                      LevelArgs<S> la) {
+    f2cBody<S, R, ORDER>(Ff, Bc, nodes, count, c, la, blockIdx.x);
+}
+
 
 // ---------------------------------------------------------------------------
 // direct coupling (Coupling-Approach DC1 / DC2, Overlap 0).  The reference
@@ -1080,9 +1141,9 @@ __device__ __forceinline__ void regulariseNeq(const R* neq, R* out) {
 // th < 1: the fine side at t+1/2 (coarse state blended in time with the
 // saved pre-step state); th == 1: both sides at t+1.  One thread per shared node.
 template <typename S, typename R, int ORDER>
-__global__ void k_dc_couple(S* Bc, S* Ff, const DCDev* __restrict__ nodes, int count, const R* __restrict__ pre,
-                            R th, int dc2, CouplingArgs c, LevelArgs<S> la) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void dcCoupleBody(S* Bc, S* Ff, const DCDev* __restrict__ nodes, int count, const R* __restrict__ pre,
+                                             R th, int dc2, const CouplingArgs& c, const LevelArgs<S>& la, int bx) {
+    const int t = bx * blockDim.x + threadIdx.x;
     if (t >= count) return;
     const DCDev& nd = nodes[t];
     const bool full = th == R(1);
@@ -1166,5 +1227,11 @@ __global__ void k_dc_couple(S* Bc, S* Ff, const DCDev* __restrict__ nodes, int c
                                 la.hscale[q]);
     }
 }
+template <typename S, typename R, int ORDER>
+__global__ void k_dc_couple(S* Bc, S* Ff, const DCDev* __restrict__ nodes, int count, const R* __restrict__ pre,
+                            R th, int dc2, CouplingArgs c, LevelArgs<S> la) {
+    dcCoupleBody<S, R, ORDER>(Bc, Ff, nodes, count, pre, th, dc2, c, la, blockIdx.x);
+}
+
 
 }  // namespace acp

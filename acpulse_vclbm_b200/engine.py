@@ -53,6 +53,15 @@ def lib():
         L.acp_status_string.argtypes = [C.c_int]
         L.acp_status_string.restype = C.c_char_p
         L.acp_abi_version.restype = C.c_int
+        L.acp_batch_create.argtypes = [vp, C.c_int, C.POINTER(vp)]
+        L.acp_batch_step.argtypes = [vp, C.c_int]
+        L.acp_batch_sync.argtypes = [vp]
+        L.acp_batch_tune.argtypes = [vp, C.c_int, C.c_char_p, C.c_size_t]
+        L.acp_batch_configure.argtypes = [vp, C.c_int, C.c_int, C.c_int]
+        L.acp_batch_info.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_longlong)]
+        L.acp_batch_destroy.argtypes = [vp]
+        L.acp_batch_last_error.argtypes = [vp]
+        L.acp_batch_last_error.restype = C.c_char_p
         _LIB = L
     return _LIB
 
@@ -149,8 +158,67 @@ class Lattice:
 
     def close(self):
         if getattr(self, "_h", None) and self._h.value:
+            if getattr(self, "_batch", None) is not None:
+                self._batch.close()
             lib().acp_destroy(self._h)
             self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Initialised lattices advanced together (acp_batch_*): one CUDA graph
+    per coarse step, every phase one persistent launch per group of cases
+    with the same kernels.  The lattices stay readable; they are stepped
+    only through the batch until it is closed."""
+
+    def __init__(self, lattices):
+        self.lattices = list(lattices)
+        arr = (C.c_void_p * len(self.lattices))(*[L._h.value for L in self.lattices])
+        self._b = C.c_void_p()
+        s = lib().acp_batch_create(arr, len(self.lattices), C.byref(self._b))
+        if s != ACP_OK:
+            msg = lib().acp_batch_last_error(self._b).decode() if self._b else ""
+            self.close()
+            raise AcpError(s, msg)
+        for L in self.lattices:
+            L._batch = self
+
+    def _check(self, s):
+        if s != ACP_OK:
+            raise AcpError(s, lib().acp_batch_last_error(self._b).decode())
+
+    def step(self, n=1):
+        self._check(lib().acp_batch_step(self._b, n))
+
+    def sync(self):
+        self._check(lib().acp_batch_sync(self._b))
+
+    def tune(self, trial_steps=5):
+        """Time every candidate schedule over trial_steps real coarse steps
+        each (the cases advance) and keep the fastest; returns the report."""
+        rep = C.create_string_buffer(4096)
+        self._check(lib().acp_batch_tune(self._b, trial_steps, rep, 4096))
+        return rep.value.decode()
+
+    def configure(self, persist=0, largest_first=False, chunk_scale=1):
+        self._check(lib().acp_batch_configure(self._b, persist, int(largest_first), chunk_scale))
+
+    def info(self):
+        g, l, u = C.c_int(), C.c_int(), C.c_longlong()
+        self._check(lib().acp_batch_info(self._b, C.byref(g), C.byref(l), C.byref(u)))
+        return {"groups": g.value, "launches_per_step": l.value, "updates_per_step": u.value}
+
+    def close(self):
+        if getattr(self, "_b", None) and self._b.value:
+            lib().acp_batch_destroy(self._b)
+            self._b = C.c_void_p()
+            for L in self.lattices:
+                L._batch = None
 
     def __del__(self):
         try:

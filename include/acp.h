@@ -202,6 +202,36 @@ int acp_boundary_wiring(const acp_case_desc* d, long long* rows, long long max_r
  * streams) race and must be serialised by the caller.  Nothing in it needs to
  * start at zero; each call overwrites the part it reads back. */
 int acp_read_populations_window(acp_handle* h, int level, long long node_begin, int node_count, double* host_out);
+/* ---- batched form --------------------------------------------------------
+ * Many initialised cases of uneven sizes, operators, storage forms and
+ * refinement layouts advance together: cases with the same kernel templates
+ * form a group, each group runs its phases as one persistent launch per phase
+ * over all of its cases, groups run side by side, and one coarse step of the
+ * whole batch is one CUDA graph launch.  There is no counterpart in the
+ * reference, which runs one case per process (main.cpp:37-271).  While a case
+ * belongs to a batch, acp_step on it returns ACP_ERR_STATE; the reading calls
+ * (acp_sync, acp_read_*) wait for the batch's work.  Results are the same as
+ * stepping each case alone. */
+typedef struct acp_batch acp_batch;
+int acp_batch_create(acp_handle* const* cases, int n, acp_batch** out);
+/* n coarse steps of every case, asynchronous on the batch's stream. */
+int acp_batch_step(acp_batch* b, int n_coarse_steps);
+/* Wait for the batch and report the first case's numeric fault, if any. */
+int acp_batch_sync(acp_batch* b);
+/* Autotuner: time every candidate schedule (persistent grid of 1/2/4 x the
+ * resident blocks or one block per work item; cases in given or descending-
+ * size order; tiled z chunk x1 or x2 for 3-D cases) over trial_steps real
+ * coarse steps each (the cases advance), keep the fastest and write one line
+ * per candidate into report (may be NULL). */
+int acp_batch_tune(acp_batch* b, int trial_steps, char* report, size_t report_len);
+/* Set the schedule explicitly (persist 0: one block per work item). */
+int acp_batch_configure(acp_batch* b, int persist, int largest_first, int chunk_scale);
+/* Groups, kernel launches per coarse step, node updates per coarse step. */
+int acp_batch_info(acp_batch* b, int* groups, int* launches_per_step, long long* updates_per_step);
+/* Releases the batch; its cases stay valid and can be stepped alone again. */
+int acp_batch_destroy(acp_batch* b);
+const char* acp_batch_last_error(const acp_batch* b);
+
 int acp_destroy(acp_handle* h);
 const char* acp_last_error(const acp_handle* h);
 const char* acp_status_string(int status);
