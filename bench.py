@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--filter", default="LAG")
     ap.add_argument("--coupling", default="STD", choices=["STD", "DC1", "DC2"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batched-cases", type=int, default=64, help="cases of the batched form (0: skip)")
+    ap.add_argument("--serve-requests", type=int, default=16, help="requests of the serving form (0: skip)")
     return ap.parse_args()
 
 
@@ -223,6 +225,65 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def bench_batched(args, engine, torch, device, peak):
+    """The batched form: seeded quasi-2D cases of uneven sizes and operators
+    (FP32 deviation), one CUDA graph per coarse step, schedule chosen by the
+    autotuner; beside it the same cases stepped one after the other."""
+    from acpulse_vclbm_b200 import workloads
+    descs = workloads.batched_cases(seed=2024, n=args.batched_cases)
+    Ls = [engine.Lattice(d, device=device).init() for d in descs]
+    B = engine.Batch(Ls)
+    report = B.tune(trial_steps=3)
+    info = B.info()
+    steps = max(20, args.steps // 2)
+    B.step(3)
+    B.sync()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    B.step(steps)
+    B.sync()
+    batched_s = (time.perf_counter() - t0) / steps
+    B.close()
+    # the same cases stepped one by one (each its own CUDA graph), for comparison
+    n1 = 10
+    for L in Ls:
+        L.step(1)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for L in Ls:
+        L.step(n1)
+    for L in Ls:
+        L.sync()
+    alone_s = (time.perf_counter() - t0) / n1
+    for L in Ls:
+        L.close()
+    upd = info["updates_per_step"]
+    mlups = upd / batched_s / 1e6
+    achieved = upd * 152 / batched_s / 1e9
+    return {"cases": len(descs), "seed": 2024, "groups": info["groups"],
+            "launches_per_step": info["launches_per_step"], "updates_per_step": upd,
+            "mlups": round(mlups, 1), "ms_per_step": batched_s * 1e3,
+            "hbm_frac_whole_step": round(achieved / peak, 4), "achieved_gbs_whole_step": round(achieved, 1),
+            "alone_sequential_mlups": round(upd / alone_s / 1e6, 1),
+            "speedup_over_sequential": round(alone_s / batched_s, 2),
+            "tuner": report.strip().split("\n")[-1],
+            "timing": "host clock around synchronised graph launches"}
+
+
+def bench_serving(args, engine, device):
+    """The serving form: a seeded Poisson stream of 3-D patch solves, FP32
+    deviation and FP64 side by side, continuous batching under a 40 GB budget."""
+    from acpulse_vclbm_b200 import serve, workloads
+    stream = workloads.request_stream(seed=7, n=args.serve_requests, rate_hz=4.0, size_range=(32, 96),
+                                      steps_range=(200, 2000))
+    reqs = [serve.Request(k, t, d, n) for k, (t, d, n) in enumerate(stream)]
+    s = serve.Server(budget_bytes=40 << 30, tick_steps=50, device=device)
+    rep = s.run(reqs)
+    rep["stream"] = (f"{len(reqs)} requests, Poisson 4/s (seed 7), 3-D boxes 32^3-96^3 with a centred 2:1 patch, "
+                     "200-2000 coarse steps, FP32-DEV / FP64 alternating, 5 operators")
+    return rep
+
+
 def run_engine(args):
     import torch
     dist, rank = dist_setup(args.gpus)
@@ -298,6 +359,11 @@ def run_engine(args):
     Le.close()
     e2e = nodes * args.steps / (t1 - t0) / 1e6
 
+    batched = serving = None
+    if rank == 0 and args.batched_cases > 0:
+        batched = bench_batched(args, engine, torch, local, peak)
+    if rank == 0 and args.serve_requests > 0:
+        serving = bench_serving(args, engine, local)
     mlups32 = nodes * args.steps / (ms32 * 1e-3) / 1e6 * args.gpus
     mlups64 = nodes * args.steps / (ms64 * 1e-3) / 1e6 * args.gpus
     cpu = None
@@ -323,7 +389,9 @@ def run_engine(args):
                 "e2e": {"value": round(e2e, 2), "unit": "MLUPS", "h2d_bytes_per_step": h2d // args.steps,
                         "d2h_bytes_per_step": d2h // args.steps},
                 "gpu_launches": lps.value * args.steps,
-                "clocks": clk}
+                "clocks": clk,
+                "batched": batched,
+                "serving": serving}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
