@@ -530,20 +530,11 @@ void enqueueGroup(acp_batch* b, Group& g, int flip) {
 // pressure probes of a case after the step (as the single-case engine samples them)
 void enqueueProbes(const acp_batch* b, acp_handle* h, cudaStream_t st, int flip) {
     if (!h->nProbes) return;
-    const int l = h->probeLevel;
     const int coarseNew = 1 - (h->cur ^ b->flip ^ flip);
-    auto launch = [&](auto tag) {
-        using S = decltype(tag);
-        LevelArgs<S> a = levelArgs<S>(h, l, 0);
-        const S* arr = (const S*)h->dev[l].f[l == 0 ? coarseNew : 0];
-        k_probes<S><<<1, 128, 0, st>>>(arr, a, h->dProbeNodes, h->nProbes, h->shift,
-                                       h->d.speed_of_sound * h->d.speed_of_sound, h->dSeries, h->dCounter,
-                                       h->probeCapacity);
-    };
     switch (h->d.storage) {
-        case ACP_STORE_F64: launch(double()); break;
-        case ACP_STORE_F32_DEV: launch(float()); break;
-        default: launch(__half()); break;
+        case ACP_STORE_F64: launchProbes<double>(h, st, coarseNew); break;
+        case ACP_STORE_F32_DEV: launchProbes<float>(h, st, coarseNew); break;
+        default: launchProbes<__half>(h, st, coarseNew); break;
     }
 }
 

@@ -108,7 +108,35 @@ struct EqCoef {
         if (ORDER == 4) p += R(20.25) * h4dot<R>(q, a4, kappa);
         return p;
     }
+    // the same polynomial split into its even (second and fourth order) and
+    // odd (first and third order) parts: direction q gives even + odd, its
+    // opposite even - odd
+    __device__ __forceinline__ void evenOdd(int q, R kappa, R& even, R& odd) const {
+        odd = R(3) * (R(ex(q)) * u[0] + R(ey(q)) * u[1] + R(ez(q)) * u[2]);
+        if (ORDER >= 3) odd += R(4.5) * h3dot<R>(q, a3);
+        even = R(4.5) * h2dot<R>(q, uu);
+        if (ORDER == 4) even += R(20.25) * h4dot<R>(q, a4, kappa);
+    }
 };
+
+// the nine pairs of opposite directions (FluidNode.h:43-62); the rest
+// direction 18 is its own opposite
+__host__ __device__ constexpr int pairA(int p) { return p == 0 ? 0 : p == 1 ? 1 : p == 2 ? 4 : p == 3 ? 6 : p == 4 ? 7 : p == 5 ? 8 : p == 6 ? 9 : p == 7 ? 14 : 16; }
+__host__ __device__ constexpr int pairB(int p) { return p == 0 ? 2 : p == 1 ? 3 : p == 2 ? 5 : p == 3 ? 11 : p == 4 ? 10 : p == 5 ? 13 : p == 6 ? 12 : p == 7 ? 15 : 17; }
+
+// visit (q, value) for every direction of a polynomial given per pair as
+// even +- odd: f(q, even + odd), f(opposite, even - odd), then the rest
+template <typename R, int ORDER, typename F>
+__device__ __forceinline__ void forEachDirection(const EqCoef<R, ORDER>& c, R kappa, F&& f) {
+#pragma unroll
+    for (int p = 0; p < 9; ++p) {
+        R even, odd;
+        c.evenOdd(pairA(p), kappa, even, odd);
+        f(pairA(p), even + odd);
+        f(pairB(p), even - odd);
+    }
+    f(18, c.poly(18, kappa));
+}
 
 // Recursive off-equilibrium of a second-order coefficient tensor A
 // (RR: A = Pi1; HRR: A = hybrid of Pi1 and the finite-difference strain).

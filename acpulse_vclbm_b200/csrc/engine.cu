@@ -716,12 +716,7 @@ int enqueueStepT(acp_handle* h, int src, PhaseTimer* tm) {
         if (tm) tm->mark(ACP_K_COUPLING);
     }
     if (h->nProbes) {
-        const int l = h->probeLevel;
-        LevelArgs<S> a = levelArgs<S>(h, l, 0);
-        const S* cur = (const S*)h->dev[l].f[l == 0 ? 1 - src : 0];
-        k_probes<S><<<1, 128, 0, h->stream>>>(cur, a, h->dProbeNodes, h->nProbes, h->shift,
-                                             h->d.speed_of_sound * h->d.speed_of_sound, h->dSeries, h->dCounter,
-                                             h->probeCapacity);
+        launchProbes<S>(h, h->stream, 1 - src);
         if (tm) tm->mark(ACP_K_PROBES);
     }
     return ACP_OK;
@@ -1154,33 +1149,37 @@ int acp_read_field(acp_handle* h, int level, int field, double* out) {
 
 int acp_set_probes(acp_handle* h, int n, const int* lijk) {
     if (!h || n < 0 || (n > 0 && !lijk)) return ACP_ERR_INVALID;
+    if (h->batch) return fail(h, ACP_ERR_STATE, "the case belongs to a batch");
     CU(h, cudaSetDevice(h->device));
     std::vector<long long> nodes(n);
-    int level = n ? lijk[0] : 0;
+    std::vector<int> levels(n);
     for (int m = 0; m < n; ++m) {
         const int l = lijk[4 * m];
-        if (l != level || l < 0 || l >= (int)h->host.size())
-            return fail(h, ACP_ERR_INVALID, "probes must all lie on one existing level");
+        if (l < 0 || l >= (int)h->host.size()) return fail(h, ACP_ERR_INVALID, "probe %d: no level %d", m, l);
         const LevelHost& L = h->host[l];
         const int i = lijk[4 * m + 1] - L.off[0], j = lijk[4 * m + 2] - L.off[1], k = lijk[4 * m + 3] - L.off[2];
         if (i < 0 || i >= L.nx || j < 0 || j >= L.ny || k < 0 || k >= L.nz)
             return fail(h, ACP_ERR_INVALID, "probe %d outside its level", m);
         nodes[m] = ((long long)k * L.ny + j) * L.nx + i;
+        if (L.code[nodes[m]] == CODE_DEAD) return fail(h, ACP_ERR_INVALID, "probe %d on a node covered by the fine level", m);
+        levels[m] = l;
     }
     if (h->dProbeNodes) { cudaFree(h->dProbeNodes); h->dProbeNodes = nullptr; }
+    if (h->dProbeLevels) { cudaFree(h->dProbeLevels); h->dProbeLevels = nullptr; }
     if (h->dSeries) { cudaFree(h->dSeries); h->dSeries = nullptr; }
     if (!h->dCounter) {
         int s = devAlloc(h, (void**)&h->dCounter, sizeof(int));
         if (s) return s;
     }
     h->nProbes = n;
-    h->probeLevel = level;
     h->probeCapacity = 1 << 16;
     if (n) {
         int s = devAlloc(h, (void**)&h->dProbeNodes, n * sizeof(long long));
         if (s) return s;
+        if ((s = devAlloc(h, (void**)&h->dProbeLevels, n * sizeof(int)))) return s;
         if ((s = devAlloc(h, (void**)&h->dSeries, (size_t)n * h->probeCapacity * sizeof(double)))) return s;
         CU(h, cudaMemcpyAsync(h->dProbeNodes, nodes.data(), n * sizeof(long long), cudaMemcpyHostToDevice, h->stream));
+        CU(h, cudaMemcpyAsync(h->dProbeLevels, levels.data(), n * sizeof(int), cudaMemcpyHostToDevice, h->stream));
     }
     CU(h, cudaMemsetAsync(h->dCounter, 0, sizeof(int), h->stream));
     CU(h, cudaStreamSynchronize(h->stream));
@@ -1318,6 +1317,7 @@ int acp_destroy(acp_handle* h) {
     cudaFree(h->dDC);
     cudaFree(h->dPre);
     cudaFree(h->dProbeNodes);
+    cudaFree(h->dProbeLevels);
     cudaFree(h->dSeries);
     cudaFree(h->dCounter);
     if (h->ownStream && h->stream) cudaStreamDestroy(h->stream);

@@ -66,11 +66,11 @@ struct acp_handle {
     int* dErr = nullptr;
     // probes
     long long* dProbeNodes = nullptr;
+    int* dProbeLevels = nullptr;
     int nProbes = 0;
     double* dSeries = nullptr;
     int* dCounter = nullptr;
     int probeCapacity = 0;
-    int probeLevel = 0;
     size_t devBytes = 0;
     std::string err;
     double c = 0, kappa = 0, shift = 0;
@@ -165,6 +165,18 @@ cudaEvent_t batchDoneEvent(acp_batch* b);
 // a case stepped by a batch: order the case's own stream after the batch's work
 inline void joinBatch(acp_handle* h) {
     if (h && h->batch) cudaStreamWaitEvent(h->stream, batchDoneEvent(h->batch), 0);
+}
+
+// probe sampling after a step whose coarse level wrote array coarseNew
+template <typename S>
+void launchProbes(const acp_handle* h, cudaStream_t st, int coarseNew) {
+    LevelArgs<S> a = levelArgs<S>(h, 0, 0);
+    const S* fine = h->host.size() > 1 ? (const S*)h->dev[1].f[0] : nullptr;
+    const long long Nf = h->host.size() > 1 ? h->host[1].N : 0;
+    k_probes<S><<<1, 128, 0, st>>>((const S*)h->dev[0].f[coarseNew], h->host[0].N, fine, Nf, a, h->dProbeNodes,
+                                   h->dProbeLevels, h->nProbes, h->shift,
+                                   h->d.speed_of_sound * h->d.speed_of_sound, h->dSeries, h->dCounter,
+                                   h->probeCapacity);
 }
 
 inline bool needsMoments(const acp_case_desc& d) { return d.op == OP_HRR || (d.op == OP_RR && d.cubic_mach); }

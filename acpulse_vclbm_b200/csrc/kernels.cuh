@@ -215,8 +215,7 @@ __device__ __forceinline__ void regularisedEmit(R drho, const R* u, const R* s2,
 #pragma unroll
         for (int c = 0; c < 3; ++c) mc.a4[c] = rho * ec.a4[c] + om1 * nc.a4[c];
     }
-#pragma unroll
-    for (int q = 0; q < Q; ++q) emit(q, R(wq(q)) * (drho + mc.poly(q, kappa)));
+    forEachDirection<R, ORDER>(mc, kappa, [&](int q, R poly) { emit(q, R(wq(q)) * (drho + poly)); });
 }
 
 template <typename R, int OP, int ORDER, bool CUBIC, bool MRTWB>
@@ -329,11 +328,10 @@ struct Collider {
         if (OP == OP_SRT) {
             EqCoef<R, ORDER> ec;
             ec.set(u, kappa);
-#pragma unroll
-            for (int q = 0; q < Q; ++q) {
-                const R geq = R(wq(q)) * (drho + rho * ec.poly(q, kappa));
+            forEachDirection<R, ORDER>(ec, kappa, [&](int q, R poly) {
+                const R geq = R(wq(q)) * (drho + rho * poly);
                 emit(q, g[q] + omega * (geq - g[q]));
-            }
+            });
             return;
         }
 
@@ -887,16 +885,20 @@ __global__ void k_from_f64(const double* __restrict__ src, S* dst0, S* dst1, lon
 }
 
 // pressure probes: p = rho cs^2 (Node::calcPressure, Node.cpp:64-83) at each
-// probe after the step, appended to an FP64 series
+// probe after the step, appended to an FP64 series; a probe reads the coarse
+// array (level 0) or the fine one (level 1)
 template <typename S>
-__global__ void k_probes(const S* __restrict__ arr, LevelArgs<S> la, const long long* nodes, int count, double shift,
+__global__ void k_probes(const S* __restrict__ coarse, long long Nc, const S* __restrict__ fine, long long Nf,
+                         LevelArgs<S> la, const long long* nodes, const int* levels, int count, double shift,
                          double cs2, double* series, int* counter, int capacity) {
     const int t = threadIdx.x;
     const int s = *counter;
     for (int m = t; m < count; m += blockDim.x) {
+        const S* arr = levels[m] ? fine : coarse;
+        const long long N = levels[m] ? Nf : Nc;
         double d = 0;
 #pragma unroll
-        for (int q = 0; q < Q; ++q) d += (double)Store<S>::load(arr + q * la.N + nodes[m], la.hscale[q]);
+        for (int q = 0; q < Q; ++q) d += (double)Store<S>::load(arr + q * N + nodes[m], la.hscale[q]);
         if (s < capacity) series[(long long)s * count + m] = (shift + d) * cs2;
     }
     __syncthreads();

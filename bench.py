@@ -160,12 +160,11 @@ def ncu_traffic(kernel_key):
 
 
 def dist_setup(n):
+    """replicas, one rank per GPU (NCCL); no lattice data crosses ranks"""
     if n <= 1:
         return None, 0
-    import torch.distributed as dist
-    import datetime
-    rank = int(os.environ.get("RANK", "0"))
-    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from acpulse_vclbm_b200 import replicas
+    dist, rank, _ = replicas.init("nccl", timeout_s=120)
     return dist, rank
 
 
@@ -313,9 +312,8 @@ def run_engine(args):
     ms64 = time_gpu(L64, args.steps, args.warmup, torch, tstream)
     clk = clocks.stop()
     if dist:
-        t = torch.tensor([ms32, ms64], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms32, ms64 = t.tolist()
+        from acpulse_vclbm_b200 import replicas
+        ms32, ms64 = replicas.reduce([ms32, ms64], dist, "max", device="cuda")
 
     # accuracy of the FP32 deviation form against FP64 after the same steps
     cs2 = d64.speed_of_sound ** 2
@@ -394,8 +392,8 @@ def run_engine(args):
                 "serving": serving}
         print(json.dumps(line), flush=True)
     if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+        from acpulse_vclbm_b200 import replicas
+        replicas.finish(dist)
 
 
 if __name__ == "__main__":

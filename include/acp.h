@@ -153,7 +153,9 @@ int acp_read_populations(acp_handle* h, int level, double* host_out);
 int acp_write_populations(acp_handle* h, int level, const double* host_in);
 /* A macroscopic field of a level (SI: kg/m^3, m/s, Pa), host buffer of nodes doubles. */
 int acp_read_field(acp_handle* h, int level, int field, double* host_out);
-/* Pressure probes: n probes at (level, i, j, k) quadruples; sampled after every coarse step into an FP64 device buffer. */
+/* Pressure probes: n probes at (level, i, j, k) quadruples, i j k in the
+ * level's global node indices (fine: twice the coarse ones), on either level;
+ * sampled after every coarse step into an FP64 device buffer. */
 int acp_set_probes(acp_handle* h, int n, const int* level_ijk);
 /* Copy the probe series: out[sample * n + probe] in Pa; *n_samples set to the count. */
 int acp_read_probes(acp_handle* h, double* out, int max_samples, int* n_samples);
@@ -210,8 +212,9 @@ int acp_read_populations_window(acp_handle* h, int level, long long node_begin, 
  * whole batch is one CUDA graph launch.  There is no counterpart in the
  * reference, which runs one case per process (main.cpp:37-271).  While a case
  * belongs to a batch, acp_step on it returns ACP_ERR_STATE; the reading calls
- * (acp_sync, acp_read_*) wait for the batch's work.  Results are the same as
- * stepping each case alone. */
+ * (acp_sync, acp_read_*) wait for the batch's work.  Results are those of
+ * stepping each case alone, to rounding (the same device code, inlined into
+ * other kernels, may contract a multiply-add differently). */
 typedef struct acp_batch acp_batch;
 int acp_batch_create(acp_handle* const* cases, int n, acp_batch** out);
 /* n coarse steps of every case, asynchronous on the batch's stream. */

@@ -1200,6 +1200,24 @@ int orc_write_populations(void* h, int level, const double* in) {
 
 long long orc_steps_done(void* h) { return static_cast<Oracle*>(h)->steps; }
 
+// pressure p = rho cs^2 (Node::calcPressure, Node.cpp:64-83) of the current
+// state at probes (level, i, j, k) in the level's global node indices
+int orc_probe_pressures(void* h, int n, const int* lijk, double* out) {
+    Oracle* o = static_cast<Oracle*>(h);
+    for (int m = 0; m < n; ++m) {
+        const int l = lijk[4 * m];
+        if (l < 0 || l >= (int)o->lev.size()) return -1;
+        const orc::Level& L = o->lev[l];
+        const int i = lijk[4 * m + 1] - L.org[0], j = lijk[4 * m + 2] - L.org[1], k = lijk[4 * m + 3] - L.org[2];
+        if (i < 0 || i >= L.nx || j < 0 || j >= L.ny || k < 0 || k >= L.nz) return -1;
+        const double* f = &L.f[l == 0 ? o->alt : o->altf][L.idx(i, j, k) * orc::Q];
+        double rho = 0;
+        for (int q = 0; q < orc::Q; ++q) rho += f[q];
+        out[m] = rho * o->k.cs2;
+    }
+    return 0;
+}
+
 void orc_destroy(void* h) { delete static_cast<Oracle*>(h); }
 
 }  // extern "C"

