@@ -19,6 +19,8 @@
 #include <cuda_runtime.h>
 #include <cuda_fp16.h>
 
+#include <utility>
+
 namespace acp {
 
 constexpr int Q = 19;
@@ -201,6 +203,67 @@ __host__ __device__ constexpr int gsRow(int m, int q) {
         default: return z * (x * x - y * y);
     }
 }
+// Inverse of the Gram-Schmidt basis, evaluated by the compiler (Gauss-Jordan
+// with partial pivoting on the integer rows above); GsInv<q, m>::v is a
+// compile-time constant, so the back transforms skip its zero entries
+// (154 of 361) and fold the others into the instructions.
+struct Mat19 {
+    double a[19][19];
+};
+constexpr double cabs(double x) { return x < 0 ? -x : x; }
+constexpr Mat19 gsInverse() {
+    double m[19][38] = {};
+    for (int r = 0; r < 19; ++r)
+        for (int c = 0; c < 19; ++c) {
+            m[r][c] = gsRow(r, c);
+            m[r][19 + c] = r == c ? 1.0 : 0.0;
+        }
+    for (int c = 0; c < 19; ++c) {
+        int p = c;
+        for (int r = c + 1; r < 19; ++r)
+            if (cabs(m[r][c]) > cabs(m[p][c])) p = r;
+        for (int k = 0; k < 38; ++k) {
+            const double t = m[p][k];
+            m[p][k] = m[c][k];
+            m[c][k] = t;
+        }
+        const double piv = m[c][c];
+        for (int k = 0; k < 38; ++k) m[c][k] /= piv;
+        for (int r = 0; r < 19; ++r) {
+            if (r == c) continue;
+            const double f = m[r][c];
+            if (f == 0) continue;
+            for (int k = 0; k < 38; ++k) m[r][k] -= f * m[c][k];
+        }
+    }
+    Mat19 out = {};
+    for (int r = 0; r < 19; ++r)
+        for (int c = 0; c < 19; ++c) out.a[r][c] = m[r][19 + c];
+    return out;
+}
+constexpr Mat19 kGsInverse = gsInverse();
+template <int q, int m>
+struct GsInv {
+    static constexpr double v = kGsInverse.a[q][m];
+};
+__host__ __device__ constexpr bool gsConserved(int m) { return m == 0 || m == 3 || m == 5 || m == 7; }
+
+// sum_m Minv[q][m] * x[m] over the moments (the conserved ones skipped when
+// `skipConserved`), zero coefficients dropped at compile time
+template <typename R, int q, bool skipConserved, int... m>
+__device__ __forceinline__ R gsBackRow(const R* x, std::integer_sequence<int, m...>) {
+    R acc = 0;
+    ((GsInv<q, m>::v != 0.0 && !(skipConserved && gsConserved(m)) ? (void)(acc += R(GsInv<q, m>::v) * x[m])
+                                                                     : (void)0),
+     ...);
+    return acc;
+}
+// f(q, back-transformed value) for every direction q
+template <typename R, bool skipConserved, typename F, int... q>
+__device__ __forceinline__ void gsBackAll(const R* x, F&& f, std::integer_sequence<int, q...>) {
+    (f(q, gsBackRow<R, q, skipConserved>(x, std::make_integer_sequence<int, 19>{})), ...);
+}
+
 // raw-moment basis rows 5..9: the deviatoric second-order moments relaxed with
 // omega (Node.cpp:2720-2733, 2580-2584)
 __host__ __device__ constexpr int rmRow2(int m, int q) {

@@ -151,14 +151,25 @@ int validate(const acp_case_desc* d, std::string& why) {
     }
     if (d->max_level != 0 && d->max_level != 1) { why = "MaxLevel must be 0 or 1"; return ACP_ERR_INVALID; }
     if (d->max_level == 1) {
-        if (d->layout != ACP_LAYOUT_BOX) {
-            why = "two-level cases use the box layout (Refinement-Layout BOX)";
-            return ACP_ERR_UNSUPPORTED;
-        }
+        if (d->layout != ACP_LAYOUT_BOX && d->layout != ACP_LAYOUT_SHELL) { why = "unknown refinement layout"; return ACP_ERR_INVALID; }
         if (d->coupling < ACP_COUPLING_STD || d->coupling > ACP_COUPLING_DC2) { why = "unknown coupling approach"; return ACP_ERR_INVALID; }
         if ((d->coupling == ACP_COUPLING_STD) != (d->overlap == 1)) {
             why = "Coupling-Approach STD needs Overlap 1, DC1 and DC2 need Overlap 0";
             return ACP_ERR_INVALID;
+        }
+        if (d->layout == ACP_LAYOUT_SHELL) {
+            // the reference's layout: a coarse core inside a fine shell reaching every face
+            const int ov = d->coupling == ACP_COUPLING_STD ? 1 : 0;
+            const int refLo[3] = {d->ref_layer_x, d->ref_layer_yz, d->ref_layer_yz};
+            for (int a = 0; a < 3; ++a) {
+                if (d->bc[a] != ACP_BC_LODI) { why = "the shell layout has LODI boundaries on every face"; return ACP_ERR_UNSUPPORTED; }
+                if (refLo[a] < 2 || d->ref_layer_yz < 2) { why = "refinement layers of at least 2 coarse cells"; return ACP_ERR_INVALID; }
+                const int lo = refLo[a] - ov, hi = dims[a] - 1 - d->ref_layer_yz + ov;
+                if (hi - lo < 4) { why = "the coarse core needs at least 4 coarse cells per axis"; return ACP_ERR_INVALID; }
+            }
+            const long long fine = (2LL * d->nx - 1) * (2LL * d->ny - 1) * (2LL * d->nz - 1);
+            if (fine > 100000000LL) { why = "more than 1e8 nodes in the fine level"; return ACP_ERR_UNSUPPORTED; }
+            return ACP_OK;
         }
         bool spans[3];
         for (int a = 0; a < 3; ++a) {
@@ -267,80 +278,137 @@ uint32_t replaceMask(int mode, const int* f) {
     return m;
 }
 
-// two levels, box layout: the coarse level covers the domain with the box
-// interior (beyond the one-cell overlap) dead, the fine level covers the box
+// Coupling geometry of a level: its coupling nodes lie on the faces of the
+// box [cl, ch] (local node indices) that are interfaces.  The level is live
+// inside the box (`inside`: the fine level of the box layout, the coarse core
+// of the shell layout) or outside it and on its faces (the coarse level of the
+// box layout, the fine level of the shell layout), the nodes strictly inside
+// being covered by the other level.
+struct CouplingGeom {
+    int cl[3], ch[3];
+    int loIf[3], hiIf[3];
+    bool inside;
+    // outward normal of the level's live region at a coupling node
+    void normal(const int* c, int* f) const {
+        const int sg = inside ? 1 : -1;
+        for (int a = 0; a < 3; ++a) f[a] = (loIf[a] && c[a] == cl[a]) ? -sg : ((hiIf[a] && c[a] == ch[a]) ? sg : 0);
+    }
+    bool dead(const int* c) const {
+        if (inside) return false;
+        for (int a = 0; a < 3; ++a) {
+            const int lo = loIf[a] ? cl[a] + 1 : cl[a], hi = hiIf[a] ? ch[a] - 1 : ch[a];
+            if (c[a] < lo || c[a] > hi) return false;
+        }
+        return true;
+    }
+    bool coupling(const int* c) const {
+        bool within = true, face = false;
+        for (int a = 0; a < 3; ++a) {
+            if (c[a] < cl[a] || c[a] > ch[a]) within = false;
+            if ((loIf[a] && c[a] == cl[a]) || (hiIf[a] && c[a] == ch[a])) face = true;
+        }
+        return within && face && !dead(c);
+    }
+};
+
+// node classes of a level from its coupling geometry: dead nodes, coupling
+// nodes (pushing everywhere when the level lies outside its box, where the
+// covered nodes exist in the array, else only within the level)
+void markLevel(LevelHost& L, const CouplingGeom& g) {
+    L.code.assign(L.N, CODE_FLUID);
+    for (int k = 0; k < L.nz; ++k)
+        for (int j = 0; j < L.ny; ++j)
+            for (int i = 0; i < L.nx; ++i) {
+                const int c[3] = {i, j, k};
+                const long long n = ((long long)k * L.ny + j) * L.nx + i;
+                if (g.dead(c)) {
+                    L.code[n] = CODE_DEAD;
+                } else if (g.coupling(c)) {
+                    int f[3];
+                    g.normal(c, f);
+                    L.code[n] = (uint8_t)(CODE_IFACE0 + (g.inside ? faceCode(f[0], f[1], f[2]) : CODE_FLUID));
+                }
+            }
+}
+
+// Two levels.  Box layout: the fine level covers the box [box_lo, box_hi]
+// (coarse node indices), the coarse level the domain with the box interior
+// covered.  Shell layout (the reference's, Lattice.cpp:17-234): the coarse
+// level is the core [RefinementLayerX - Overlap, nx-1 - RefinementLayerYZ +
+// Overlap] x [RefinementLayerYZ - Overlap, n-1 - RefinementLayerYZ + Overlap]^2,
+// the fine level the domain with the core covered.  STD couples with an
+// overlap of one coarse cell, DC1/DC2 on shared nodes (Overlap 0).
 int buildTwoLevel(acp_handle* h) {
     const acp_case_desc& d = h->d;
     const int dom[3] = {d.nx, d.ny, d.nz};
     const bool direct = d.coupling != ACP_COUPLING_STD;
     const int ov = direct ? 0 : 1;
-    int lo[3], hi[3], loIf[3], hiIf[3], spans[3];
-    for (int a = 0; a < 3; ++a) {
-        lo[a] = d.box_lo[a];
-        hi[a] = d.box_hi[a];
-        spans[a] = lo[a] == 0 && hi[a] == dom[a] - 1;
-        const bool lodi = d.bc[a] == ACP_BC_LODI;
-        loIf[a] = !spans[a] && !(lo[a] == 0 && lodi);
-        hiIf[a] = !spans[a] && !(hi[a] == dom[a] - 1 && lodi);
+    const bool shell = d.layout == ACP_LAYOUT_SHELL;
+    LevelHost C, F;
+    CouplingGeom gc, gf;
+    int fd[3];
+    if (!shell) {
+        for (int a = 0; a < 3; ++a) {
+            const int lo = d.box_lo[a], hi = d.box_hi[a];
+            const bool spans = lo == 0 && hi == dom[a] - 1;
+            const bool lodi = d.bc[a] == ACP_BC_LODI;
+            gc.loIf[a] = gf.loIf[a] = !spans && !(lo == 0 && lodi);
+            gc.hiIf[a] = gf.hiIf[a] = !spans && !(hi == dom[a] - 1 && lodi);
+            C.per[a] = d.bc[a] == ACP_BC_PERIODIC;
+            gc.cl[a] = gc.loIf[a] ? lo + ov : lo;
+            gc.ch[a] = gc.hiIf[a] ? hi - ov : hi;
+            F.per[a] = spans && d.bc[a] == ACP_BC_PERIODIC;
+            fd[a] = F.per[a] ? 2 * dom[a] : 2 * (hi - lo) + 1;
+            F.off[a] = 2 * lo;
+            gf.cl[a] = 0;
+            gf.ch[a] = fd[a] - 1;
+        }
+        C.nx = d.nx; C.ny = d.ny; C.nz = d.nz;
+        gc.inside = false;
+        gf.inside = true;
+    } else {
+        const int refLo[3] = {d.ref_layer_x, d.ref_layer_yz, d.ref_layer_yz};
+        int cd[3];
+        for (int a = 0; a < 3; ++a) {
+            const int lo = refLo[a] - ov, hi = dom[a] - 1 - d.ref_layer_yz + ov;
+            gc.loIf[a] = gf.loIf[a] = gc.hiIf[a] = gf.hiIf[a] = 1;
+            cd[a] = hi - lo + 1;
+            C.off[a] = lo;
+            gc.cl[a] = 0;
+            gc.ch[a] = cd[a] - 1;
+            fd[a] = 2 * (dom[a] - 1) + 1;
+            gf.cl[a] = 2 * (lo + ov);
+            gf.ch[a] = 2 * (hi - ov);
+        }
+        C.nx = cd[0]; C.ny = cd[1]; C.nz = cd[2];
+        gc.inside = true;
+        gf.inside = false;
     }
-    // coarse
-    LevelHost C;
-    C.nx = d.nx; C.ny = d.ny; C.nz = d.nz;
     C.N = (long long)C.nx * C.ny * C.nz;
-    for (int a = 0; a < 3; ++a) C.per[a] = d.bc[a] == ACP_BC_PERIODIC;
-    C.code.assign(C.N, CODE_FLUID);
-    for (int k = 0; k < C.nz; ++k)
-        for (int j = 0; j < C.ny; ++j)
-            for (int i = 0; i < C.nx; ++i) {
-                const int c[3] = {i, j, k};
-                bool dead = true, inner = true;
-                for (int a = 0; a < 3; ++a) {
-                    // coupling nodes one cell inside the box (STD, Overlap 1) or on its faces (DC, Overlap 0)
-                    const int dlo = loIf[a] ? lo[a] + 1 + ov : lo[a], dhi = hiIf[a] ? hi[a] - 1 - ov : hi[a];
-                    const int ilo = loIf[a] ? lo[a] + ov : lo[a], ihi = hiIf[a] ? hi[a] - ov : hi[a];
-                    if (c[a] < dlo || c[a] > dhi) dead = false;
-                    if (c[a] < ilo || c[a] > ihi) inner = false;
-                }
-                const long long n = ((long long)k * C.ny + j) * C.nx + i;
-                if (dead) C.code[n] = CODE_DEAD;
-                else if (inner) C.code[n] = CODE_IFACE0 + CODE_FLUID;  // pushes everywhere (into dead nodes too)
-            }
+    markLevel(C, gc);
     int s = wireLevel(h, C, 0);
     if (s) return s;
-    // fine
-    LevelHost F;
-    int fd[3];
-    for (int a = 0; a < 3; ++a) {
-        F.per[a] = spans[a] && d.bc[a] == ACP_BC_PERIODIC;
-        fd[a] = F.per[a] ? 2 * dom[a] : 2 * (hi[a] - lo[a]) + 1;
-        F.off[a] = 2 * lo[a];
-    }
     F.nx = fd[0]; F.ny = fd[1]; F.nz = fd[2];
     F.N = (long long)F.nx * F.ny * F.nz;
-    F.code.assign(F.N, CODE_FLUID);
-    auto fidx = [&](int i, int j, int k) { return ((long long)k * F.ny + j) * F.nx + i; };
-    for (int k = 0; k < F.nz; ++k)
-        for (int j = 0; j < F.ny; ++j)
-            for (int i = 0; i < F.nx; ++i) {
-                const int c[3] = {i, j, k};
-                int f[3];
-                bool iface = false;
-                for (int a = 0; a < 3; ++a) {
-                    f[a] = (loIf[a] && c[a] == 0) ? -1 : ((hiIf[a] && c[a] == fd[a] - 1) ? 1 : 0);
-                    iface = iface || f[a] != 0;
-                }
-                if (iface) F.code[fidx(i, j, k)] = (uint8_t)(CODE_IFACE0 + faceCode(f[0], f[1], f[2]));
-            }
+    markLevel(F, gf);
     if ((s = wireLevel(h, F, 1))) return s;
-    // coupling lists
-    auto fineLocal = [&](const int* g, int& out) {
+    auto fidx = [&](int i, int j, int k) { return ((long long)k * F.ny + j) * F.nx + i; };
+    // coupling lists; nodes addressed by their level-global indices
+    auto local = [](const LevelHost& L, const int* g, long long& out) {
         int c[3];
+        const int dd[3] = {L.nx, L.ny, L.nz};
         for (int a = 0; a < 3; ++a) {
-            c[a] = g[a] - F.off[a];
-            if (F.per[a]) c[a] = (c[a] % fd[a] + fd[a]) % fd[a];
-            if (c[a] < 0 || c[a] >= fd[a]) return false;
+            c[a] = g[a] - L.off[a];
+            if (L.per[a]) c[a] = (c[a] % dd[a] + dd[a]) % dd[a];
+            if (c[a] < 0 || c[a] >= dd[a]) return false;
         }
-        out = (int)fidx(c[0], c[1], c[2]);
+        out = ((long long)c[2] * L.ny + c[1]) * L.nx + c[0];
+        return true;
+    };
+    auto fineLocal = [&](const int* g, int& out) {
+        long long n;
+        if (!local(F, g, n)) return false;
+        out = (int)n;
         return true;
     };
     std::vector<C2FDev> coinc, mid, cen;
@@ -351,9 +419,9 @@ int buildTwoLevel(acp_handle* h) {
                 if (F.code[n] < CODE_IFACE0 || F.code[n] == CODE_DEAD) continue;
                 const int c[3] = {i, j, k};
                 int g[3], f[3], odd[3], nodd = 0;
+                gf.normal(c, f);
                 for (int a = 0; a < 3; ++a) {
                     g[a] = c[a] + F.off[a];
-                    f[a] = (loIf[a] && c[a] == 0) ? -1 : ((hiIf[a] && c[a] == fd[a] - 1) ? 1 : 0);
                     odd[a] = g[a] & 1;
                     nodd += odd[a];
                 }
@@ -364,9 +432,12 @@ int buildTwoLevel(acp_handle* h) {
                 cn.mask = replaceMask(direct && d.c2f_replace == ACP_C2F_FALL ? ACP_C2F_MFP : d.c2f_replace, f);
                 for (int m = 0; m < 4; ++m) { cn.st[m] = -1; cn.w[m] = 0.f; }
                 if (nodd == 0) {
-                    int cc[3];
-                    for (int a = 0; a < 3; ++a) cc[a] = ((g[a] / 2) % dom[a] + dom[a]) % dom[a];
-                    cn.src = (int)(((long long)cc[2] * C.ny + cc[1]) * C.nx + cc[0]);
+                    int gc2[3];
+                    for (int a = 0; a < 3; ++a) gc2[a] = g[a] / 2;
+                    long long src;
+                    if (!local(C, gc2, src) || C.code[src] == CODE_DEAD)
+                        return fail(h, ACP_ERR_INVALID, "coarse source of a fine coupling node missing");
+                    cn.src = (int)src;
                     coinc.push_back(cn);
                     continue;
                 }
@@ -434,11 +505,11 @@ int buildTwoLevel(acp_handle* h) {
             const uint32_t both = dn.vc & dn.vf;
             dn.rc = (~dn.vc & all) | (d.f2c_replace != ACP_F2C_MC ? both : 0u);
             dn.rf = (~dn.vf & all) | (d.c2f_replace != ACP_C2F_MF ? both : 0u);
-            int fa = 0;
+            int fa = 0, fn[3];
+            gf.normal(cf, fn);
             for (int a = 0; a < 3; ++a)
-                if ((loIf[a] && cf[a] == 0) || (hiIf[a] && cf[a] == fd[a] - 1)) { fa = a; break; }
+                if (fn[a]) { fa = a; break; }
             const int b1 = fa == 0 ? 1 : 0, b2 = fa == 2 ? 1 : 2;
-            double wsum = 0;
             for (int m = 0; m < 9; ++m) {
                 const int d1 = m % 3 - 1, d2 = m / 3 - 1;
                 int c2[3] = {cf[0], cf[1], cf[2]};
@@ -454,9 +525,13 @@ int buildTwoLevel(acp_handle* h) {
                 }
                 dn.plane[m] = ok && w > 0 ? (int)t : -1;
                 dn.w[m] = dn.plane[m] >= 0 ? w : 0.;
-                wsum += dn.w[m];
+                dn.pv[m] = 0;
+                if (dn.plane[m] >= 0)
+                    for (int q = 0; q < Q; ++q) {
+                        const int sf[3] = {c2[0] - ex(q), c2[1] - ey(q), c2[2] - ez(q)};
+                        if (liveIn(F, sf) >= 0) dn.pv[m] |= 1u << q;
+                    }
             }
-            for (int m = 0; m < 9; ++m) dn.w[m] /= wsum;
             h->dcHost.push_back(dn);
         }
     }
@@ -464,13 +539,11 @@ int buildTwoLevel(acp_handle* h) {
         for (int j = 0; j < C.ny; ++j)
             for (int i = 0; i < C.nx; ++i) {
                 const long long n = ((long long)k * C.ny + j) * C.nx + i;
-                if (C.code[n] != CODE_IFACE0 + CODE_FLUID) continue;
+                if (C.code[n] < CODE_IFACE0 || C.code[n] == CODE_DEAD) continue;
                 const int c[3] = {i, j, k};
                 int g[3], f[3];
-                for (int a = 0; a < 3; ++a) {
-                    g[a] = 2 * c[a];
-                    f[a] = (loIf[a] && c[a] == lo[a] + 1) ? 1 : ((hiIf[a] && c[a] == hi[a] - 1) ? -1 : 0);
-                }
+                gc.normal(c, f);
+                for (int a = 0; a < 3; ++a) g[a] = 2 * (c[a] + C.off[a]);
                 F2CDev fn;
                 fn.n = (int)n;
                 fn.mask = replaceMask(d.f2c_replace, f);
@@ -813,6 +886,14 @@ size_t estimateBytes(const acp_case_desc& d) {
     const size_t per = 2 * Q * storageBytes(d.storage) + 1;  // two population arrays and the node class
     long long nodes = (long long)d.nx * d.ny * d.nz;
     long long surf = 2LL * ((long long)d.nx * d.ny + (long long)d.ny * d.nz + (long long)d.nx * d.nz);
+    if (d.max_level == 1 && d.layout == ACP_LAYOUT_SHELL) {
+        // coarse core (at most the domain) and the fine level over the whole domain
+        const long long fine = (2LL * d.nx - 1) * (2LL * d.ny - 1) * (2LL * d.nz - 1);
+        const long long fsurf = 2 * ((2LL * d.nx) * (2LL * d.ny) + (2LL * d.ny) * (2LL * d.nz) + (2LL * d.nx) * (2LL * d.nz));
+        const size_t rb = d.storage == ACP_STORE_F64 ? 8 : 4;
+        return (size_t)(nodes + fine) * per + (size_t)fsurf * sizeof(BNodeDev) +
+               (size_t)surf * (sizeof(C2FDev) + sizeof(F2CDev) / 4 + sizeof(DCDev) / 4 + Q * rb);
+    }
     if (d.max_level == 1) {
         const int dom[3] = {d.nx, d.ny, d.nz};
         long long f[3];
@@ -1043,6 +1124,12 @@ int acp_sync(acp_handle* h) {
 int acp_level_dims(acp_handle* h, int level, int dims[3]) {
     if (!h || level < 0 || level >= (int)h->host.size()) return ACP_ERR_INVALID;
     dims[0] = h->host[level].nx; dims[1] = h->host[level].ny; dims[2] = h->host[level].nz;
+    return ACP_OK;
+}
+
+int acp_level_origin(acp_handle* h, int level, int origin[3]) {
+    if (!h || !origin || level < 0 || level >= (int)h->host.size()) return ACP_ERR_INVALID;
+    for (int a = 0; a < 3; ++a) origin[a] = h->host[level].off[a];
     return ACP_OK;
 }
 

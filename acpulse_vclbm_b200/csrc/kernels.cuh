@@ -269,16 +269,7 @@ struct Collider {
                 const bool visc = mm == 1 || mm == 9 || mm == 11 || mm == 13 || mm == 14 || mm == 15;
                 dm[mm] = conserved ? R(0) : (visc ? omega : R(1)) * (meq - m);
             }
-#pragma unroll
-            for (int q = 0; q < Q; ++q) {
-                R acc = g[q];
-#pragma unroll
-                for (int mm = 0; mm < Q; ++mm) {
-                    const bool conserved = mm == 0 || mm == 3 || mm == 5 || mm == 7;
-                    if (!conserved) acc += RT<R>::gsMinv(q, mm) * dm[mm];
-                }
-                emit(q, acc);
-            }
+            gsBackAll<R, true>(dm, [&](int q, R back) { emit(q, g[q] + back); }, std::make_integer_sequence<int, Q>{});
             return;
         }
 
@@ -979,13 +970,7 @@ __device__ __forceinline__ void rescaleNeq(R* neq, const CouplingArgs& c, bool t
         const R f = visc ? R(toFine ? c.alphaC2F : c.alphaF2C) : R(toFine ? 0.5 : 2.0);
         m[mm] = f * s;
     }
-#pragma unroll
-    for (int q = 0; q < Q; ++q) {
-        R acc = 0;
-#pragma unroll
-        for (int mm = 0; mm < Q; ++mm) acc += RT<R>::gsMinv(q, mm) * m[mm];
-        neq[q] = acc;
-    }
+    gsBackAll<R, false>(m, [&](int q, R back) { neq[q] = back; }, std::make_integer_sequence<int, Q>{});
 }
 
 // populations of the coincident coupling sources before the coarse step
@@ -1120,7 +1105,8 @@ struct DCDev {
     uint32_t vc, vf;            // populations whose source node is live on the coarse / fine level
     uint32_t rc, rf;            // populations replaced on the coarse / fine level
     int plane[9];               // 3x3 fine stencil in the interface plane (-1: none)
-    double w[9];                // F2C filter weights over the stencil (normalised)
+    uint32_t pv[9];             // populations valid at each stencil node (source node live)
+    double w[9];                // F2C filter weights over the stencil
 };
 
 // 4.5 w_q H2_q : Pi, Pi = sum_q H2_q neq_q (lattice units)
@@ -1170,16 +1156,19 @@ __device__ __forceinline__ void dcCoupleBody(S* Bc, S* Ff, const DCDev* __restri
     // t+1: the fine populations filtered over the interface plane, gathered
     // before this thread overwrites the shared node's fine populations (the
     // stencil's other nodes are hanging fine nodes, which this kernel does
-    // not write)
+    // not write), and the weights of each population are renormalised over the
+    // stencil nodes where it is valid (no slot that a level leaves unwritten is read)
     R ff[Q];
     if (full) {
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
-            R acc = 0;
+            R acc = 0, ws = 0;
             for (int m = 0; m < 9; ++m)
-                if (nd.plane[m] >= 0)
+                if (nd.plane[m] >= 0 && (nd.pv[m] >> q & 1u)) {
                     acc += R(nd.w[m]) * R(Store<S>::load(Ff + (long long)q * c.Nf + nd.plane[m], la.hscale[q]));
-            ff[q] = acc;
+                    ws += R(nd.w[m]);
+                }
+            ff[q] = ws > R(0) ? acc / ws : R(0);
         }
     }
     // fine side

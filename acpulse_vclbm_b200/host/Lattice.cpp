@@ -21,8 +21,7 @@ Lattice::Lattice(Control& bc) : bc_(bc) {
     const acp_case_desc& d = bc.caseDescription();
     for (int l = 0; l <= d.max_level; ++l) {
         check(acp_level_dims(h_, l, dims_[l]), "Lattice");
-        if (l == 1)
-            for (int a = 0; a < 3; ++a) origin_[1][a] = 2 * d.box_lo[a];
+        check(acp_level_origin(h_, l, origin_[l]), "Lattice");
     }
 }
 

@@ -67,7 +67,10 @@ enum acp_f2c_replace { ACP_F2C_MC = 0, ACP_F2C_MCP = 1, ACP_F2C_CALL = 2 };
 
 /* refinement layout */
 enum acp_layout {
-    ACP_LAYOUT_SHELL = 0, /* the reference's: fine shell around a coarse core (Lattice.cpp:17-234) */
+    ACP_LAYOUT_SHELL = 0, /* the reference's: fine shell around a coarse core (Lattice.cpp:17-234); the
+                           * core spans [RefinementLayerX - Overlap, nx-1 - RefinementLayerYZ + Overlap]
+                           * in x and [RefinementLayerYZ - Overlap, n-1 - RefinementLayerYZ + Overlap]
+                           * in y and z; LODI on every face */
     ACP_LAYOUT_BOX = 1    /* fine box [box_lo, box_hi] (coarse node indices) inside the coarse grid */
 };
 
@@ -144,6 +147,10 @@ int acp_step(acp_handle* h, int n_coarse_steps);
 int acp_sync(acp_handle* h);
 /* Node counts of a level's dense box (nodes = dims[0]*dims[1]*dims[2]). */
 int acp_level_dims(acp_handle* h, int level, int dims[3]);
+/* Level-global node index of a level's local node (0, 0, 0): the fine box's
+ * corner (box layout) or the coarse core's corner (shell layout); level-global
+ * indices of the fine level are twice the coarse ones. */
+int acp_level_origin(acp_handle* h, int level, int origin[3]);
 /* Nodes updated per coarse step, for MLUPS: coarse active + 2 * fine active. */
 int acp_active_updates(acp_handle* h, long long* coarse_nodes, long long* fine_nodes);
 /* Populations of a level as FP64 f_i (see header comment), host buffer of

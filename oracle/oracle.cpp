@@ -201,7 +201,8 @@ struct Oracle {
         unsigned vc, vf;        // populations whose source node is live on the coarse / fine level
         unsigned rc, rf;        // populations replaced on the coarse / fine level
         long plane[9];          // 3x3 fine stencil in the interface plane (-1: none), [4] = nf
-        double w[9];            // F2C filter weights over the stencil (normalised)
+        unsigned pv[9];         // populations valid at each stencil node
+        double w[9];            // F2C filter weights over the stencil
     };
     std::vector<DCNode> dc;     // one per coincident C2F node, same order
     bool isDC() const { return desc.coupling != ACP_COUPLING_STD; }
@@ -544,6 +545,44 @@ struct Oracle {
     // coarse nodes one cell inside the box take theirs from the fine level
     // (F2C), with the coarse step, two fine sub-steps and the couplings in the
     // order of Lattice::nestedTimeStepping* (Lattice.cpp:4354-5771).
+    // coupling geometry of a level: coupling nodes on the interface faces of
+    // the box [cl, ch] (local indices); the level lives inside the box, or
+    // outside it and on its faces (then the nodes strictly inside are dead)
+    struct Geom {
+        int cl[3], ch[3], loIf[3], hiIf[3];
+        bool inside;
+        void normal(const int* c, int* f) const {
+            const int sg = inside ? 1 : -1;
+            for (int a = 0; a < 3; ++a) f[a] = (loIf[a] && c[a] == cl[a]) ? -sg : ((hiIf[a] && c[a] == ch[a]) ? sg : 0);
+        }
+        bool dead(const int* c) const {
+            if (inside) return false;
+            for (int a = 0; a < 3; ++a) {
+                const int lo = loIf[a] ? cl[a] + 1 : cl[a], hi = hiIf[a] ? ch[a] - 1 : ch[a];
+                if (c[a] < lo || c[a] > hi) return false;
+            }
+            return true;
+        }
+        bool coupling(const int* c) const {
+            bool within = true, face = false;
+            for (int a = 0; a < 3; ++a) {
+                if (c[a] < cl[a] || c[a] > ch[a]) within = false;
+                if ((loIf[a] && c[a] == cl[a]) || (hiIf[a] && c[a] == ch[a])) face = true;
+            }
+            return within && face && !dead(c);
+        }
+    };
+    Geom geom[2];
+
+    void markLevel(Level& L, const Geom& g) {
+        for (int kk = 0; kk < L.nz; ++kk)
+            for (int j = 0; j < L.ny; ++j)
+                for (int i = 0; i < L.nx; ++i) {
+                    const int c[3] = {i, j, kk};
+                    L.type[L.idx(i, j, kk)] = g.dead(c) ? NT_DEAD : (g.coupling(c) ? NT_IFACE : NT_INTERIOR);
+                }
+    }
+
     bool buildTwoLevel() {
         const acp_case_desc& d = desc;
         k.setup(d.speed_of_sound, d.spacing, d.kinematic_viscosity, d.density, d.mach, d.k1, d.hybrid_sigma, d.eq_order,
@@ -551,73 +590,76 @@ struct Oracle {
         gsBasis(gsM);
         rmBasis(rmM);
         if (!invert19(gsM, gsMinv) || !invert19(rmM, rmMinv)) { err = "moment basis not invertible"; return false; }
-        if (d.layout != ACP_LAYOUT_BOX) { err = "two-level oracle: box layout only"; return false; }
         if ((d.coupling == ACP_COUPLING_STD) != (d.overlap == 1)) { err = "STD needs Overlap 1, DC1/DC2 Overlap 0"; return false; }
         const int dims[3] = {d.nx, d.ny, d.nz};
-        for (int a = 0; a < 3; ++a) {
-            boxLo[a] = d.box_lo[a];
-            boxHi[a] = d.box_hi[a];
-            spans[a] = boxLo[a] == 0 && boxHi[a] == dims[a] - 1;
-            const bool lodi = d.bc[a] == ACP_BC_LODI;
-            loIf[a] = !spans[a] && !(boxLo[a] == 0 && lodi);
-            hiIf[a] = !spans[a] && !(boxHi[a] == dims[a] - 1 && lodi);
-            if (d.bc[a] == ACP_BC_LODI && dims[a] < 4) { err = "LODI axes need at least 4 nodes"; return false; }
-            if (!(spans[a] && d.bc[a] == ACP_BC_PERIODIC) && boxHi[a] - boxLo[a] < 4) { err = "box too thin"; return false; }
-            if (boxLo[a] < 0 || boxHi[a] >= dims[a] || boxLo[a] > boxHi[a]) { err = "box outside the lattice"; return false; }
-        }
-        // a box reaching a LODI face spans the other two axes: no coupling node on a LODI face
-        for (int a = 0; a < 3; ++a)
-            if (d.bc[a] == ACP_BC_LODI && (boxLo[a] == 0 || boxHi[a] == dims[a] - 1))
-                for (int b = 0; b < 3; ++b)
-                    if (b != a && !spans[b]) { err = "a box touching a LODI face must span the other axes"; return false; }
+        const int ov = isDC() ? 0 : 1;
         lev.resize(2);
-        // ---- coarse level: the whole domain
-        {
-            Level& L = lev[0];
-            L.nx = d.nx; L.ny = d.ny; L.nz = d.nz;
-            for (int a = 0; a < 3; ++a) L.per[a] = d.bc[a] == ACP_BC_PERIODIC;
-            initLevelArrays(L, 0);
-            for (int kk = 0; kk < L.nz; ++kk)
-                for (int j = 0; j < L.ny; ++j)
-                    for (int i = 0; i < L.nx; ++i) {
-                        const int c[3] = {i, j, kk};
-                        bool dead = true, inner = true;
-                        for (int a = 0; a < 3; ++a) {
-                            // STD: the coupling nodes lie one cell inside the box (Overlap 1);
-                            // DC: on the box faces (Overlap 0); the nodes inside them are dead
-                            const int ov = isDC() ? 0 : 1;
-                            const int dlo = loIf[a] ? boxLo[a] + 1 + ov : boxLo[a], dhi = hiIf[a] ? boxHi[a] - 1 - ov : boxHi[a];
-                            const int ilo = loIf[a] ? boxLo[a] + ov : boxLo[a], ihi = hiIf[a] ? boxHi[a] - ov : boxHi[a];
-                            if (c[a] < dlo || c[a] > dhi) dead = false;
-                            if (c[a] < ilo || c[a] > ihi) inner = false;
-                        }
-                        const long n = L.idx(i, j, kk);
-                        L.type[n] = dead ? NT_DEAD : (inner ? NT_IFACE : NT_INTERIOR);
-                    }
-            if (!wireLevel(L)) return false;
-        }
-        // ---- fine level: the box at twice the resolution
-        {
-            Level& L = lev[1];
-            int fd[3];
+        Level& C = lev[0];
+        Level& F = lev[1];
+        Geom& gc = geom[0];
+        Geom& gf = geom[1];
+        int cd[3], fd[3];
+        if (d.layout == ACP_LAYOUT_BOX) {
             for (int a = 0; a < 3; ++a) {
-                L.per[a] = spans[a] && d.bc[a] == ACP_BC_PERIODIC;
-                fd[a] = L.per[a] ? 2 * dims[a] : 2 * (boxHi[a] - boxLo[a]) + 1;
-                L.org[a] = 2 * boxLo[a];
+                boxLo[a] = d.box_lo[a];
+                boxHi[a] = d.box_hi[a];
+                spans[a] = boxLo[a] == 0 && boxHi[a] == dims[a] - 1;
+                const bool lodi = d.bc[a] == ACP_BC_LODI;
+                loIf[a] = !spans[a] && !(boxLo[a] == 0 && lodi);
+                hiIf[a] = !spans[a] && !(boxHi[a] == dims[a] - 1 && lodi);
+                if (d.bc[a] == ACP_BC_LODI && dims[a] < 4) { err = "LODI axes need at least 4 nodes"; return false; }
+                if (!(spans[a] && d.bc[a] == ACP_BC_PERIODIC) && boxHi[a] - boxLo[a] < 4) { err = "box too thin"; return false; }
+                if (boxLo[a] < 0 || boxHi[a] >= dims[a] || boxLo[a] > boxHi[a]) { err = "box outside the lattice"; return false; }
             }
-            L.nx = fd[0]; L.ny = fd[1]; L.nz = fd[2];
-            initLevelArrays(L, 1);
-            for (int kk = 0; kk < L.nz; ++kk)
-                for (int j = 0; j < L.ny; ++j)
-                    for (int i = 0; i < L.nx; ++i) {
-                        const int c[3] = {i, j, kk};
-                        bool iface = false;
-                        for (int a = 0; a < 3; ++a)
-                            if ((loIf[a] && c[a] == 0) || (hiIf[a] && c[a] == fd[a] - 1)) iface = true;
-                        L.type[L.idx(i, j, kk)] = iface ? NT_IFACE : NT_INTERIOR;
-                    }
-            if (!wireLevel(L)) return false;
+            // a box reaching a LODI face spans the other two axes: no coupling node on a LODI face
+            for (int a = 0; a < 3; ++a)
+                if (d.bc[a] == ACP_BC_LODI && (boxLo[a] == 0 || boxHi[a] == dims[a] - 1))
+                    for (int b = 0; b < 3; ++b)
+                        if (b != a && !spans[b]) { err = "a box touching a LODI face must span the other axes"; return false; }
+            for (int a = 0; a < 3; ++a) {
+                gc.loIf[a] = gf.loIf[a] = loIf[a];
+                gc.hiIf[a] = gf.hiIf[a] = hiIf[a];
+                C.per[a] = d.bc[a] == ACP_BC_PERIODIC;
+                cd[a] = dims[a];
+                gc.cl[a] = loIf[a] ? boxLo[a] + ov : boxLo[a];
+                gc.ch[a] = hiIf[a] ? boxHi[a] - ov : boxHi[a];
+                F.per[a] = spans[a] && d.bc[a] == ACP_BC_PERIODIC;
+                fd[a] = F.per[a] ? 2 * dims[a] : 2 * (boxHi[a] - boxLo[a]) + 1;
+                F.org[a] = 2 * boxLo[a];
+                gf.cl[a] = 0;
+                gf.ch[a] = fd[a] - 1;
+            }
+            gc.inside = false;
+            gf.inside = true;
+        } else {
+            // the reference's shell layout (Lattice.cpp:17-234): a coarse core
+            // inside a fine shell that reaches every (LODI) face
+            const int refLo[3] = {d.ref_layer_x, d.ref_layer_yz, d.ref_layer_yz};
+            for (int a = 0; a < 3; ++a) {
+                if (d.bc[a] != ACP_BC_LODI) { err = "the shell layout has LODI boundaries on every face"; return false; }
+                const int lo = refLo[a] - ov, hi = dims[a] - 1 - d.ref_layer_yz + ov;
+                if (refLo[a] < 2 || d.ref_layer_yz < 2 || hi - lo < 4) { err = "shell layout too thin"; return false; }
+                loIf[a] = hiIf[a] = 1;
+                gc.loIf[a] = gf.loIf[a] = gc.hiIf[a] = gf.hiIf[a] = 1;
+                cd[a] = hi - lo + 1;
+                C.org[a] = lo;
+                gc.cl[a] = 0;
+                gc.ch[a] = cd[a] - 1;
+                fd[a] = 2 * (dims[a] - 1) + 1;
+                gf.cl[a] = 2 * (lo + ov);
+                gf.ch[a] = 2 * (hi - ov);
+            }
+            gc.inside = true;
+            gf.inside = false;
         }
+        C.nx = cd[0]; C.ny = cd[1]; C.nz = cd[2];
+        initLevelArrays(C, 0);
+        markLevel(C, gc);
+        if (!wireLevel(C)) return false;
+        F.nx = fd[0]; F.ny = fd[1]; F.nz = fd[2];
+        initLevelArrays(F, 1);
+        markLevel(F, gf);
+        if (!wireLevel(F)) return false;
         buildCouplings();
         return true;
     }
@@ -644,8 +686,8 @@ struct Oracle {
             // the level's local index 0 / last lies on a domain face
             lodiLo[a] = lodi && L.org[a] == 0;
             const int domTop = (&desc.nx)[a] - 1;
-            const int scale = L.org[a] == 0 && &L == &lev[0] ? 1 : 2;
-            lodiHi[a] = lodi && (&L == &lev[0] ? true : (L.org[a] + dims[a] - 1 == scale * domTop));
+            const int scale = &L == &lev[0] ? 1 : 2;  // level-global index of the domain's last node
+            lodiHi[a] = lodi && L.org[a] + dims[a] - 1 == scale * domTop;
         }
         auto inRange = [&](int i, int j, int kk, long& out) {
             int c[3] = {i, j, kk};
@@ -724,17 +766,19 @@ struct Oracle {
     void buildCouplings() {
         Level& C = lev[0];
         Level& F = lev[1];
-        const int fd[3] = {F.nx, F.ny, F.nz};
-        auto fineIdx = [&](const int* g, long& out) {  // fine global -> local
+        // level-global -> local (periodic axes wrap)
+        auto local = [](const Level& L, const int* g, long& out) {
+            const int dd[3] = {L.nx, L.ny, L.nz};
             int c[3];
             for (int a = 0; a < 3; ++a) {
-                c[a] = g[a] - F.org[a];
-                if (F.per[a]) c[a] = (c[a] % fd[a] + fd[a]) % fd[a];
-                if (c[a] < 0 || c[a] >= fd[a]) return false;
+                c[a] = g[a] - L.org[a];
+                if (L.per[a]) c[a] = (c[a] % dd[a] + dd[a]) % dd[a];
+                if (c[a] < 0 || c[a] >= dd[a]) return false;
             }
-            out = F.idx(c[0], c[1], c[2]);
+            out = L.idx(c[0], c[1], c[2]);
             return true;
         };
+        auto fineIdx = [&](const int* g, long& out) { return local(F, g, out); };
         std::vector<C2FNode> coinc, mid, cen;
         for (int kk = 0; kk < F.nz; ++kk)
             for (int j = 0; j < F.ny; ++j)
@@ -743,9 +787,9 @@ struct Oracle {
                     if (F.type[n] != NT_IFACE) continue;
                     const int c[3] = {i, j, kk};
                     int g[3], face[3], odd[3], nodd = 0;
+                    geom[1].normal(c, face);
                     for (int a = 0; a < 3; ++a) {
                         g[a] = c[a] + F.org[a];
-                        face[a] = (loIf[a] && c[a] == 0) ? -1 : ((hiIf[a] && c[a] == fd[a] - 1) ? 1 : 0);
                         odd[a] = g[a] & 1;
                         nodd += odd[a];
                     }
@@ -758,11 +802,8 @@ struct Oracle {
                     if (nodd == 0) {
                         cn.kind = 0;
                         int cc[3];
-                        for (int a = 0; a < 3; ++a) {
-                            cc[a] = g[a] / 2;
-                            if (C.per[a]) cc[a] = (cc[a] % (&desc.nx)[a] + (&desc.nx)[a]) % (&desc.nx)[a];
-                        }
-                        cn.src = C.idx(cc[0], cc[1], cc[2]);
+                        for (int a = 0; a < 3; ++a) cc[a] = g[a] / 2;
+                        local(C, cc, cn.src);
                         coinc.push_back(cn);
                         continue;
                     }
@@ -803,11 +844,8 @@ struct Oracle {
                     fn.n = n;
                     const int c[3] = {i, j, kk};
                     int g[3], face[3];
-                    for (int a = 0; a < 3; ++a) {
-                        g[a] = 2 * c[a];
-                        // the coarse coupling node lies one cell inside the box face it faces
-                        face[a] = (loIf[a] && c[a] == boxLo[a] + 1) ? 1 : ((hiIf[a] && c[a] == boxHi[a] - 1) ? -1 : 0);
-                    }
+                    geom[0].normal(c, face);
+                    for (int a = 0; a < 3; ++a) g[a] = 2 * (c[a] + C.org[a]);
                     fineIdx(g, fn.partner);
                     int m = 0;
                     for (int dz = -1; dz <= 1; ++dz)
@@ -816,7 +854,7 @@ struct Oracle {
                                 int gg[3] = {g[0] + dx, g[1] + dy, g[2] + dz};
                                 fineIdx(gg, fn.cube[m++]);
                             }
-                    // populations arriving from the dead interior of the box are the missing ones
+                    // populations arriving from the covered side are the missing ones
                     fn.mask = replaceMask(desc.f2c_replace, face);
                     f2c.push_back(fn);
                 }
@@ -866,11 +904,11 @@ struct Oracle {
             dn.rc = (~dn.vc & all) | (desc.f2c_replace != ACP_F2C_MC ? both : 0u);
             dn.rf = (~dn.vf & all) | (desc.c2f_replace != ACP_C2F_MF ? both : 0u);
             // interface plane: spanned by the axes other than the first face axis
-            int fa = 0;
+            int fa = 0, fnrm[3];
+            geom[1].normal(cf, fnrm);
             for (int a = 0; a < 3; ++a)
-                if ((loIf[a] && cf[a] == 0) || (hiIf[a] && cf[a] == fd[a] - 1)) { fa = a; break; }
+                if (fnrm[a]) { fa = a; break; }
             const int b1 = fa == 0 ? 1 : 0, b2 = fa == 2 ? 1 : 2;
-            double wsum = 0;
             for (int m = 0; m < 9; ++m) {
                 const int d1 = m % 3 - 1, d2 = m / 3 - 1;
                 int c2[3] = {cf[0], cf[1], cf[2]};
@@ -886,9 +924,14 @@ struct Oracle {
                 }
                 dn.plane[m] = ok && w > 0 ? t : -1;
                 dn.w[m] = dn.plane[m] >= 0 ? w : 0.;
-                wsum += dn.w[m];
+                dn.pv[m] = 0;
+                if (dn.plane[m] >= 0)
+                    for (int q = 0; q < Q; ++q) {
+                        const int sf[3] = {c2[0] - EX[q], c2[1] - EY[q], c2[2] - EZ[q]};
+                        long tt;
+                        if (live(F, fd, sf, tt)) dn.pv[m] |= 1u << q;
+                    }
             }
-            for (int m = 0; m < 9; ++m) dn.w[m] /= wsum;
             dc.push_back(dn);
         }
     }
@@ -964,12 +1007,16 @@ struct Oracle {
             }
             // coarse side (t+1): filtered fine populations in the interface plane
             if (th == 1.) {
+                // each population filtered over the stencil nodes where it is valid
                 double ff[Q], neq[Q], sc[Q];
                 for (int q = 0; q < Q; ++q) {
-                    double acc = 0;
+                    double acc = 0, ws = 0;
                     for (int m = 0; m < 9; ++m)
-                        if (dn.plane[m] >= 0) acc += dn.w[m] * FB[dn.plane[m] * Q + q];
-                    ff[q] = acc;
+                        if (dn.plane[m] >= 0 && (dn.pv[m] >> q & 1u)) {
+                            acc += dn.w[m] * FB[dn.plane[m] * Q + q];
+                            ws += dn.w[m];
+                        }
+                    ff[q] = ws > 0 ? acc / ws : 0.;
                 }
                 // fine non-equilibrium; the fine-missing populations take the
                 // coarse one brought to the fine scale

@@ -204,3 +204,56 @@ def test_direct_coupling_fp32_within_1e5():
     pf = np.abs(L.populations(1).sum(0) - o.populations(1).sum(0)).max() * cs2 / amp
     L.close()
     assert pc < 1e-5 and pf < 1e-5, (pc, pf)
+
+
+# the reference's shell layout (Lattice.cpp:17-234): a coarse core inside a
+# fine shell reaching every (LODI) face
+def shell_case(op, coupling="STD", filt="LAG", storage="FP64"):
+    from acpulse_vclbm_b200.capi import LAYOUT_SHELL
+    d = lattice_units_case(40, 24, 20, op=op, nu_lu=1e-3, order=3, periodic=(False, False, False), eps=1e-3, b=3.0,
+                           center=(12.0, 12.0, 10.0), storage=storage, ic_dims=3)
+    d.max_level = 1
+    d.layout = LAYOUT_SHELL
+    d.ref_layer_x, d.ref_layer_yz = 8, 4
+    d.coupling = COUPLING[coupling]
+    d.overlap = 1 if coupling == "STD" else 0
+    d.f2c_filter = F2C_FILTER[filt]
+    d.mrt_writeback = 1
+    if coupling != "STD":
+        d.c2f_replace, d.f2c_replace = C2F_REPLACE["Mf"], F2C_REPLACE["Mc"]
+    return d
+
+
+def fine_live_mask(d, shape):
+    """the fine nodes outside the covered core (strictly inside the fine coupling box)"""
+    lo = [d.ref_layer_x, d.ref_layer_yz, d.ref_layer_yz]  # fine coupling box in coarse cells
+    hi = [n - 1 - d.ref_layer_yz for n in (d.nx, d.ny, d.nz)]
+    m = np.ones(shape, dtype=bool)
+    m[2 * lo[2] + 1:2 * hi[2], 2 * lo[1] + 1:2 * hi[1], 2 * lo[0] + 1:2 * hi[0]] = False
+    return m
+
+
+@pytest.mark.parametrize("op", ["SRT", "MRT-GS", "RR", "HRR"])
+@pytest.mark.parametrize("coupling", ["STD", "DC1", "DC2"])
+def test_shell_layout_matches_oracle(op, coupling):
+    d = shell_case(op, coupling, filt="TOU" if coupling == "DC2" else "LAG")
+    g, r = run_both(d, 40)
+    err_c = np.abs(g[0] - r[0]).max() / d.ic_eps
+    live = fine_live_mask(d, g[1].shape[1:])
+    err_f = np.abs(g[1][:, live] - r[1][:, live]).max() / d.ic_eps
+    assert err_c < 1e-9 and err_f < 1e-9, (err_c, err_f)
+
+
+def test_reference_default_case_two_levels():
+    """the reference's shipped case (BoundaryConditions.txt values: 151 x 151 x
+    21 nodes, HRR, MaxLevel 1, RefinementLayerYZ 4, RefinementLayerX 75,
+    Overlap 1, the reference pulse) through the shell layout, against the oracle"""
+    from acpulse_vclbm_b200.capi import default_case
+    d = default_case()
+    d.max_level = 1
+    g, r = run_both(d, 3)
+    amp = 0.01 * d.density
+    err_c = np.abs(g[0] - r[0]).max() / amp
+    live = fine_live_mask(d, g[1].shape[1:])
+    err_f = np.abs(g[1][:, live] - r[1][:, live]).max() / amp
+    assert err_c < 1e-9 and err_f < 1e-9, (err_c, err_f)
