@@ -124,12 +124,14 @@ template <typename S, typename R>
 __global__ void __launch_bounds__(128) kb_c2f_save(const BatchCase<S>* __restrict__ cases,
                                                    const WorkItem* __restrict__ items, int n, int flip) {
     __shared__ LevelArgs<S> sa;
+    __shared__ CouplingArgs sc;
     for (int w = blockIdx.x; w < n; w += gridDim.x) {
         const WorkItem it = items[w];
         const BatchCase<S>& bc = cases[it.c];
         stage(&sa, &bc.lv[0].a[bc.base ^ flip]);
+        stage(&sc, &bc.cpl);
         __syncthreads();
-        c2fSaveBody<S, R>(sa.A, bc.c2f, bc.nCoinc, (R*)bc.pre, sa, it.bx);
+        c2fSaveBody<S, R>(sa.A, bc.c2f, bc.nCoinc, (R*)bc.pre, sa, sc, it.bx);
         __syncthreads();
     }
 }
@@ -436,9 +438,16 @@ int buildGroup(acp_batch* b, Group& g) {
     }
     if (g.levels == 2) {
         phase(g.save, [&](int c, const acp_handle* h) { blockItems(c, h->nCoinc, 128, items); });
-        phase(g.coinc, [&](int c, const acp_handle* h) { blockItems(c, h->nCoinc, 128, items); });
-        phase(g.mid, [&](int c, const acp_handle* h) { blockItems(c, (long long)h->nMid * Q, 256, items); });
-        phase(g.cen, [&](int c, const acp_handle* h) { blockItems(c, (long long)h->nCen * Q, 256, items); });
+        phase(g.coinc, [&](int c, const acp_handle* h) {
+            blockItems(c, (long long)h->nCoinc * (h->dcHost.empty() ? coincidentThreadsPerNode(couplingArgs(h)) : 1), 128,
+                       items);
+        });
+        phase(g.mid, [&](int c, const acp_handle* h) {
+            blockItems(c, (long long)h->nMid * interpComponents(h), 256, items);
+        });
+        phase(g.cen, [&](int c, const acp_handle* h) {
+            blockItems(c, (long long)h->nCen * interpComponents(h), 256, items);
+        });
         phase(g.f2c, [&](int c, const acp_handle* h) { blockItems(c, (long long)h->f2cHost.size() * 32, 128, items); });
     }
     BCU(b, cudaMalloc(&g.dCases, std::max<size_t>(1, recs.size()) * sizeof(BatchCase<S>)));

@@ -557,6 +557,37 @@ int buildTwoLevel(acp_handle* h) {
                         }
                 h->f2cHost.push_back(fn);
             }
+    // partner strain of the coupling nodes (STD scheme, HRR or RR with cubic-Mach)
+    h->partner = !direct && (d.op == OP_HRR || (d.op == OP_RR && d.cubic_mach));
+    h->nbHost.clear();
+    if (h->partner) {
+        F.slot.assign(F.N, -1);
+        for (size_t i = 0; i < h->c2fHost.size(); ++i) F.slot[h->c2fHost[i].n] = (int)i;
+        F.nSlots = (int)h->c2fHost.size();
+        C.slot.assign(C.N, -1);
+        for (size_t i = 0; i < h->f2cHost.size(); ++i) C.slot[h->f2cHost[i].n] = (int)i;
+        C.nSlots = (int)h->f2cHost.size();
+        auto regular = [](const LevelHost& L, long long n) { return L.code[n] < CODE_IFACE0; };
+        for (int t = 0; t < h->nCoinc; ++t) {
+            const C2FDev& cn = h->c2fHost[t];
+            const int cc[3] = {(int)(cn.src % C.nx), (int)((cn.src / C.nx) % C.ny), (int)(cn.src / ((long long)C.nx * C.ny))};
+            C2FNbDev nb;
+            for (int q = 0; q < 6; ++q) {
+                const int g[3] = {cc[0] + C.off[0] + ex(q), cc[1] + C.off[1] + ey(q), cc[2] + C.off[2] + ez(q)};
+                long long m;
+                nb.c[q] = nb.f[q] = -1;
+                if (local(C, g, m) && regular(C, m)) {
+                    nb.c[q] = (int)m;
+                    continue;
+                }
+                const int gf[3] = {2 * g[0], 2 * g[1], 2 * g[2]};
+                if (!local(F, gf, m) || !regular(F, m))
+                    return fail(h, ACP_ERR_INVALID, "partner strain stencil missing at a coupling node");
+                nb.f[q] = (int)m;
+            }
+            h->nbHost.push_back(nb);
+        }
+    }
     h->host.push_back(std::move(C));
     h->host.push_back(std::move(F));
     return ACP_OK;
@@ -742,16 +773,18 @@ void enqueueC2F(acp_handle* h, int cnew, int fdst, R th) {
         else if (o == 3) k_dc_couple<S, R, 3><<<g, 128, 0, h->stream>>>(Bw, Ff, h->dDC, h->nCoinc, pre, th, dc2, c, la);
         else k_dc_couple<S, R, 4><<<g, 128, 0, h->stream>>>(Bw, Ff, h->dDC, h->nCoinc, pre, th, dc2, c, la);
     } else if (h->nCoinc) {
-        const unsigned g = (h->nCoinc + 127) / 128;
+        const unsigned g = (h->nCoinc * coincidentThreadsPerNode(c) + 127) / 128;
         if (o == 2) k_c2f_coincident<S, R, 2><<<g, 128, 0, h->stream>>>(Bc, Ff, h->dC2F, h->nCoinc, pre, th, c, la);
         else if (o == 3) k_c2f_coincident<S, R, 3><<<g, 128, 0, h->stream>>>(Bc, Ff, h->dC2F, h->nCoinc, pre, th, c, la);
         else k_c2f_coincident<S, R, 4><<<g, 128, 0, h->stream>>>(Bc, Ff, h->dC2F, h->nCoinc, pre, th, c, la);
     }
+    const int comps = interpComponents(h);
     if (h->nMid)
-        k_c2f_interp<S, R><<<(h->nMid * Q + 255) / 256, 256, 0, h->stream>>>(Ff, h->dC2F + h->nCoinc, h->nMid, c, la);
+        k_c2f_interp<S, R><<<(h->nMid * comps + 255) / 256, 256, 0, h->stream>>>(Ff, h->dC2F + h->nCoinc, h->nMid, c,
+                                                                                    la);
     if (h->nCen)
-        k_c2f_interp<S, R><<<(h->nCen * Q + 255) / 256, 256, 0, h->stream>>>(Ff, h->dC2F + h->nCoinc + h->nMid,
-                                                                                h->nCen, c, la);
+        k_c2f_interp<S, R><<<(h->nCen * comps + 255) / 256, 256, 0, h->stream>>>(Ff, h->dC2F + h->nCoinc + h->nMid,
+                                                                                    h->nCen, c, la);
 }
 
 // one coarse step: single level, or the two-level sequence of
@@ -765,7 +798,7 @@ int enqueueStepT(acp_handle* h, int src, PhaseTimer* tm) {
         const CouplingArgs c = couplingArgs(h);
         if (tm) tm->mark(-1);
         if (h->nCoinc)
-            k_c2f_save<S, R><<<(h->nCoinc + 127) / 128, 128, 0, h->stream>>>(lc.A, h->dC2F, h->nCoinc, (R*)h->dPre, lc);
+            k_c2f_save<S, R><<<(h->nCoinc + 127) / 128, 128, 0, h->stream>>>(lc.A, h->dC2F, h->nCoinc, (R*)h->dPre, lc, c);
         if (tm) tm->mark(ACP_K_COUPLING);
         enqueueLevelStep<S, R>(h, 0, src, tm);  // coarse t -> t+1
         enqueueLevelStep<S, R>(h, 1, 0, tm);    // fine t -> t+1/2
@@ -1060,6 +1093,22 @@ int acp_create(const acp_case_desc* d, int device, acp_handle** out) {
                                   cudaMemcpyHostToDevice, h->stream));
         }
         if (h->nCoinc && (s = devAlloc(h, &h->dPre, (size_t)h->nCoinc * Q * rb))) return s;
+        if (h->partner) {
+            for (int l = 0; l < 2; ++l) {
+                LevelHost& L = h->host[l];
+                LevelDev& D = h->dev[l];
+                if ((s = devAlloc(h, (void**)&D.slot, (size_t)L.N * sizeof(int)))) return s;
+                CU(h, cudaMemcpyAsync(D.slot, L.slot.data(), (size_t)L.N * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+                if ((s = devAlloc(h, (void**)&D.sg, std::max<size_t>(1, (size_t)L.nSlots) * 12 * sizeof(double)))) return s;
+                CU(h, cudaMemsetAsync(D.sg, 0, std::max<size_t>(1, (size_t)L.nSlots) * 12 * sizeof(double), h->stream));
+            }
+            if (h->nCoinc) {
+                if ((s = devAlloc(h, (void**)&h->dNb, h->nbHost.size() * sizeof(C2FNbDev)))) return s;
+                CU(h, cudaMemcpyAsync(h->dNb, h->nbHost.data(), h->nbHost.size() * sizeof(C2FNbDev),
+                                      cudaMemcpyHostToDevice, h->stream));
+                if ((s = devAlloc(h, &h->dPreNb, (size_t)h->nCoinc * 24 * rb))) return s;
+            }
+        }
         if (!h->dcHost.empty()) {
             if ((s = devAlloc(h, (void**)&h->dDC, h->dcHost.size() * sizeof(DCDev)))) return s;
             CU(h, cudaMemcpyAsync(h->dDC, h->dcHost.data(), h->dcHost.size() * sizeof(DCDev), cudaMemcpyHostToDevice,
@@ -1086,6 +1135,10 @@ int acp_init(acp_handle* h) {
         }
     }
     CU(h, cudaGetLastError());
+    for (size_t l = 0; l < h->dev.size(); ++l)
+        if (h->dev[l].sg)
+            CU(h, cudaMemsetAsync(h->dev[l].sg, 0, std::max<size_t>(1, (size_t)h->host[l].nSlots) * 12 * sizeof(double),
+                                  h->stream));
     h->cur = 0;
     h->steps = 0;
     if (h->dCounter) CU(h, cudaMemsetAsync(h->dCounter, 0, sizeof(int), h->stream));
@@ -1397,7 +1450,11 @@ int acp_destroy(acp_handle* h) {
         cudaFree(D.code);
         cudaFree(D.lodiX);
         cudaFree(D.lodiZY);
+        cudaFree(D.slot);
+        cudaFree(D.sg);
     }
+    cudaFree(h->dNb);
+    cudaFree(h->dPreNb);
     cudaFree(h->dErr);
     cudaFree(h->dC2F);
     cudaFree(h->dF2C);

@@ -25,6 +25,8 @@ struct LevelHost {
     int per[3] = {0, 0, 0};  // periodic axes of this level
     std::vector<uint8_t> code;
     std::vector<BNodeDev> lodiX, lodiZY;
+    std::vector<int> slot;  // coupling node -> partner-strain record (empty: none kept)
+    int nSlots = 0;
     long long active = 0;
     double omega = 0, dt = 0, spacing = 0;
 };
@@ -35,6 +37,8 @@ struct LevelDev {
     BNodeDev* lodiX = nullptr;
     BNodeDev* lodiZY = nullptr;
     int nLodiX = 0, nLodiZY = 0;
+    int* slot = nullptr;    // see LevelHost::slot
+    double* sg = nullptr;   // [12][nSlots] partner strain S and cubic-Mach gradient G
 };
 
 inline size_t storageBytes(int storage) {
@@ -63,6 +67,11 @@ struct acp_handle {
     acp::C2FDev* dC2F = nullptr;
     acp::F2CDev* dF2C = nullptr;
     void* dPre = nullptr;  // coarse populations before the coarse step, [Q][nCoinc]
+    // partner strain of the coupling nodes (STD; HRR, or RR with cubic-Mach)
+    bool partner = false;
+    std::vector<acp::C2FNbDev> nbHost;
+    acp::C2FNbDev* dNb = nullptr;
+    void* dPreNb = nullptr;  // [24][nCoinc] drho, u of the coincident nodes' coarse neighbours at t
     int* dErr = nullptr;
     // probes
     long long* dProbeNodes = nullptr;
@@ -118,6 +127,9 @@ LevelArgs<S> levelArgs(const acp_handle* h, int l, int src) {
     a.sigma = h->d.hybrid_sigma;
     for (int q = 0; q < Q; ++q) a.hscale[q] = h->hscale[q];
     for (int c = 0; c < 18; ++c) a.m4[c] = h->m4[c];
+    a.slot = D.slot;
+    a.sg = D.sg;
+    a.nSlots = L.nSlots;
     return a;
 }
 
@@ -133,8 +145,20 @@ inline CouplingArgs couplingArgs(const acp_handle* h) {
     c.alphaF2C = 2.0 * c.omegaF / c.omegaC;
     c.mrtStyle = h->d.scaling_style == ACP_SCALING_MRT;
     c.filter = h->d.f2c_filter;
+    c.partner = h->partner ? 1 : 0;
+    c.nSlotsF = h->host[1].nSlots;
+    c.nSlotsC = h->host[0].nSlots;
+    c.nb = h->dNb;
+    c.preNb = h->dPreNb;
+    c.sgF = h->dev[1].sg;
+    c.sgC = h->dev[0].sg;
+    c.slotF = h->dev[1].slot;
     return c;
 }
+
+// components one C2F interpolation thread handles per hanging node: the
+// populations, and the partner strain when it is kept
+inline int interpComponents(const acp_handle* h) { return Q + (h->partner ? 12 : 0); }
 
 // LODI arguments of level l (Node::LODIpressureOutlet's constants: L is the
 // node count times the coarse spacing on every level, Node.cpp:311)

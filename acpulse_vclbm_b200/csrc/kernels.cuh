@@ -81,6 +81,9 @@ struct LevelArgs {
     double sigma;   // HRR hybrid parameter
     float hscale[Q];  // FP16 per-population scales (1 otherwise)
     double m4[18];    // sum_q w_q H2_q,ab H4_q,k(kappa), ab in {xx,yy,zz,xy,xz,yz}, k in 0..2
+    const int* slot;  // coupling node -> record of its partner strain (null: none kept)
+    const double* sg; // partner strain S and cubic-Mach gradient G, [12][nSlots], level lattice units
+    int nSlots;
 };
 
 __device__ __forceinline__ int wrapc(int c, int n, int per) {
@@ -497,19 +500,21 @@ __device__ __forceinline__ void planePass(const LevelArgs<S>& a, MomR<R> (*slot)
 // neighbours' velocities, Node.cpp:1882-1888) and the cubic-Mach gradient
 // G of the Psi terms (Node.cpp:1832-1878), both in lattice units, from the
 // six axis neighbours' moments (+x, -x, +y, -y, +z, -z)
+// (inv2h: 1 / (2 h) for neighbours h level cells away; 1/2 on the level's own lattice)
 template <typename R, bool STRAIN, bool CUBIC>
 __device__ __forceinline__ void neighbourTerms(const MomR<R>& mxp, const MomR<R>& mxm, const MomR<R>& myp,
                                                const MomR<R>& mym, const MomR<R>& mzp, const MomR<R>& mzm, R shift,
-                                               R* SG) {
+                                               R* SG, R inv2h = R(0.5)) {
 #pragma unroll
     for (int c = 0; c < 12; ++c) SG[c] = 0;
     if (STRAIN) {
-        SG[0] = R(0.5) * (mxp.ux - mxm.ux);
-        SG[1] = R(0.5) * (myp.uy - mym.uy);
-        SG[2] = R(0.5) * (mzp.uz - mzm.uz);
-        SG[3] = R(0.25) * ((mxp.uy - mxm.uy) + (myp.ux - mym.ux));
-        SG[4] = R(0.25) * ((mxp.uz - mxm.uz) + (mzp.ux - mzm.ux));
-        SG[5] = R(0.25) * ((myp.uz - mym.uz) + (mzp.uy - mzm.uy));
+        const R half = R(0.5) * inv2h;
+        SG[0] = inv2h * (mxp.ux - mxm.ux);
+        SG[1] = inv2h * (myp.uy - mym.uy);
+        SG[2] = inv2h * (mzp.uz - mzm.uz);
+        SG[3] = half * ((mxp.uy - mxm.uy) + (myp.ux - mym.ux));
+        SG[4] = half * ((mxp.uz - mxm.uz) + (mzp.ux - mzm.ux));
+        SG[5] = half * ((myp.uz - mym.uz) + (mzp.uy - mzm.uy));
     }
     if (CUBIC) {
         auto psiT = [shift](const MomR<R>& m, R* P) {
@@ -527,15 +532,16 @@ __device__ __forceinline__ void neighbourTerms(const MomR<R>& mxp, const MomR<R>
         };
         R* G = SG + 6;
         R Pp[10], Pm[10];
+        const R h = inv2h;
         psiT(mxp, Pp); psiT(mxm, Pm);
-        G[0] += R(0.5) * (Pp[0] - Pm[0]); G[1] += R(0.5) * (Pp[3] - Pm[3]); G[2] += R(0.5) * (Pp[6] - Pm[6]);
-        G[3] += R(0.5) * (Pp[1] - Pm[1]); G[4] += R(0.5) * (Pp[2] - Pm[2]); G[5] += R(0.5) * (Pp[9] - Pm[9]);
+        G[0] += h * (Pp[0] - Pm[0]); G[1] += h * (Pp[3] - Pm[3]); G[2] += h * (Pp[6] - Pm[6]);
+        G[3] += h * (Pp[1] - Pm[1]); G[4] += h * (Pp[2] - Pm[2]); G[5] += h * (Pp[9] - Pm[9]);
         psiT(myp, Pp); psiT(mym, Pm);
-        G[0] += R(0.5) * (Pp[1] - Pm[1]); G[1] += R(0.5) * (Pp[4] - Pm[4]); G[2] += R(0.5) * (Pp[7] - Pm[7]);
-        G[3] += R(0.5) * (Pp[3] - Pm[3]); G[4] += R(0.5) * (Pp[9] - Pm[9]); G[5] += R(0.5) * (Pp[5] - Pm[5]);
+        G[0] += h * (Pp[1] - Pm[1]); G[1] += h * (Pp[4] - Pm[4]); G[2] += h * (Pp[7] - Pm[7]);
+        G[3] += h * (Pp[3] - Pm[3]); G[4] += h * (Pp[9] - Pm[9]); G[5] += h * (Pp[5] - Pm[5]);
         psiT(mzp, Pp); psiT(mzm, Pm);
-        G[0] += R(0.5) * (Pp[2] - Pm[2]); G[1] += R(0.5) * (Pp[5] - Pm[5]); G[2] += R(0.5) * (Pp[8] - Pm[8]);
-        G[3] += R(0.5) * (Pp[9] - Pm[9]); G[4] += R(0.5) * (Pp[6] - Pm[6]); G[5] += R(0.5) * (Pp[7] - Pm[7]);
+        G[0] += h * (Pp[2] - Pm[2]); G[1] += h * (Pp[5] - Pm[5]); G[2] += h * (Pp[8] - Pm[8]);
+        G[3] += h * (Pp[9] - Pm[9]); G[4] += h * (Pp[6] - Pm[6]); G[5] += h * (Pp[7] - Pm[7]);
     }
 }
 
@@ -575,8 +581,17 @@ __device__ __forceinline__ void tiledNode(const LevelArgs<S>& a, MomR<R> (*sm)[T
         const MomR<R> me = sm[sc][ty + 1][tx + 1];
         const R u[3] = {me.ux, me.uy, me.uz};
         if (code >= CODE_IFACE0) {
+            // coupling node: partner strain from the other level when kept, else Pi1 alone
             Pusher<S> emit{a, n, c_pushMask[code], nbOffsets(a, i, j, z)};
-            regularisedEmit<R, OP, ORDER, CUBIC>(me.drho, u, s2, a, (const R*)nullptr, emit);
+            if (a.slot) {
+                const int sl = a.slot[n];
+                R SG[12];
+#pragma unroll
+                for (int c = 0; c < 12; ++c) SG[c] = R(a.sg[c * a.nSlots + sl]);
+                regularisedEmit<R, OP, ORDER, CUBIC>(me.drho, u, s2, a, SG, emit);
+            } else {
+                regularisedEmit<R, OP, ORDER, CUBIC>(me.drho, u, s2, a, (const R*)nullptr, emit);
+            }
         } else {
             // fluid nodes are interior or on periodic axes: every axis neighbour exists
             R SG[12];
@@ -918,6 +933,13 @@ struct F2CDev {
     uint32_t mask;
     int cube[27];    // 3x3x3 fine neighbourhood, x fastest
 };
+// sources of a fine coincident node's partner strain: the regular coarse axis
+// neighbours of its coarse node (+x +y -x -y +z -z), or where that neighbour
+// is a coupling node, the regular fine node two fine cells away
+struct C2FNbDev {
+    int c[6];  // coarse neighbour or -1
+    int f[6];  // fine node (used when c < 0)
+};
 struct CouplingArgs {
     long long Nc, Nf;  // node counts of the coarse and fine arrays
     double shiftC;     // storage shift (both levels)
@@ -926,7 +948,39 @@ struct CouplingArgs {
     double omegaC, omegaF;
     int mrtStyle;      // Scaling-Style MRTSTYLE
     int filter;        // F2C-Filter
+    // partner strain of the coupling nodes (HRR, RR with cubic-Mach; STD)
+    int partner;
+    int nSlotsF, nSlotsC;
+    const C2FNbDev* nb;  // per coincident node
+    void* preNb;         // [24][coincident] drho, u of the coarse neighbours at t (compute type)
+    double* sgF;         // [12][nSlotsF] fine coupling nodes, in C2F list order
+    double* sgC;         // [12][nSlotsC] coarse coupling nodes, in F2C list order
+    const int* slotF;    // fine node -> slot
 };
+
+// threads per node of the coincident C2F kernel (blocks of 128 threads)
+__host__ __device__ inline int coincidentThreadsPerNode(const CouplingArgs& c) { return c.partner ? 8 : 1; }
+
+// drho and lattice velocity of node n of an arbitrary array of a level
+template <typename S, typename R>
+__device__ __forceinline__ MomR<R> nodeMomentsAt(const S* arr, long long N, const LevelArgs<S>& la, long long n) {
+    R d = 0, jx = 0, jy = 0, jz = 0;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const R g = R(Store<S>::load(arr + (long long)q * N + n, la.hscale[q]));
+        d += g;
+        jx += R(ex(q)) * g;
+        jy += R(ey(q)) * g;
+        jz += R(ez(q)) * g;
+    }
+    MomR<R> m;
+    m.drho = d;
+    const R inv = R(1) / (R(la.shift) + d);
+    m.ux = jx * inv;
+    m.uy = jy * inv;
+    m.uz = jz * inv;
+    return m;
+}
 
 // equilibrium split of one node's populations (deviation form)
 template <typename R, int ORDER>
@@ -976,17 +1030,29 @@ __device__ __forceinline__ void rescaleNeq(R* neq, const CouplingArgs& c, bool t
 // populations of the coincident coupling sources before the coarse step
 template <typename S, typename R>
 __device__ __forceinline__ void c2fSaveBody(const S* __restrict__ Ac, const C2FDev* __restrict__ nodes, int count, R* pre,
-                                            const LevelArgs<S>& la, int bx) {
+                                            const LevelArgs<S>& la, const CouplingArgs& c, int bx) {
     const int t = bx * blockDim.x + threadIdx.x;
     if (t >= count) return;
     const int src = nodes[t].src;
 #pragma unroll
     for (int q = 0; q < Q; ++q) pre[(long long)q * count + t] = R(Store<S>::load(Ac + (long long)q * la.N + src, la.hscale[q]));
+    if (c.partner) {
+        R* pn = (R*)c.preNb;
+        for (int d = 0; d < 6; ++d) {
+            const int m = c.nb[t].c[d];
+            if (m < 0) continue;
+            const MomR<R> mo = nodeMomentsAt<S, R>(Ac, la.N, la, m);
+            pn[(long long)(d * 4 + 0) * count + t] = mo.drho;
+            pn[(long long)(d * 4 + 1) * count + t] = mo.ux;
+            pn[(long long)(d * 4 + 2) * count + t] = mo.uy;
+            pn[(long long)(d * 4 + 3) * count + t] = mo.uz;
+        }
+    }
 }
 template <typename S, typename R>
 __global__ void k_c2f_save(const S* __restrict__ Ac, const C2FDev* __restrict__ nodes, int count, R* pre,
-                           LevelArgs<S> la) {
-    c2fSaveBody<S, R>(Ac, nodes, count, pre, la, blockIdx.x);
+                           LevelArgs<S> la, CouplingArgs c) {
+    c2fSaveBody<S, R>(Ac, nodes, count, pre, la, c, blockIdx.x);
 }
 
 
@@ -995,22 +1061,66 @@ template <typename S, typename R, int ORDER>
 __device__ __forceinline__ void c2fCoincidentBody(const S* __restrict__ Bc, S* Ff, const C2FDev* __restrict__ nodes, int count,
                                                   const R* __restrict__ pre, R th, const CouplingArgs& c,
                                                   const LevelArgs<S>& la, int bx) {
-    const int t = bx * blockDim.x + threadIdx.x;
-    if (t >= count) return;
-    const C2FDev nd = nodes[t];
-    R g[Q], geq[Q];
+    // one thread per node, or (partner strain kept) eight: the first forms the
+    // populations, the first six each gather one stencil neighbour's moments
+    const int tpn = coincidentThreadsPerNode(c);
+    const int tg = bx * blockDim.x + threadIdx.x;
+    const int t = tg / tpn, sub = tg - t * tpn;
+    const bool valid = t < count;
+    if (valid && sub == 0) {
+        const C2FDev nd = nodes[t];
+        R g[Q], geq[Q];
 #pragma unroll
-    for (int q = 0; q < Q; ++q) {
-        const R now = R(Store<S>::load(Bc + (long long)q * c.Nc + nd.src, la.hscale[q]));
-        g[q] = (R(1) - th) * pre[(long long)q * count + t] + th * now;
+        for (int q = 0; q < Q; ++q) {
+            const R now = R(Store<S>::load(Bc + (long long)q * c.Nc + nd.src, la.hscale[q]));
+            g[q] = (R(1) - th) * pre[(long long)q * count + t] + th * now;
+        }
+        eqSplit<R, ORDER>(g, R(c.shiftC), R(c.kappa), geq);
+#pragma unroll
+        for (int q = 0; q < Q; ++q) g[q] -= geq[q];
+        rescaleNeq<R>(g, c, true);
+#pragma unroll
+        for (int q = 0; q < Q; ++q)
+            if (nd.mask >> q & 1u) Store<S>::store(Ff + (long long)q * c.Nf + nd.n, geq[q] + g[q], la.hscale[q]);
     }
-    eqSplit<R, ORDER>(g, R(c.shiftC), R(c.kappa), geq);
+    if (!c.partner) return;  // uniform over the launch
+    // partner strain on the coarse stencil (two fine cells) at the fine state's time
+    // (Node.cpp:2114-2380): regular coarse neighbours blended between t and t+1,
+    // the other neighbours from regular fine nodes at the current fine time
+    __shared__ R mom[128 / 8][6][4];
+    const int local = threadIdx.x / 8;
+    if (valid && sub < 6) {
+        const R* pn = (const R*)c.preNb;
+        const int cn = c.nb[t].c[sub];
+        MomR<R> m;
+        if (cn >= 0) {
+            const MomR<R> now = nodeMomentsAt<S, R>(Bc, c.Nc, la, cn);
+            m.drho = (R(1) - th) * pn[(long long)(sub * 4 + 0) * count + t] + th * now.drho;
+            m.ux = (R(1) - th) * pn[(long long)(sub * 4 + 1) * count + t] + th * now.ux;
+            m.uy = (R(1) - th) * pn[(long long)(sub * 4 + 2) * count + t] + th * now.uy;
+            m.uz = (R(1) - th) * pn[(long long)(sub * 4 + 3) * count + t] + th * now.uz;
+        } else {
+            m = nodeMomentsAt<S, R>((const S*)Ff, c.Nf, la, c.nb[t].f[sub]);
+        }
+        mom[local][sub][0] = m.drho;
+        mom[local][sub][1] = m.ux;
+        mom[local][sub][2] = m.uy;
+        mom[local][sub][3] = m.uz;
+    }
+    __syncthreads();
+    if (valid && sub == 0) {
+        MomR<R> m[6];
+        for (int d = 0; d < 6; ++d) {
+            m[d].drho = mom[local][d][0];
+            m[d].ux = mom[local][d][1];
+            m[d].uy = mom[local][d][2];
+            m[d].uz = mom[local][d][3];
+        }
+        R SG[12];
+        neighbourTerms<R, true, true>(m[0], m[2], m[1], m[3], m[4], m[5], R(c.shiftC), SG, R(0.25));
 #pragma unroll
-    for (int q = 0; q < Q; ++q) g[q] -= geq[q];
-    rescaleNeq<R>(g, c, true);
-#pragma unroll
-    for (int q = 0; q < Q; ++q)
-        if (nd.mask >> q & 1u) Store<S>::store(Ff + (long long)q * c.Nf + nd.n, geq[q] + g[q], la.hscale[q]);
+        for (int k = 0; k < 12; ++k) c.sgF[(long long)k * c.nSlotsF + t] = double(SG[k]);
+    }
 }
 template <typename S, typename R, int ORDER>
 __global__ void k_c2f_coincident(const S* __restrict__ Bc, S* Ff, const C2FDev* __restrict__ nodes, int count,
@@ -1026,10 +1136,19 @@ template <typename S, typename R>
 __device__ __forceinline__ void c2fInterpBody(S* Ff, const C2FDev* __restrict__ nodes, int count, const CouplingArgs& c,
                                               const LevelArgs<S>& la, int bx) {
     const long long t = (long long)bx * blockDim.x + threadIdx.x;
-    if (t >= (long long)count * Q) return;
+    if (t >= (long long)count * (Q + (c.partner ? 12 : 0))) return;
     const int q = (int)(t / count);
     const int m = (int)(t - (long long)q * count);
     const C2FDev& nd = nodes[m];
+    if (q >= Q) {
+        // partner strain of the hanging node, interpolated like its populations
+        const int k = q - Q;
+        double acc = 0;
+        for (int s = 0; s < 4; ++s)
+            if (nd.st[s] >= 0) acc += double(nd.w[s]) * c.sgF[(long long)k * c.nSlotsF + c.slotF[nd.st[s]]];
+        c.sgF[(long long)k * c.nSlotsF + c.slotF[nd.n]] = acc;
+        return;
+    }
     if (!(nd.mask >> q & 1u)) return;
     R acc = 0;
 #pragma unroll
@@ -1073,7 +1192,29 @@ __device__ __forceinline__ void f2cBody(const S* __restrict__ Ff, S* Bc, const F
     for (int q = 0; q < Q; ++q)
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) neq[q] += __shfl_down_sync(0xffffffffu, neq[q], off);
+    // partner strain from the fine partner's axis neighbours at t+1 (half a
+    // coarse cell away, Node.cpp:2383-2490): lane d < 6 gathers neighbour d
+    // (+x +y -x -y +z -z of the cube), lane 0 assembles
+    R SG[12];
+    if (c.partner) {
+        const int face[6] = {14, 16, 12, 10, 22, 4};
+        MomR<R> mine = {R(0), R(0), R(0), R(0)};
+        if (lane < 6) mine = nodeMomentsAt<S, R>(Ff, c.Nf, la, nd.cube[face[lane]]);
+        MomR<R> m[6];
+#pragma unroll
+        for (int d = 0; d < 6; ++d) {
+            m[d].drho = __shfl_sync(0xffffffffu, mine.drho, d);
+            m[d].ux = __shfl_sync(0xffffffffu, mine.ux, d);
+            m[d].uy = __shfl_sync(0xffffffffu, mine.uy, d);
+            m[d].uz = __shfl_sync(0xffffffffu, mine.uz, d);
+        }
+        neighbourTerms<R, true, true>(m[0], m[2], m[1], m[3], m[4], m[5], R(c.shiftC), SG, R(1));
+    }
     if (lane != 0) return;
+    if (c.partner) {
+#pragma unroll
+        for (int k = 0; k < 12; ++k) c.sgC[(long long)k * c.nSlotsC + warp] = double(SG[k]);
+    }
     R g[Q], geq[Q];
 #pragma unroll
     for (int q = 0; q < Q; ++q) g[q] = R(Store<S>::load(Ff + (long long)q * c.Nf + nd.partner, la.hscale[q]));

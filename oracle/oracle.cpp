@@ -51,6 +51,7 @@ struct Level {
     std::vector<double> f[2];  // [N][19] per ping-pong array (Node::distr_)
     std::vector<double> preCol;
     std::vector<double> psi;   // Node::psi_ (cubic-Mach correction, persistent)
+    std::vector<double> strain;  // [N][6] finite-difference strain of coupling nodes from partners
     std::vector<unsigned char> type;
     std::vector<BNode> bnodes;
     std::vector<long> nb;      // [N][18] push targets (-1: none)
@@ -206,6 +207,21 @@ struct Oracle {
     };
     std::vector<DCNode> dc;     // one per coincident C2F node, same order
     bool isDC() const { return desc.coupling != ACP_COUPLING_STD; }
+    // HRR partner strain (Node.cpp:2114-2490, the STD scheme's partner passes
+    // of Lattice.cpp:12142-12177, 12882-12934, 13211-13246): a coupling node's
+    // finite-difference strain and cubic-Mach terms come from the other
+    // level's stencil; every node read is a regular node whose state is
+    // complete at that time
+    bool partnerStrain() const {
+        return !isDC() && lev.size() == 2 && (desc.op == ACP_OP_HRR || (desc.op == ACP_OP_RR && desc.cubic_mach));
+    }
+    struct NbSrc {
+        long c[6];  // coarse axis neighbour (regular) of the coincident coarse node, or -1
+        long f[6];  // else the regular fine node two fine cells away
+    };
+    std::vector<NbSrc> nbsrc;   // per coincident C2F node
+    std::vector<double> preNb;  // [coincident][6][4] rho, u of the coarse neighbours at t
+    bool couplingOk = true;
     std::vector<double> pre;    // coarse populations before the coarse step, per coincident C2F node
     int boxLo[3], boxHi[3], loIf[3], hiIf[3], spans[3];
 
@@ -396,10 +412,15 @@ struct Oracle {
             return;
         }
         const bool iface = L.type[n] == NT_IFACE;
+        const bool partner = iface && partnerStrain();
         bool needStrain = ((op == ACP_OP_HRR) || k.cubic) && !iface;
         double S[6] = {0, 0, 0, 0, 0, 0};
-        if (iface)
+        if (partner) {
+            // strain and cubic-Mach terms set by the coupling passes from the partner level
+            for (int c = 0; c < 6; ++c) S[c] = L.strain[n * 6 + c];
+        } else if (iface) {
             for (int q = 0; q < Q; ++q) psi[q] = 0.;  // no finite differences across the interface
+        }
         if (needStrain) {
             // neighbours' pre-collision moments (calcDensityPreCol/VelocityPreCol)
             double nbRho[6], nbU[6][3], dist[6];
@@ -421,7 +442,7 @@ struct Oracle {
             double kinVisc = k.nu;
             double dynVisc = kinVisc * densH;
             double invPreFactor = -((dt * k.cs2) / (L.omega * kinVisc));
-            double sg = iface ? 1. : k.sigma, a[6];  // coupling nodes: recursive regularisation of Pi1
+            double sg = iface && !partner ? 1. : k.sigma, a[6];  // without partners: regularisation of Pi1
             for (int c = 0; c < 6; ++c) a[c] = sg * P[c] + (1. - sg) * invPreFactor * (2. * dynVisc * S[c]);
             recursiveNeq(k, k.order, a, u, neq);
         }
@@ -661,6 +682,7 @@ struct Oracle {
         markLevel(F, gf);
         if (!wireLevel(F)) return false;
         buildCouplings();
+        if (!couplingOk) { err = "partner strain stencil missing"; return false; }
         return true;
     }
 
@@ -669,6 +691,7 @@ struct Oracle {
         for (int a = 0; a < 2; ++a) L.f[a].assign(L.N * Q, 0.);
         L.preCol.assign(L.N * Q, 0.);
         L.psi.assign(L.N * Q, 0.);
+        L.strain.assign(L.N * 6, 0.);
         L.type.assign(L.N, NT_INTERIOR);
         L.nb.assign(L.N * 18, -1);
         L.dt = k.dt(l);
@@ -834,6 +857,25 @@ struct Oracle {
         c2f.insert(c2f.end(), mid.begin(), mid.end());
         c2f.insert(c2f.end(), cen.begin(), cen.end());
         pre.assign(coinc.size() * Q, 0.);
+        nbsrc.clear();
+        if (partnerStrain()) {
+            auto regular = [](const Level& L, long n) { return L.type[n] == NT_INTERIOR || L.type[n] == NT_BOUNDARY; };
+            for (const C2FNode& cn : coinc) {
+                NbSrc nb;
+                const int cc[3] = {(int)(cn.src % C.nx), (int)((cn.src / C.nx) % C.ny), (int)(cn.src / ((long)C.nx * C.ny))};
+                for (int q = 0; q < 6; ++q) {
+                    int g[3] = {cc[0] + C.org[0] + EX[q], cc[1] + C.org[1] + EY[q], cc[2] + C.org[2] + EZ[q]};
+                    long t;
+                    nb.c[q] = nb.f[q] = -1;
+                    if (local(C, g, t) && regular(C, t)) { nb.c[q] = t; continue; }
+                    int gf[3] = {2 * g[0], 2 * g[1], 2 * g[2]};
+                    if (local(F, gf, t) && regular(F, t)) nb.f[q] = t;
+                    else couplingOk = false;
+                }
+                nbsrc.push_back(nb);
+            }
+            preNb.assign(coinc.size() * 24, 0.);
+        }
         f2c.clear();
         for (int kk = 0; kk < C.nz; ++kk)
             for (int j = 0; j < C.ny; ++j)
@@ -1093,8 +1135,41 @@ struct Oracle {
         double* FB = F.f[fnew].data();
         const double* CB = C.f[cnew].data();
         long ic = 0;
+        const bool ps = !nbsrc.empty();
         for (const C2FNode& cn : c2f) {
             double v[Q];
+            if (ps && cn.kind == 0) {
+                // coarse stencil at the time of the fine state: regular coarse
+                // neighbours blended between t and t+1, the others from the
+                // regular fine node two cells away (Node.cpp:2244-2380)
+                const NbSrc& nb = nbsrc[ic];
+                double nbRho[6], nbU[6][3], dist[6];
+                for (int d = 0; d < 6; ++d) {
+                    dist[d] = k.spacing;
+                    if (nb.c[d] >= 0) {
+                        double r, u[3];
+                        plainMoments(k, &CB[nb.c[d] * Q], r, u);
+                        nbRho[d] = (1. - th) * preNb[ic * 24 + d * 4] + th * r;
+                        for (int c = 0; c < 3; ++c) nbU[d][c] = (1. - th) * preNb[ic * 24 + d * 4 + 1 + c] + th * u[c];
+                    } else {
+                        plainMoments(k, &FB[nb.f[d] * Q], nbRho[d], nbU[d]);
+                    }
+                }
+                strainAndPsi(k, nbRho, nbU, dist, &F.strain[cn.n * 6], &F.psi[cn.n * Q]);
+            } else if (ps) {
+                for (int c = 0; c < 6; ++c) {
+                    double acc = 0;
+                    for (int m = 0; m < 4; ++m)
+                        if (cn.st[m] >= 0) acc += cn.w[m] * F.strain[cn.st[m] * 6 + c];
+                    F.strain[cn.n * 6 + c] = acc;
+                }
+                for (int q = 0; q < Q; ++q) {
+                    double acc = 0;
+                    for (int m = 0; m < 4; ++m)
+                        if (cn.st[m] >= 0) acc += cn.w[m] * F.psi[cn.st[m] * Q + q];
+                    F.psi[cn.n * Q + q] = acc;
+                }
+            }
             if (cn.kind == 0) {
                 double f[Q], eq[Q], rho, u[3], neq[Q], sc[Q];
                 for (int q = 0; q < Q; ++q) f[q] = (1. - th) * pre[ic * Q + q] + th * CB[cn.src * Q + q];
@@ -1149,6 +1224,16 @@ struct Oracle {
             rescale(neq, sc, false);
             for (int q = 0; q < Q; ++q)
                 if (fn.mask >> q & 1u) CB[fn.n * Q + q] = eq[q] + sc[q];
+            if (!nbsrc.empty()) {
+                // the fine partner's axis neighbours at t+1, fine spacing (Node.cpp:2383-2490)
+                const int face[6] = {14, 16, 12, 10, 22, 4};  // +x +y -x -y +z -z in the 3x3x3 cube
+                double nbRho[6], nbU[6][3], dist[6];
+                for (int d = 0; d < 6; ++d) {
+                    plainMoments(k, &FA[fn.cube[face[d]] * Q], nbRho[d], nbU[d]);
+                    dist[d] = F.spacing;
+                }
+                strainAndPsi(k, nbRho, nbU, dist, &C.strain[fn.n * 6], &C.psi[fn.n * Q]);
+            }
         }
     }
 
@@ -1159,6 +1244,14 @@ struct Oracle {
         for (const C2FNode& cn : c2f)
             if (cn.kind == 0) {
                 for (int q = 0; q < Q; ++q) pre[ic * Q + q] = C.f[alt][cn.src * Q + q];
+                if (!nbsrc.empty())
+                    for (int d = 0; d < 6; ++d)
+                        if (nbsrc[ic].c[d] >= 0) {
+                            double r, u[3];
+                            plainMoments(k, &C.f[alt][nbsrc[ic].c[d] * Q], r, u);
+                            preNb[ic * 24 + d * 4] = r;
+                            for (int c = 0; c < 3; ++c) preNb[ic * 24 + d * 4 + 1 + c] = u[c];
+                        }
                 ++ic;
             }
         const int cnew = 1 - alt;
