@@ -103,7 +103,7 @@ __global__ void __launch_bounds__(TX * TY, TiledMinBlocks<R>::value)
 }
 
 template <typename S, int ORDER>
-__global__ void __launch_bounds__(128) kb_lodi(const BatchCase<S>* __restrict__ cases,
+__global__ void __launch_bounds__(32) kb_lodi(const BatchCase<S>* __restrict__ cases,
                                                const WorkItem* __restrict__ items, int n, int level, int fineSrc,
                                                int flip, int zy) {
     __shared__ LevelArgs<S> sa;
@@ -283,6 +283,8 @@ struct Group {
     Range collide[2], lodiX[2], lodiZY[2], save, coinc, mid, cen, f2c;
     cudaStream_t stream = nullptr;
     cudaEvent_t joined = nullptr;
+    cudaStream_t side = nullptr;  // the coarse step beside the first fine sub-step
+    cudaEvent_t sideFork = nullptr, sideJoin = nullptr;
     int resident[9] = {0};  // resident blocks per SM of each batch kernel (occupancy)
 };
 
@@ -433,11 +435,13 @@ int buildGroup(acp_batch* b, Group& g) {
         phase(g.collide[l], [&](int c, const acp_handle* h) {
             collideItems(h->host[l], c, g.tiled, recs[c].lv[l].zChunk, items);
         });
-        phase(g.lodiX[l], [&](int c, const acp_handle* h) { blockItems(c, h->dev[l].nLodiX, 128, items); });
-        phase(g.lodiZY[l], [&](int c, const acp_handle* h) { blockItems(c, h->dev[l].nLodiZY, 128, items); });
+        phase(g.lodiX[l], [&](int c, const acp_handle* h) { blockItems(c, h->dev[l].nLodiX, 32, items); });
+        phase(g.lodiZY[l], [&](int c, const acp_handle* h) { blockItems(c, h->dev[l].nLodiZY, 32, items); });
     }
     if (g.levels == 2) {
-        phase(g.save, [&](int c, const acp_handle* h) { blockItems(c, h->nCoinc, 128, items); });
+        phase(g.save, [&](int c, const acp_handle* h) {
+            blockItems(c, (long long)h->nCoinc * coincidentThreadsPerNode(couplingArgs(h)), 128, items);
+        });
         phase(g.coinc, [&](int c, const acp_handle* h) {
             blockItems(c, (long long)h->nCoinc * (h->dcHost.empty() ? coincidentThreadsPerNode(couplingArgs(h)) : 1), 128,
                        items);
@@ -475,7 +479,7 @@ int occupancy(Group& g, const acp_case_desc& d) {
     };
     const int o = d.eq_order;
     g.resident[0] = occ((const void*)pickBatchCollide<S, R>(d), g.tiled ? TX * TY : 128);
-    g.resident[1] = occ((const void*)pickBatchLodi<S>(o), 128);
+    g.resident[1] = occ((const void*)pickBatchLodi<S>(o), 32);
     g.resident[2] = occ((const void*)kb_c2f_save<S, R>, 128);
     g.resident[3] = occ((const void*)pickBatchCoinc<S, R>(o), 128);
     g.resident[4] = occ((const void*)kb_c2f_interp<S, R>, 256);
@@ -495,20 +499,20 @@ void enqueueGroup(acp_batch* b, Group& g, int flip) {
     KbCollide<S> collide = pickBatchCollide<S, R>(d);
     KbLodi<S> lodi = pickBatchLodi<S>(o);
     const dim3 cblock = g.tiled ? dim3(TX, TY) : dim3(128);
-    auto levelStep = [&](int l, int fineSrc) {
+    auto levelStep = [&](int l, int fineSrc, cudaStream_t ls) {
         if (g.collide[l].count)
-            collide<<<gridFor(b, g.collide[l].count, g.resident[0]), cblock, 0, st>>>(cs, it + g.collide[l].off,
+            collide<<<gridFor(b, g.collide[l].count, g.resident[0]), cblock, 0, ls>>>(cs, it + g.collide[l].off,
                                                                                      g.collide[l].count, l, fineSrc,
                                                                                      flip);
         if (g.lodiX[l].count)
-            lodi<<<gridFor(b, g.lodiX[l].count, g.resident[1]), 128, 0, st>>>(cs, it + g.lodiX[l].off,
+            lodi<<<gridFor(b, g.lodiX[l].count, g.resident[1]), 32, 0, ls>>>(cs, it + g.lodiX[l].off,
                                                                              g.lodiX[l].count, l, fineSrc, flip, 0);
         if (g.lodiZY[l].count)
-            lodi<<<gridFor(b, g.lodiZY[l].count, g.resident[1]), 128, 0, st>>>(cs, it + g.lodiZY[l].off,
+            lodi<<<gridFor(b, g.lodiZY[l].count, g.resident[1]), 32, 0, ls>>>(cs, it + g.lodiZY[l].off,
                                                                               g.lodiZY[l].count, l, fineSrc, flip, 1);
     };
     if (g.levels == 1) {
-        levelStep(0, 0);
+        levelStep(0, 0, st);
         return;
     }
     KbCoinc<S, R> coinc = pickBatchCoinc<S, R>(o);
@@ -523,13 +527,18 @@ void enqueueGroup(acp_batch* b, Group& g, int flip) {
             kb_c2f_interp<S, R><<<gridFor(b, g.cen.count, g.resident[4]), 256, 0, st>>>(cs, it + g.cen.off,
                                                                                        g.cen.count, fdst, 1);
     };
+    // the coarse step (and the saving of the coupling sources) beside the first fine sub-step
+    cudaEventRecord(g.sideFork, st);
+    cudaStreamWaitEvent(g.side, g.sideFork, 0);
     if (g.save.count)
-        kb_c2f_save<S, R><<<gridFor(b, g.save.count, g.resident[2]), 128, 0, st>>>(cs, it + g.save.off, g.save.count,
-                                                                                  flip);
-    levelStep(0, 0);  // coarse t -> t+1
-    levelStep(1, 0);  // fine t -> t+1/2
+        kb_c2f_save<S, R><<<gridFor(b, g.save.count, g.resident[2]), 128, 0, g.side>>>(cs, it + g.save.off,
+                                                                                      g.save.count, flip);
+    levelStep(0, 0, g.side);  // coarse t -> t+1
+    levelStep(1, 0, st);      // fine t -> t+1/2
+    cudaEventRecord(g.sideJoin, g.side);
+    cudaStreamWaitEvent(st, g.sideJoin, 0);
     c2f(1, R(0.5));   // C2F (or direct coupling, fine side) at t+1/2
-    levelStep(1, 1);  // fine t+1/2 -> t+1
+    levelStep(1, 1, st);  // fine t+1/2 -> t+1
     if (g.f2c.count)
         pickBatchF2C<S, R>(o)<<<gridFor(b, g.f2c.count, g.resident[5]), 128, 0, st>>>(cs, it + g.f2c.off,
                                                                                       g.f2c.count, flip);
@@ -679,6 +688,9 @@ int acp_batch_create(acp_handle* const* cases, int n, acp_batch** out) {
     for (Group& g : b->groups) {
         BCU(b, cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
         BCU(b, cudaEventCreateWithFlags(&g.joined, cudaEventDisableTiming));
+        BCU(b, cudaStreamCreateWithFlags(&g.side, cudaStreamNonBlocking));
+        BCU(b, cudaEventCreateWithFlags(&g.sideFork, cudaEventDisableTiming));
+        BCU(b, cudaEventCreateWithFlags(&g.sideJoin, cudaEventDisableTiming));
         const acp_case_desc& d = b->cases[g.members[0]]->d;
         switch (g.storage) {
             case ACP_STORE_F64: occupancy<double, double>(g, d); break;
@@ -810,6 +822,9 @@ int acp_batch_destroy(acp_batch* b) {
         cudaFree(g.dItems);
         if (g.stream) cudaStreamDestroy(g.stream);
         if (g.joined) cudaEventDestroy(g.joined);
+        if (g.side) cudaStreamDestroy(g.side);
+        if (g.sideFork) cudaEventDestroy(g.sideFork);
+        if (g.sideJoin) cudaEventDestroy(g.sideJoin);
     }
     for (acp_handle* h : b->cases)
         if (h->batch == b) h->batch = nullptr;

@@ -36,6 +36,10 @@ __host__ __device__ constexpr int ez(int q) {
 }
 __host__ __device__ constexpr double wq(int q) { return q < 6 ? 1.0 / 18.0 : (q < 18 ? 1.0 / 36.0 : 1.0 / 3.0); }
 
+// correctly rounded reciprocal (the same value as 1 / x under IEEE division)
+__device__ __forceinline__ float rcpRN(float x) { return __frcp_rn(x); }
+__device__ __forceinline__ double rcpRN(double x) { return __drcp_rn(x); }
+
 // operator ids (enum acp_op)
 enum { OP_SRT = 0, OP_MRT_GS = 1, OP_MRT_RM = 2, OP_RR = 3, OP_HRR = 4 };
 

@@ -732,7 +732,8 @@ dim3 gridOf(const LevelHost& L, int bx) { return dim3((L.nx + bx - 1) / bx, L.ny
 
 // enqueue one step of a single level, reading array src
 template <typename S, typename R>
-int enqueueLevelStep(acp_handle* h, int l, int src, PhaseTimer* tm = nullptr) {
+int enqueueLevelStep(acp_handle* h, int l, int src, PhaseTimer* tm = nullptr, cudaStream_t st = nullptr) {
+    if (!st) st = h->stream;
     const LevelHost& L = h->host[l];
     const LevelDev& D = h->dev[l];
     LevelArgs<S> a = levelArgs<S>(h, l, src);
@@ -741,15 +742,17 @@ int enqueueLevelStep(acp_handle* h, int l, int src, PhaseTimer* tm = nullptr) {
     if (needsMoments(h->d)) {
         const int chunk = tiledChunk(L);
         dim3 grid((L.nx + TX - 1) / TX, (L.ny + TY - 1) / TY, (L.nz + chunk - 1) / chunk);
-        pickTiled<S, R>(h->d)<<<grid, dim3(TX, TY), 0, h->stream>>>(a, chunk);
+        pickTiled<S, R>(h->d)<<<grid, dim3(TX, TY), 0, st>>>(a, chunk);
     } else {
-        pickCollide<S, R>(h->d)<<<gridOf(L, bx), bx, 0, h->stream>>>(a);
+        pickCollide<S, R>(h->d)<<<gridOf(L, bx), bx, 0, st>>>(a);
     }
     if (tm) tm->mark(ACP_K_COLLIDE);
     const LodiArgs p = lodiArgsOf(h, l);
     LodiFn<S> lf = pickLodi<S>(h->d.eq_order);
-    if (D.nLodiX) lf<<<(D.nLodiX + 127) / 128, 128, 0, h->stream>>>(a.A, a.B, D.lodiX, D.nLodiX, p, a);
-    if (D.nLodiZY) lf<<<(D.nLodiZY + 127) / 128, 128, 0, h->stream>>>(a.A, a.B, D.lodiZY, D.nLodiZY, p, a);
+    // one thread per boundary node with long FP64 work: small blocks spread the few
+    // thousand nodes of a face over every SM
+    if (D.nLodiX) lf<<<(D.nLodiX + 31) / 32, 32, 0, st>>>(a.A, a.B, D.lodiX, D.nLodiX, p, a);
+    if (D.nLodiZY) lf<<<(D.nLodiZY + 31) / 32, 32, 0, st>>>(a.A, a.B, D.lodiZY, D.nLodiZY, p, a);
     if (tm && (D.nLodiX || D.nLodiZY)) tm->mark(ACP_K_LODI);
     return ACP_OK;
 }
@@ -796,12 +799,26 @@ int enqueueStepT(acp_handle* h, int src, PhaseTimer* tm) {
     } else {
         LevelArgs<S> lc = levelArgs<S>(h, 0, src);
         const CouplingArgs c = couplingArgs(h);
+        // the coarse step (with the saving of the coupling sources) and the first
+        // fine sub-step touch different arrays: in a graph they run side by side
+        const bool fork = tm == nullptr;
+        cudaStream_t cs = h->stream;
+        if (fork) {
+            cudaEventRecord(h->forkEv, h->stream);
+            cudaStreamWaitEvent(h->side, h->forkEv, 0);
+            cs = h->side;
+        }
         if (tm) tm->mark(-1);
         if (h->nCoinc)
-            k_c2f_save<S, R><<<(h->nCoinc + 127) / 128, 128, 0, h->stream>>>(lc.A, h->dC2F, h->nCoinc, (R*)h->dPre, lc, c);
+            k_c2f_save<S, R><<<(h->nCoinc * coincidentThreadsPerNode(c) + 127) / 128, 128, 0, cs>>>(
+                lc.A, h->dC2F, h->nCoinc, (R*)h->dPre, lc, c);
         if (tm) tm->mark(ACP_K_COUPLING);
-        enqueueLevelStep<S, R>(h, 0, src, tm);  // coarse t -> t+1
-        enqueueLevelStep<S, R>(h, 1, 0, tm);    // fine t -> t+1/2
+        enqueueLevelStep<S, R>(h, 0, src, tm, cs);  // coarse t -> t+1
+        enqueueLevelStep<S, R>(h, 1, 0, tm);        // fine t -> t+1/2
+        if (fork) {
+            cudaEventRecord(h->joinEv, h->side);
+            cudaStreamWaitEvent(h->stream, h->joinEv, 0);
+        }
         if (tm) tm->mark(-1);
         enqueueC2F<S, R>(h, 1 - src, 1, R(0.5));  // C2F at t+1/2
         if (tm) tm->mark(ACP_K_COUPLING);
@@ -1061,6 +1078,9 @@ int acp_create(const acp_case_desc* d, int device, acp_handle** out) {
     if (s) return s;
     CU(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     h->ownStream = true;
+    CU(h, cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
+    CU(h, cudaEventCreateWithFlags(&h->forkEv, cudaEventDisableTiming));
+    CU(h, cudaEventCreateWithFlags(&h->joinEv, cudaEventDisableTiming));
     if ((s = devAlloc(h, (void**)&h->dErr, sizeof(int)))) return s;
     CU(h, cudaMemsetAsync(h->dErr, 0, sizeof(int), h->stream));
     h->dev.resize(h->host.size());
@@ -1465,6 +1485,9 @@ int acp_destroy(acp_handle* h) {
     cudaFree(h->dSeries);
     cudaFree(h->dCounter);
     if (h->ownStream && h->stream) cudaStreamDestroy(h->stream);
+    if (h->side) cudaStreamDestroy(h->side);
+    if (h->forkEv) cudaEventDestroy(h->forkEv);
+    if (h->joinEv) cudaEventDestroy(h->joinEv);
     delete h;
     return ACP_OK;
 }

@@ -57,6 +57,8 @@ struct acp_handle {
     long long steps = 0;
     cudaStream_t stream = nullptr;
     bool ownStream = false;
+    cudaStream_t side = nullptr;  // second branch of a captured step (coarse level beside the fine sub-step)
+    cudaEvent_t forkEv = nullptr, joinEv = nullptr;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};  // one step starting from cur == 0 / cur == 1
     // two-level coupling (fine state always in array 0 between coarse steps)
     std::vector<acp::C2FDev> c2fHost;

@@ -241,7 +241,7 @@ struct Collider {
             jz += R(ez(q)) * g[q];
         }
         const R rho = R(a.shift) + drho;
-        const R inv = R(1) / rho;
+        const R inv = rcpRN(rho);
         R u[3] = {jx * inv, jy * inv, jz * inv};
         const R omega = R(a.omega);
         const R kappa = R(a.kappa);
@@ -439,7 +439,7 @@ __device__ __forceinline__ MomR<R> nodeMoments(const LevelArgs<S>& a, int n) {
     }
     MomR<R> m;
     m.drho = d;
-    const R inv = R(1) / (R(a.shift) + d);
+    const R inv = rcpRN(R(a.shift) + d);
     m.ux = jx * inv;
     m.uy = jy * inv;
     m.uz = jz * inv;
@@ -472,7 +472,7 @@ __device__ __forceinline__ void planePass(const LevelArgs<S>& a, MomR<R> (*slot)
                 secondSums<R>(g, s2);
                 MomR<R> m;
                 m.drho = d;
-                const R inv = R(1) / (R(a.shift) + d);
+                const R inv = rcpRN(R(a.shift) + d);
                 m.ux = jx * inv;
                 m.uy = jy * inv;
                 m.uz = jz * inv;
@@ -807,11 +807,10 @@ __device__ __forceinline__ void lodiBody(const S* __restrict__ A, S* B, const BN
     EqCoef<double, ORDER> ec;
     ec.set(u, p.kappa);
     const double drho = rho - p.shift;
-#pragma unroll
-    for (int q = 0; q < Q; ++q) {
-        const double geq = wq(q) * (drho + rho * ec.poly(q, p.kappa));
+    forEachDirection<double, ORDER>(ec, p.kappa, [&](int q, double poly) {
+        const double geq = wq(q) * (drho + rho * poly);
         Store<S>::store(B + q * p.N + b.n, (decltype(Store<S>::load(B, 1.f)))geq, hs[q]);
-    }
+    });
 }
 template <typename S, int ORDER>
 __global__ void k_lodi(const S* __restrict__ A, S* B, const BNodeDev* __restrict__ nodes, int count, LodiArgs p,
@@ -975,7 +974,7 @@ __device__ __forceinline__ MomR<R> nodeMomentsAt(const S* arr, long long N, cons
     }
     MomR<R> m;
     m.drho = d;
-    const R inv = R(1) / (R(la.shift) + d);
+    const R inv = rcpRN(R(la.shift) + d);
     m.ux = jx * inv;
     m.uy = jy * inv;
     m.uz = jz * inv;
@@ -994,7 +993,7 @@ __device__ __forceinline__ void eqSplit(const R* g, R shift, R kappa, R* geq) {
         jz += R(ez(q)) * g[q];
     }
     const R rho = shift + drho;
-    const R inv = R(1) / rho;
+    const R inv = rcpRN(rho);
     R u[3] = {jx * inv, jy * inv, jz * inv};
     EqCoef<R, ORDER> ec;
     ec.set(u, kappa);
@@ -1031,22 +1030,27 @@ __device__ __forceinline__ void rescaleNeq(R* neq, const CouplingArgs& c, bool t
 template <typename S, typename R>
 __device__ __forceinline__ void c2fSaveBody(const S* __restrict__ Ac, const C2FDev* __restrict__ nodes, int count, R* pre,
                                             const LevelArgs<S>& la, const CouplingArgs& c, int bx) {
-    const int t = bx * blockDim.x + threadIdx.x;
+    // one thread per node, or (partner strain kept) eight: the first saves the
+    // populations, the first six one coarse neighbour's moments each
+    const int tpn = coincidentThreadsPerNode(c);
+    const int tg = bx * blockDim.x + threadIdx.x;
+    const int t = tg / tpn, sub = tg - t * tpn;
     if (t >= count) return;
-    const int src = nodes[t].src;
+    if (sub == 0) {
+        const int src = nodes[t].src;
 #pragma unroll
-    for (int q = 0; q < Q; ++q) pre[(long long)q * count + t] = R(Store<S>::load(Ac + (long long)q * la.N + src, la.hscale[q]));
-    if (c.partner) {
+        for (int q = 0; q < Q; ++q)
+            pre[(long long)q * count + t] = R(Store<S>::load(Ac + (long long)q * la.N + src, la.hscale[q]));
+    }
+    if (c.partner && sub < 6) {
         R* pn = (R*)c.preNb;
-        for (int d = 0; d < 6; ++d) {
-            const int m = c.nb[t].c[d];
-            if (m < 0) continue;
-            const MomR<R> mo = nodeMomentsAt<S, R>(Ac, la.N, la, m);
-            pn[(long long)(d * 4 + 0) * count + t] = mo.drho;
-            pn[(long long)(d * 4 + 1) * count + t] = mo.ux;
-            pn[(long long)(d * 4 + 2) * count + t] = mo.uy;
-            pn[(long long)(d * 4 + 3) * count + t] = mo.uz;
-        }
+        const int m = c.nb[t].c[sub];
+        if (m < 0) return;
+        const MomR<R> mo = nodeMomentsAt<S, R>(Ac, la.N, la, m);
+        pn[(long long)(sub * 4 + 0) * count + t] = mo.drho;
+        pn[(long long)(sub * 4 + 1) * count + t] = mo.ux;
+        pn[(long long)(sub * 4 + 2) * count + t] = mo.uy;
+        pn[(long long)(sub * 4 + 3) * count + t] = mo.uz;
     }
 }
 template <typename S, typename R>
