@@ -51,11 +51,27 @@ __host__ __device__ constexpr R h2yy(int q) { return R(ey(q) * ey(q)) - R(1) / R
 template <typename R>
 __host__ __device__ constexpr R h2zz(int q) { return R(ez(q) * ez(q)) - R(1) / R(3); }
 
+// s += c * x for a coefficient c that is a constant once the direction loops
+// are unrolled; zero coefficients drop the term.  Sums start from -0, the
+// additive identity of IEEE arithmetic, so the first term is not added to a
+// zero: leaving the zero terms out changes no result, while 0 * x cannot be
+// folded away by the compiler (x may be infinite or NaN).
+template <typename R>
+__device__ __forceinline__ void acc(R& s, R c, R x) {
+    if (c != R(0)) s += c * x;
+}
+
 // H2 : A for a symmetric tensor A = {xx, yy, zz, xy, xz, yz}
 template <typename R>
 __device__ __forceinline__ R h2dot(int q, const R* A) {
-    return h2xx<R>(q) * A[0] + h2yy<R>(q) * A[1] + h2zz<R>(q) * A[2] +
-           R(2) * (R(ex(q) * ey(q)) * A[3] + R(ex(q) * ez(q)) * A[4] + R(ey(q) * ez(q)) * A[5]);
+    R d = R(-0.0), o = R(-0.0);
+    acc(d, h2xx<R>(q), A[0]);
+    acc(d, h2yy<R>(q), A[1]);
+    acc(d, h2zz<R>(q), A[2]);
+    acc(o, R(ex(q) * ey(q)), A[3]);
+    acc(o, R(ex(q) * ez(q)), A[4]);
+    acc(o, R(ey(q) * ez(q)), A[5]);
+    return d + R(2) * o;
 }
 
 // sum of the six orthogonal third-order Hermite terms, weighted as the
@@ -67,8 +83,25 @@ __device__ __forceinline__ R h3dot(int q, const R* a) {
     const R hx = R(ex(q)), hy = R(ey(q)), hz = R(ez(q));
     const R xxy = h2xx<R>(q) * hy, xyy = h2yy<R>(q) * hx, xxz = h2xx<R>(q) * hz;
     const R xzz = h2zz<R>(q) * hx, yyz = h2yy<R>(q) * hz, yzz = h2zz<R>(q) * hy;
-    return R(3) * ((xxy + yzz) * a[0] + (xxz + yyz) * a[1] + (xyy + xzz) * a[2]) + (yzz - xxy) * a[3] +
-           (yyz - xxz) * a[4] + (xzz - xyy) * a[5];
+    R sym = R(-0.0);
+    acc(sym, xxy + yzz, a[0]);
+    acc(sym, xxz + yyz, a[1]);
+    acc(sym, xyy + xzz, a[2]);
+    R t = R(3) * sym;
+    acc(t, yzz - xxy, a[3]);
+    acc(t, yyz - xxz, a[4]);
+    acc(t, xzz - xyy, a[5]);
+    return t;
+}
+
+// e_q . v
+template <typename R>
+__device__ __forceinline__ R edot(int q, const R* v) {
+    R t = R(-0.0);
+    acc(t, R(ex(q)), v[0]);
+    acc(t, R(ey(q)), v[1]);
+    acc(t, R(ez(q)), v[2]);
+    return t;
 }
 
 // fully orthogonalised fourth-order combination (Node.cpp:1082-1094, 1130):
@@ -84,7 +117,11 @@ __device__ __forceinline__ R h4dot(int q, const R* a4, R kappa) {
     R h[3];
     orth4<R>(h2xx<R>(q) * h2yy<R>(q), h2xx<R>(q) * h2zz<R>(q), h2yy<R>(q) * h2zz<R>(q), h2xx<R>(q), h2yy<R>(q),
              h2zz<R>(q), kappa, h);
-    return R(8.0 / 7.0) * h[0] * a4[0] + R(56.0 / 45.0) * h[1] * a4[1] + R(40.0 / 27.0) * h[2] * a4[2];
+    R t = R(-0.0);
+    acc(t, R(8.0 / 7.0) * h[0], a4[0]);
+    acc(t, R(56.0 / 45.0) * h[1], a4[1]);
+    acc(t, R(40.0 / 27.0) * h[2], a4[2]);
+    return t;
 }
 
 // Velocity coefficients of the Hermite equilibrium up to `ORDER`.
@@ -108,8 +145,7 @@ struct EqCoef {
     }
     // feq_q / (rho w_q) - 1
     __device__ __forceinline__ R poly(int q, R kappa) const {
-        R eu = R(ex(q)) * u[0] + R(ey(q)) * u[1] + R(ez(q)) * u[2];
-        R p = R(3) * eu + R(4.5) * h2dot<R>(q, uu);
+        R p = R(3) * edot<R>(q, u) + R(4.5) * h2dot<R>(q, uu);
         if (ORDER >= 3) p += R(4.5) * h3dot<R>(q, a3);
         if (ORDER == 4) p += R(20.25) * h4dot<R>(q, a4, kappa);
         return p;
@@ -118,7 +154,7 @@ struct EqCoef {
     // odd (first and third order) parts: direction q gives even + odd, its
     // opposite even - odd
     __device__ __forceinline__ void evenOdd(int q, R kappa, R& even, R& odd) const {
-        odd = R(3) * (R(ex(q)) * u[0] + R(ey(q)) * u[1] + R(ez(q)) * u[2]);
+        odd = R(3) * edot<R>(q, u);
         if (ORDER >= 3) odd += R(4.5) * h3dot<R>(q, a3);
         even = R(4.5) * h2dot<R>(q, uu);
         if (ORDER == 4) even += R(20.25) * h4dot<R>(q, a4, kappa);
@@ -297,8 +333,10 @@ struct Store<float> {
 template <>
 struct Store<__half> {
     __device__ __forceinline__ static float load(const __half* p, float scale) { return __half2float(*p) * scale; }
+    // the scales are powers of two: their correctly rounded reciprocal is
+    // exact, so the multiply equals the division v / scale
     __device__ __forceinline__ static void store(__half* p, float v, float scale) {
-        *p = __float2half_rn(v * (1.0f / scale));
+        *p = __float2half_rn(v * __frcp_rn(scale));
     }
 };
 

@@ -740,7 +740,7 @@ int enqueueLevelStep(acp_handle* h, int l, int src, PhaseTimer* tm = nullptr, cu
     const int bx = 128;
     if (tm) tm->mark(-1);
     if (needsMoments(h->d)) {
-        const int chunk = tiledChunk(L);
+        const int chunk = tiledChunkFor(L, TiledMinBlocks<R>::value);
         dim3 grid((L.nx + TX - 1) / TX, (L.ny + TY - 1) / TY, (L.nz + chunk - 1) / chunk);
         pickTiled<S, R>(h->d)<<<grid, dim3(TX, TY), 0, st>>>(a, chunk);
     } else {
@@ -1281,29 +1281,32 @@ int acp_write_populations(acp_handle* h, int level, const double* in) {
 
 int acp_read_field(acp_handle* h, int level, int field, double* out) {
     if (!h || !out || level < 0 || level >= (int)h->host.size() || field < 0 || field > 4) return ACP_ERR_INVALID;
+    CU(h, cudaSetDevice(h->device));
+    joinBatch(h);
     const LevelHost& L = h->host[level];
-    std::vector<double> f((size_t)L.N * Q);
-    int s = acp_read_populations(h, level, f.data());
-    if (s) return s;
-    for (long long n = 0; n < L.N; ++n) {
-        double rho = 0, jx = 0, jy = 0, jz = 0;
-        for (int q = 0; q < Q; ++q) {
-            const double v = f[(size_t)q * L.N + n];
-            rho += v;
-            jx += ex(q) * v;
-            jy += ey(q) * v;
-            jz += ez(q) * v;
-        }
-        double r;
-        switch (field) {
-            case ACP_FIELD_RHO: r = rho; break;
-            case ACP_FIELD_UX: r = h->c * jx / rho; break;
-            case ACP_FIELD_UY: r = h->c * jy / rho; break;
-            case ACP_FIELD_UZ: r = h->c * jz / rho; break;
-            default: r = rho * h->d.speed_of_sound * h->d.speed_of_sound; break;
-        }
-        out[n] = r;
+    const int arr = level == 0 ? h->cur : 0;
+    double* tmp = nullptr;
+    CU(h, cudaMallocAsync((void**)&tmp, (size_t)L.N * sizeof(double), h->stream));
+    const unsigned grid = (unsigned)((L.N + 255) / 256);
+    const double cs = h->d.speed_of_sound;
+    switch (h->d.storage) {
+        case ACP_STORE_F64:
+            k_field<double><<<grid, 256, 0, h->stream>>>((const double*)h->dev[level].f[arr], tmp, L.N, h->shift, h->c,
+                                                          cs, field, levelArgs<double>(h, level, 0));
+            break;
+        case ACP_STORE_F32_DEV:
+            k_field<float><<<grid, 256, 0, h->stream>>>((const float*)h->dev[level].f[arr], tmp, L.N, h->shift, h->c,
+                                                         cs, field, levelArgs<float>(h, level, 0));
+            break;
+        default:
+            k_field<__half><<<grid, 256, 0, h->stream>>>((const __half*)h->dev[level].f[arr], tmp, L.N, h->shift, h->c,
+                                                          cs, field, levelArgs<__half>(h, level, 0));
+            break;
     }
+    cudaError_t e = cudaMemcpyAsync(out, tmp, (size_t)L.N * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+    cudaFreeAsync(tmp, h->stream);
+    if (e != cudaSuccess) return fail(h, ACP_ERR_CUDA, "copy: %s", cudaGetErrorString(e));
+    CU(h, cudaStreamSynchronize(h->stream));
     return ACP_OK;
 }
 

@@ -125,7 +125,7 @@ struct RT<float> {
 // signed products (off-diagonal)
 template <typename R>
 __device__ __forceinline__ void secondSums(const R* g, R* s2) {
-    R sxx = 0, syy = 0, szz = 0, sxy = 0, sxz = 0, syz = 0;
+    R sxx = R(-0.0), syy = R(-0.0), szz = R(-0.0), sxy = R(-0.0), sxz = R(-0.0), syz = R(-0.0);
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
         if (ex(q)) sxx += g[q];
@@ -136,6 +136,40 @@ __device__ __forceinline__ void secondSums(const R* g, R* s2) {
         if (ey(q) * ez(q)) syz += R(ey(q) * ez(q)) * g[q];
     }
     s2[0] = sxx; s2[1] = syy; s2[2] = szz; s2[3] = sxy; s2[4] = sxz; s2[5] = syz;
+}
+
+// drho, momentum j and the six second-order sums of a node's 19 deviations,
+// summed per pair of opposite directions: g_a + g_b carries the even
+// moments (drho, second order), g_a - g_b the odd ones (momentum)
+template <typename R>
+__device__ __forceinline__ void pairMoments(const R* g, R& drho, R* j, R* s2) {
+    R sp[9], dp[9];
+#pragma unroll
+    for (int p = 0; p < 9; ++p) {
+        sp[p] = g[pairA(p)] + g[pairB(p)];
+        dp[p] = g[pairA(p)] - g[pairB(p)];
+    }
+    const R z0 = R(-0.0);  // additive identity: the first term is not added to a zero
+    R d = g[18], jx = z0, jy = z0, jz = z0, sxx = z0, syy = z0, szz = z0, sxy = z0, sxz = z0, syz = z0;
+#pragma unroll
+    for (int p = 0; p < 9; ++p) {
+        const int q = pairA(p);
+        d += sp[p];
+        if (ex(q)) jx += R(ex(q)) * dp[p];
+        if (ey(q)) jy += R(ey(q)) * dp[p];
+        if (ez(q)) jz += R(ez(q)) * dp[p];
+        if (ex(q)) sxx += sp[p];
+        if (ey(q)) syy += sp[p];
+        if (ez(q)) szz += sp[p];
+        if (ex(q) * ey(q)) sxy += R(ex(q) * ey(q)) * sp[p];
+        if (ex(q) * ez(q)) sxz += R(ex(q) * ez(q)) * sp[p];
+        if (ey(q) * ez(q)) syz += R(ey(q) * ez(q)) * sp[p];
+    }
+    drho = d;
+    j[0] = jx; j[1] = jy; j[2] = jz;
+    if (s2) {
+        s2[0] = sxx; s2[1] = syy; s2[2] = szz; s2[3] = sxy; s2[4] = sxz; s2[5] = syz;
+    }
 }
 
 // Regularised collision (RR, Node.cpp:560-650; HRR, Node.cpp:653-736) of one
@@ -232,14 +266,9 @@ struct Collider {
             for (int q = 0; q < Q; ++q) emit(q, g[q]);
             return;
         }
-        R drho = 0, jx = 0, jy = 0, jz = 0;
-#pragma unroll
-        for (int q = 0; q < Q; ++q) {
-            drho += g[q];
-            jx += R(ex(q)) * g[q];
-            jy += R(ey(q)) * g[q];
-            jz += R(ez(q)) * g[q];
-        }
+        R drho, jj[3];
+        pairMoments<R>(g, drho, jj, (R*)nullptr);
+        const R jx = jj[0], jy = jj[1], jz = jj[2];
         const R rho = R(a.shift) + drho;
         const R inv = rcpRN(rho);
         R u[3] = {jx * inv, jy * inv, jz * inv};
@@ -428,21 +457,17 @@ constexpr int TX = 32, TY = ACP_TILE_Y;
 // drho, jx, jy, jz of a node's deviations
 template <typename S, typename R>
 __device__ __forceinline__ MomR<R> nodeMoments(const LevelArgs<S>& a, int n) {
-    R d = 0, jx = 0, jy = 0, jz = 0;
+    R g[Q];
 #pragma unroll
-    for (int q = 0; q < Q; ++q) {
-        const R g = R(Store<S>::load(a.A + (q * a.Ni + n), scaleOf(a, q)));
-        d += g;
-        jx += R(ex(q)) * g;
-        jy += R(ey(q)) * g;
-        jz += R(ez(q)) * g;
-    }
+    for (int q = 0; q < Q; ++q) g[q] = R(Store<S>::load(a.A + (q * a.Ni + n), scaleOf(a, q)));
+    R d, jj[3];
+    pairMoments<R>(g, d, jj, (R*)nullptr);
     MomR<R> m;
     m.drho = d;
     const R inv = rcpRN(R(a.shift) + d);
-    m.ux = jx * inv;
-    m.uy = jy * inv;
-    m.uz = jz * inv;
+    m.ux = jj[0] * inv;
+    m.uy = jj[1] * inv;
+    m.uz = jj[2] * inv;
     return m;
 }
 
@@ -461,21 +486,14 @@ __device__ __forceinline__ void planePass(const LevelArgs<S>& a, MomR<R> (*slot)
                 R g[Q];
 #pragma unroll
                 for (int q = 0; q < Q; ++q) g[q] = R(Store<S>::load(a.A + (q * a.Ni + n), scaleOf(a, q)));
-                R d = 0, jx = 0, jy = 0, jz = 0;
-#pragma unroll
-                for (int q = 0; q < Q; ++q) {
-                    d += g[q];
-                    jx += R(ex(q)) * g[q];
-                    jy += R(ey(q)) * g[q];
-                    jz += R(ez(q)) * g[q];
-                }
-                secondSums<R>(g, s2);
+                R d, jj[3];
+                pairMoments<R>(g, d, jj, s2);
                 MomR<R> m;
                 m.drho = d;
                 const R inv = rcpRN(R(a.shift) + d);
-                m.ux = jx * inv;
-                m.uy = jy * inv;
-                m.uz = jz * inv;
+                m.ux = jj[0] * inv;
+                m.uy = jj[1] * inv;
+                m.uz = jj[2] * inv;
                 slot[ty + 1][tx + 1] = m;
             }
         }
@@ -558,27 +576,16 @@ struct TiledMinBlocks {
     static constexpr int value = sizeof(R) == 8 ? ACP_TILED_MINB_F64 : ACP_TILED_MINB_F32;
 };
 
-// collide + push of the thread's node of plane z: slots sc / sp / sn hold the
-// moments of planes z, z+1, z-1; s2 the node's second-order sums (null: form
-// them from the populations again)
+// collide + push of node n = (i, j, z) of class `code` from its own moments
+// `me`, its six axis neighbours' moments (+x, -x, +y, -y, +z, -z) and its
+// second-order sums s2
 template <typename S, typename R, int OP, int ORDER, bool CUBIC>
-__device__ __forceinline__ void tiledNode(const LevelArgs<S>& a, MomR<R> (*sm)[TY + 2][TX + 2], int i, int j, int z,
-                                          int sc, int sp, int sn, const R* s2own) {
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    const int n = (z * a.ny + j) * a.nx + i;
-    const uint8_t code = a.code[n];
+__device__ __forceinline__ void tiledCollide(const LevelArgs<S>& a, int n, int i, int j, int z, uint8_t code,
+                                             const MomR<R>& me, const MomR<R>& xp, const MomR<R>& xm,
+                                             const MomR<R>& yp, const MomR<R>& ym, const MomR<R>& zp,
+                                             const MomR<R>& zm, const R* s2) {
     if (code == CODE_DEAD) return;
     if (collides(code)) {
-        R s2buf[6];
-        const R* s2 = s2own;
-        if (!s2) {
-            R g[Q];
-#pragma unroll
-            for (int q = 0; q < Q; ++q) g[q] = R(Store<S>::load(a.A + (q * a.Ni + n), scaleOf(a, q)));
-            secondSums<R>(g, s2buf);
-            s2 = s2buf;
-        }
-        const MomR<R> me = sm[sc][ty + 1][tx + 1];
         const R u[3] = {me.ux, me.uy, me.uz};
         if (code >= CODE_IFACE0) {
             // coupling node: partner strain from the other level when kept, else Pi1 alone
@@ -595,9 +602,7 @@ __device__ __forceinline__ void tiledNode(const LevelArgs<S>& a, MomR<R> (*sm)[T
         } else {
             // fluid nodes are interior or on periodic axes: every axis neighbour exists
             R SG[12];
-            neighbourTerms<R, OP == OP_HRR, CUBIC>(sm[sc][ty + 1][tx + 2], sm[sc][ty + 1][tx], sm[sc][ty + 2][tx + 1],
-                                                   sm[sc][ty][tx + 1], sm[sp][ty + 1][tx + 1], sm[sn][ty + 1][tx + 1],
-                                                   R(a.shift), SG);
+            neighbourTerms<R, OP == OP_HRR, CUBIC>(xp, xm, yp, ym, zp, zm, R(a.shift), SG);
             Pusher<S> emit{a, n, 0x3FFFFu, nbOffsets(a, i, j, z)};
             regularisedEmit<R, OP, ORDER, CUBIC>(me.drho, u, s2, a, SG, emit);
         }
@@ -607,6 +612,30 @@ __device__ __forceinline__ void tiledNode(const LevelArgs<S>& a, MomR<R> (*sm)[T
 #pragma unroll
         for (int q = 0; q < Q; ++q) emit(q, R(Store<S>::load(a.A + (q * a.Ni + n), scaleOf(a, q))));
     }
+}
+
+// collide + push of the thread's node of plane z: slots sc / sp / sn hold the
+// moments of planes z, z+1, z-1; s2 the node's second-order sums (null: form
+// them from the populations again)
+template <typename S, typename R, int OP, int ORDER, bool CUBIC>
+__device__ __forceinline__ void tiledNode(const LevelArgs<S>& a, MomR<R> (*sm)[TY + 2][TX + 2], int i, int j, int z,
+                                          int sc, int sp, int sn, const R* s2own) {
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int n = (z * a.ny + j) * a.nx + i;
+    const uint8_t code = a.code[n];
+    if (code == CODE_DEAD) return;
+    R s2buf[6];
+    const R* s2 = s2own;
+    if (!s2 && collides(code)) {
+        R g[Q];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) g[q] = R(Store<S>::load(a.A + (q * a.Ni + n), scaleOf(a, q)));
+        secondSums<R>(g, s2buf);
+        s2 = s2buf;
+    }
+    tiledCollide<S, R, OP, ORDER, CUBIC>(a, n, i, j, z, code, sm[sc][ty + 1][tx + 1], sm[sc][ty + 1][tx + 2],
+                                         sm[sc][ty + 1][tx], sm[sc][ty + 2][tx + 1], sm[sc][ty][tx + 1],
+                                         sm[sp][ty + 1][tx + 1], sm[sn][ty + 1][tx + 1], s2);
 }
 
 // plane slots of the tiled kernel: four rolling ones (the pass over plane
@@ -869,6 +898,34 @@ __global__ void k_to_f64(const S* __restrict__ src, double* dst, long long N, do
     const int q = (int)(t / N);
     dst[t] = (double)Store<S>::load(src + t, la.hscale[q]) + wq(q) * shift;
 }
+// one macroscopic field per node from the stored populations, in FP64 with
+// the arithmetic and summation order of the host read-back (absolute
+// populations as k_to_f64 forms them, summed over q = 0..18): field 0 rho,
+// 1-3 velocity (c * j / rho), 4 pressure (rho * cs^2)
+template <typename S>
+__global__ void k_field(const S* __restrict__ src, double* dst, long long N, double shift, double c, double cs,
+                        int field, LevelArgs<S> la) {
+    const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    double rho = 0, jx = 0, jy = 0, jz = 0;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const double v = (double)Store<S>::load(src + q * N + n, la.hscale[q]) + wq(q) * shift;
+        rho += v;
+        jx += ex(q) * v;
+        jy += ey(q) * v;
+        jz += ez(q) * v;
+    }
+    double r;
+    switch (field) {
+        case 0: r = rho; break;
+        case 1: r = c * jx / rho; break;
+        case 2: r = c * jy / rho; break;
+        case 3: r = c * jz / rho; break;
+        default: r = rho * cs * cs; break;
+    }
+    dst[n] = r;
+}
 // storage -> absolute FP64 populations of the node window [begin, begin+count)
 template <typename S>
 __global__ void k_to_f64_window(const S* __restrict__ src, double* dst, long long N, long long begin, int count,
@@ -963,38 +1020,28 @@ __host__ __device__ inline int coincidentThreadsPerNode(const CouplingArgs& c) {
 // drho and lattice velocity of node n of an arbitrary array of a level
 template <typename S, typename R>
 __device__ __forceinline__ MomR<R> nodeMomentsAt(const S* arr, long long N, const LevelArgs<S>& la, long long n) {
-    R d = 0, jx = 0, jy = 0, jz = 0;
+    R g[Q];
 #pragma unroll
-    for (int q = 0; q < Q; ++q) {
-        const R g = R(Store<S>::load(arr + (long long)q * N + n, la.hscale[q]));
-        d += g;
-        jx += R(ex(q)) * g;
-        jy += R(ey(q)) * g;
-        jz += R(ez(q)) * g;
-    }
+    for (int q = 0; q < Q; ++q) g[q] = R(Store<S>::load(arr + (long long)q * N + n, la.hscale[q]));
+    R d, jj[3];
+    pairMoments<R>(g, d, jj, (R*)nullptr);
     MomR<R> m;
     m.drho = d;
     const R inv = rcpRN(R(la.shift) + d);
-    m.ux = jx * inv;
-    m.uy = jy * inv;
-    m.uz = jz * inv;
+    m.ux = jj[0] * inv;
+    m.uy = jj[1] * inv;
+    m.uz = jj[2] * inv;
     return m;
 }
 
 // equilibrium split of one node's populations (deviation form)
 template <typename R, int ORDER>
 __device__ __forceinline__ void eqSplit(const R* g, R shift, R kappa, R* geq) {
-    R drho = 0, jx = 0, jy = 0, jz = 0;
-#pragma unroll
-    for (int q = 0; q < Q; ++q) {
-        drho += g[q];
-        jx += R(ex(q)) * g[q];
-        jy += R(ey(q)) * g[q];
-        jz += R(ez(q)) * g[q];
-    }
+    R drho, jj[3];
+    pairMoments<R>(g, drho, jj, (R*)nullptr);
     const R rho = shift + drho;
     const R inv = rcpRN(rho);
-    R u[3] = {jx * inv, jy * inv, jz * inv};
+    R u[3] = {jj[0] * inv, jj[1] * inv, jj[2] * inv};
     EqCoef<R, ORDER> ec;
     ec.set(u, kappa);
 #pragma unroll
