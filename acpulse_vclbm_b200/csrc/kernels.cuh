@@ -204,7 +204,7 @@ __device__ __forceinline__ void regularisedEmit(R drho, const R* u, const R* s2,
     R P[6];
     {
         const R sxx = s2[0], syy = s2[1], szz = s2[2], sxy = s2[3], sxz = s2[4], syz = s2[5];
-        const R third = drho / R(3);
+        const R third = drho * R(1.0 / 3.0);  // within an ulp of drho / 3, without a division per node
         P[0] = sxx - third - rho * ec.uu[0];
         P[1] = syy - third - rho * ec.uu[1];
         P[2] = szz - third - rho * ec.uu[2];
@@ -225,7 +225,7 @@ __device__ __forceinline__ void regularisedEmit(R drho, const R* u, const R* s2,
     R A2[6];
     if (OP == OP_HRR) {
         const R sg = nb ? R(a.sigma) : R(1);
-        const R fd = (R(1) - sg) * (R(-2) * rho / (R(3) * omega));
+        const R fd = (R(1) - sg) * (rho * (R(-2) / (R(3) * omega)));  // the quotient is the same for every node
 #pragma unroll
         for (int c = 0; c < 6; ++c) A2[c] = sg * P[c] + fd * S[c];
     } else {
