@@ -14,6 +14,7 @@
 #include <cstring>
 #include <algorithm>
 #include <mutex>
+#include <thread>
 #include <string>
 #include <vector>
 
@@ -198,6 +199,40 @@ int validate(const acp_case_desc* d, std::string& why) {
     return ACP_OK;
 }
 
+// The node scans of the set-up run over the host's cores: rows (j, k) of a
+// level split into contiguous ranges, one per thread, so that per-thread
+// results concatenated in thread order are in node order.
+template <typename F>
+void forRows(long long rows, F&& fn) {
+    const int T = std::max(1, std::min(16, (int)std::thread::hardware_concurrency()));
+    if (rows < 256 || T == 1) {
+        fn(0LL, rows, 0);
+        return;
+    }
+    std::vector<std::thread> pool;
+    for (int t = 0; t < T; ++t) pool.emplace_back([&fn, rows, t, T] { fn(rows * t / T, rows * (t + 1) / T, t); });
+    for (std::thread& th : pool) th.join();
+}
+
+// indices, in increasing order, of the nodes (i, j, k) of L for which pred(n, i, j, k) holds
+template <typename P>
+std::vector<long long> scanNodes(const LevelHost& L, P pred) {
+    const int T = std::max(1, std::min(16, (int)std::thread::hardware_concurrency()));
+    std::vector<std::vector<long long>> part(T);
+    forRows((long long)L.ny * L.nz, [&](long long r0, long long r1, int t) {
+        for (long long r = r0; r < r1; ++r) {
+            const int j = (int)(r % L.ny), k = (int)(r / L.ny);
+            for (int i = 0; i < L.nx; ++i) {
+                const long long n = r * L.nx + i;
+                if (pred(n, i, j, k)) part[t].push_back(n);
+            }
+        }
+    });
+    std::vector<long long> out;
+    for (auto& v : part) out.insert(out.end(), v.begin(), v.end());
+    return out;
+}
+
 // LODI wiring and node classes of a level whose dead / coupling nodes are
 // marked in L.code (CODE_DEAD, CODE_IFACE0 + class); the LODI faces are the
 // domain faces the level's box reaches
@@ -222,15 +257,19 @@ int wireLevel(acp_handle* h, LevelHost& L, int level) {
         out = idx(c[0], c[1], c[2]);
         return true;
     };
-    for (int k = 0; k < L.nz; ++k)
-        for (int j = 0; j < L.ny; ++j)
-            for (int i = 0; i < L.nx; ++i) {
-                const long long n = idx(i, j, k);
-                if (L.code[n] == CODE_DEAD) continue;
-                const int c[3] = {i, j, k};
+    auto faceOf = [&](int i, int j, int k, int* fc) {
+        const int c[3] = {i, j, k};
+        for (int a = 0; a < 3; ++a) fc[a] = (lodiLo[a] && c[a] == 0) ? -1 : ((lodiHi[a] && c[a] == dims[a] - 1) ? 1 : 0);
+        return fc[0] || fc[1] || fc[2];
+    };
+    const std::vector<long long> faceNodes = scanNodes(L, [&](long long n, int i, int j, int k) {
+        int fc[3];
+        return L.code[n] != CODE_DEAD && faceOf(i, j, k, fc);
+    });
+    for (const long long n : faceNodes) {
+                const int i = (int)(n % L.nx), j = (int)((n / L.nx) % L.ny), k = (int)(n / ((long long)L.nx * L.ny));
                 int fc[3];
-                for (int a = 0; a < 3; ++a) fc[a] = (lodiLo[a] && c[a] == 0) ? -1 : ((lodiHi[a] && c[a] == dims[a] - 1) ? 1 : 0);
-                if (!fc[0] && !fc[1] && !fc[2]) continue;
+                faceOf(i, j, k, fc);
                 if (L.code[n] != CODE_FLUID) return fail(h, ACP_ERR_INVALID, "a coupling node on a LODI face");
                 L.code[n] = (uint8_t)faceCode(fc[0], fc[1], fc[2]);
                 const BoundaryClass* bc = boundaryClass(fc[0], fc[1], fc[2]);
@@ -252,8 +291,14 @@ int wireLevel(acp_handle* h, LevelHost& L, int level) {
                 }
                 (fc[0] != 0 ? L.lodiX : L.lodiZY).push_back(b);
             }
+    std::vector<long long> live(16, 0);
+    forRows((long long)L.ny * L.nz, [&](long long r0, long long r1, int t) {
+        long long c = 0;
+        for (long long n = r0 * L.nx; n < r1 * L.nx; ++n) c += L.code[n] != CODE_DEAD;
+        live[t] = c;
+    });
     L.active = 0;
-    for (long long n = 0; n < L.N; ++n) L.active += L.code[n] != CODE_DEAD;
+    for (long long c : live) L.active += c;
     L.spacing = d.spacing / std::pow(2.0, (double)level);
     L.dt = d.spacing / (d.speed_of_sound * std::sqrt(3.0)) / std::pow(2.0, (double)level);
     const double cs2 = d.speed_of_sound * d.speed_of_sound;
@@ -316,11 +361,11 @@ struct CouplingGeom {
 // covered nodes exist in the array, else only within the level)
 void markLevel(LevelHost& L, const CouplingGeom& g) {
     L.code.assign(L.N, CODE_FLUID);
-    for (int k = 0; k < L.nz; ++k)
-        for (int j = 0; j < L.ny; ++j)
+    forRows((long long)L.ny * L.nz, [&](long long r0, long long r1, int) {
+        for (long long r = r0; r < r1; ++r)
             for (int i = 0; i < L.nx; ++i) {
-                const int c[3] = {i, j, k};
-                const long long n = ((long long)k * L.ny + j) * L.nx + i;
+                const int c[3] = {i, (int)(r % L.ny), (int)(r / L.ny)};
+                const long long n = r * L.nx + i;
                 if (g.dead(c)) {
                     L.code[n] = CODE_DEAD;
                 } else if (g.coupling(c)) {
@@ -329,6 +374,7 @@ void markLevel(LevelHost& L, const CouplingGeom& g) {
                     L.code[n] = (uint8_t)(CODE_IFACE0 + (g.inside ? faceCode(f[0], f[1], f[2]) : CODE_FLUID));
                 }
             }
+    });
 }
 
 // Two levels.  Box layout: the fine level covers the box [box_lo, box_hi]
@@ -392,7 +438,6 @@ int buildTwoLevel(acp_handle* h) {
     F.N = (long long)F.nx * F.ny * F.nz;
     markLevel(F, gf);
     if ((s = wireLevel(h, F, 1))) return s;
-    auto fidx = [&](int i, int j, int k) { return ((long long)k * F.ny + j) * F.nx + i; };
     // coupling lists; nodes addressed by their level-global indices
     auto local = [](const LevelHost& L, const int* g, long long& out) {
         int c[3];
@@ -412,12 +457,11 @@ int buildTwoLevel(acp_handle* h) {
         return true;
     };
     std::vector<C2FDev> coinc, mid, cen;
-    for (int k = 0; k < F.nz; ++k)
-        for (int j = 0; j < F.ny; ++j)
-            for (int i = 0; i < F.nx; ++i) {
-                const long long n = fidx(i, j, k);
-                if (F.code[n] < CODE_IFACE0 || F.code[n] == CODE_DEAD) continue;
-                const int c[3] = {i, j, k};
+    auto isCoupling = [](const LevelHost& L) {
+        return [&L](long long n, int, int, int) { return L.code[n] >= CODE_IFACE0 && L.code[n] != CODE_DEAD; };
+    };
+    for (const long long n : scanNodes(F, isCoupling(F))) {
+                const int c[3] = {(int)(n % F.nx), (int)((n / F.nx) % F.ny), (int)(n / ((long long)F.nx * F.ny))};
                 int g[3], f[3], odd[3], nodd = 0;
                 gf.normal(c, f);
                 for (int a = 0; a < 3; ++a) {
@@ -535,12 +579,8 @@ int buildTwoLevel(acp_handle* h) {
             h->dcHost.push_back(dn);
         }
     }
-    for (int k = 0; k < C.nz && !direct; ++k)
-        for (int j = 0; j < C.ny; ++j)
-            for (int i = 0; i < C.nx; ++i) {
-                const long long n = ((long long)k * C.ny + j) * C.nx + i;
-                if (C.code[n] < CODE_IFACE0 || C.code[n] == CODE_DEAD) continue;
-                const int c[3] = {i, j, k};
+    for (const long long n : direct ? std::vector<long long>() : scanNodes(C, isCoupling(C))) {
+                const int c[3] = {(int)(n % C.nx), (int)((n / C.nx) % C.ny), (int)(n / ((long long)C.nx * C.ny))};
                 int g[3], f[3];
                 gc.normal(c, f);
                 for (int a = 0; a < 3; ++a) g[a] = 2 * (c[a] + C.off[a]);
