@@ -435,8 +435,8 @@ int buildGroup(acp_batch* b, Group& g) {
         phase(g.collide[l], [&](int c, const acp_handle* h) {
             collideItems(h->host[l], c, g.tiled, recs[c].lv[l].zChunk, items);
         });
-        phase(g.lodiX[l], [&](int c, const acp_handle* h) { blockItems(c, h->dev[l].nLodiX, 32, items); });
-        phase(g.lodiZY[l], [&](int c, const acp_handle* h) { blockItems(c, h->dev[l].nLodiZY, 32, items); });
+        phase(g.lodiX[l], [&](int c, const acp_handle* h) { blockItems(c, h->dev[l].nLodiX * LODI_TPN, 32, items); });
+        phase(g.lodiZY[l], [&](int c, const acp_handle* h) { blockItems(c, h->dev[l].nLodiZY * LODI_TPN, 32, items); });
     }
     if (g.levels == 2) {
         phase(g.save, [&](int c, const acp_handle* h) {

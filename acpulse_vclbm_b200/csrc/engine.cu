@@ -789,10 +789,10 @@ int enqueueLevelStep(acp_handle* h, int l, int src, PhaseTimer* tm = nullptr, cu
     if (tm) tm->mark(ACP_K_COLLIDE);
     const LodiArgs p = lodiArgsOf(h, l);
     LodiFn<S> lf = pickLodi<S>(h->d.eq_order);
-    // one thread per boundary node with long FP64 work: small blocks spread the few
-    // thousand nodes of a face over every SM
-    if (D.nLodiX) lf<<<(D.nLodiX + 31) / 32, 32, 0, st>>>(a.A, a.B, D.lodiX, D.nLodiX, p, a);
-    if (D.nLodiZY) lf<<<(D.nLodiZY + 31) / 32, 32, 0, st>>>(a.A, a.B, D.lodiZY, D.nLodiZY, p, a);
+    // eight lanes per boundary node (one per stencil member) and small blocks
+    // spread the few thousand nodes of a face over every SM
+    if (D.nLodiX) lf<<<(D.nLodiX * LODI_TPN + 63) / 64, 64, 0, st>>>(a.A, a.B, D.lodiX, D.nLodiX, p, a);
+    if (D.nLodiZY) lf<<<(D.nLodiZY * LODI_TPN + 63) / 64, 64, 0, st>>>(a.A, a.B, D.lodiZY, D.nLodiZY, p, a);
     if (tm && (D.nLodiX || D.nLodiZY)) tm->mark(ACP_K_LODI);
     return ACP_OK;
 }

@@ -752,9 +752,9 @@ __device__ __forceinline__ void absMoments(const S* arr, long long N, long long 
     for (int q = 0; q < Q; ++q) {
         const double g = (double)Store<S>::load(arr + q * N + n, hs[q]);
         d += g;
-        jx += ex(q) * g;
-        jy += ey(q) * g;
-        jz += ez(q) * g;
+        if (ex(q)) jx += ex(q) * g;
+        if (ey(q)) jy += ey(q) * g;
+        if (ez(q)) jz += ez(q) * g;
     }
     rho = shift + d;
     uSI[0] = c * jx / rho;
@@ -762,26 +762,51 @@ __device__ __forceinline__ void absMoments(const S* arr, long long N, long long 
     uSI[2] = c * jz / rho;
 }
 
+// threads per LODI boundary node: lane m of a node's group forms the moments
+// of its stencil member m (0 the node, 1-2 the normal neighbours, 3-6 the
+// tangent neighbours), lane 0 then the characteristic update
+constexpr int LODI_TPN = 8;
+
 template <typename S, int ORDER>
 __device__ __forceinline__ void lodiBody(const S* __restrict__ A, S* B, const BNodeDev* __restrict__ nodes, int count,
                                          const LodiArgs& p, const LevelArgs<S>& la, int bx) {
-    const int t = bx * blockDim.x + threadIdx.x;
-    if (t >= count) return;
-    const BNodeDev b = nodes[t];
+    const int tg = bx * blockDim.x + threadIdx.x;
+    const int t = tg / LODI_TPN, lane = tg % LODI_TPN;
+    const bool valid = t < count;
     const float* hs = la.hscale;
-    double densB, veloB[3];
-    absMoments(A, p.N, b.n, p.shift, hs, p.c, densB, veloB);
-    double dN, d2N, vN[3], v2N[3];
-    absMoments((const S*)B, p.N, b.n1, p.shift, hs, p.c, dN, vN);
-    absMoments((const S*)B, p.N, b.n2, p.shift, hs, p.c, d2N, v2N);
+    // every lane of the warp reaches the shuffles below
+    BNodeDev b;
+    double mr = 0, mu[3] = {0, 0, 0};
+    if (valid) {
+        b = nodes[t];
+        long long src = -1;
+        const S* arr = A;
+        if (lane == 0) src = b.n;
+        else if (lane == 1) { src = b.n1; arr = (const S*)B; }
+        else if (lane == 2) { src = b.n2; arr = (const S*)B; }
+        else if (lane < 7 && b.transverse) src = b.t[lane - 3];
+        if (src >= 0) absMoments(arr, p.N, src, p.shift, hs, p.c, mr, mu);
+    }
+    double sr[7], su[7][3];
+#pragma unroll
+    for (int m = 0; m < 7; ++m) {
+        sr[m] = __shfl_sync(0xffffffffu, mr, m, LODI_TPN);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) su[m][c] = __shfl_sync(0xffffffffu, mu[c], m, LODI_TPN);
+    }
+    if (!valid || lane != 0) return;
+    const double densB = sr[0], dN = sr[1], d2N = sr[2];
+    const double* veloB = su[0];
+    const double* vN = su[1];
+    const double* v2N = su[2];
     const double ls = p.localSpacing;
     double dG = (4. * dN - d2N - 3. * densB) / (-2. * ls);
     double vG[3];
     for (int c = 0; c < 3; ++c) vG[c] = (4. * vN[c] - v2N[c] - 3. * veloB[c]) / (-2. * ls);
     double dGT[2] = {0, 0}, vGT[2][3] = {{0, 0, 0}, {0, 0, 0}};
     if (b.transverse) {
-        double dT[4], vT[4][3];
-        for (int m = 0; m < 4; ++m) absMoments(A, p.N, b.t[m], p.shift, hs, p.c, dT[m], vT[m]);
+        const double* dT = sr + 3;
+        const double(*vT)[3] = su + 3;
         dGT[0] = (dT[0] - dT[1]) / (2. * ls);
         dGT[1] = (dT[2] - dT[3]) / (2. * ls);
         for (int c = 0; c < 3; ++c) {
