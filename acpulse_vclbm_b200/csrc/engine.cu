@@ -12,6 +12,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <utility>
 #include <algorithm>
 #include <mutex>
 #include <thread>
@@ -1316,6 +1317,117 @@ int acp_write_populations(acp_handle* h, int level, const double* in) {
     cudaFreeAsync(tmp, h->stream);
     if (e != cudaSuccess) return fail(h, ACP_ERR_CUDA, "copy: %s", cudaGetErrorString(e));
     CU(h, cudaStreamSynchronize(h->stream));
+    return ACP_OK;
+}
+
+namespace {
+// checkpoint file: header, then per level both population arrays (storage
+// bytes) and the partner-strain records
+struct CheckpointHeader {
+    char magic[8];
+    int abi, storage, levels, cur;
+    long long steps;
+    long long dims[2][3];
+    long long slots[2];
+};
+constexpr char kCheckpointMagic[8] = {'A', 'C', 'P', 'C', 'K', 'P', 'T', '1'};
+
+CheckpointHeader checkpointHeader(const acp_handle* h) {
+    CheckpointHeader c;
+    std::memset(&c, 0, sizeof c);
+    std::memcpy(c.magic, kCheckpointMagic, sizeof c.magic);
+    c.abi = ACP_ABI_VERSION;
+    c.storage = h->d.storage;
+    c.levels = (int)h->host.size();
+    c.cur = h->cur;
+    c.steps = h->steps;
+    for (size_t l = 0; l < h->host.size() && l < 2; ++l) {
+        c.dims[l][0] = h->host[l].nx;
+        c.dims[l][1] = h->host[l].ny;
+        c.dims[l][2] = h->host[l].nz;
+        c.slots[l] = h->dev[l].sg ? h->host[l].nSlots : 0;
+    }
+    return c;
+}
+
+// device regions of the state, in file order
+std::vector<std::pair<void*, size_t>> checkpointRegions(acp_handle* h) {
+    std::vector<std::pair<void*, size_t>> r;
+    const size_t sb = storageBytes(h->d.storage);
+    for (size_t l = 0; l < h->host.size(); ++l) {
+        for (int a = 0; a < 2; ++a) r.push_back({h->dev[l].f[a], (size_t)h->host[l].N * Q * sb});
+        if (h->dev[l].sg) r.push_back({h->dev[l].sg, std::max<size_t>(1, (size_t)h->host[l].nSlots) * 12 * sizeof(double)});
+    }
+    return r;
+}
+constexpr size_t kCheckpointChunk = 64u << 20;  // host staging per copy
+}  // namespace
+
+int acp_checkpoint_save(acp_handle* h, const char* path) {
+    if (!h || !path) return ACP_ERR_INVALID;
+    if (!h->inited) return fail(h, ACP_ERR_STATE, "checkpoint before acp_init");
+    if (h->batch) return fail(h, ACP_ERR_STATE, "the case belongs to a batch");
+    CU(h, cudaSetDevice(h->device));
+    CU(h, cudaStreamSynchronize(h->stream));
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return fail(h, ACP_ERR_INVALID, "cannot write %s", path);
+    const CheckpointHeader hd = checkpointHeader(h);
+    bool ok = std::fwrite(&hd, sizeof hd, 1, f) == 1;
+    std::vector<char> buf;
+    for (const auto& reg : checkpointRegions(h)) {
+        for (size_t o = 0; ok && o < reg.second; o += kCheckpointChunk) {
+            const size_t n = std::min(kCheckpointChunk, reg.second - o);
+            buf.resize(n);
+            const cudaError_t e = cudaMemcpy(buf.data(), (const char*)reg.first + o, n, cudaMemcpyDeviceToHost);
+            if (e != cudaSuccess) {
+                std::fclose(f);
+                return fail(h, ACP_ERR_CUDA, "checkpoint copy: %s", cudaGetErrorString(e));
+            }
+            ok = std::fwrite(buf.data(), 1, n, f) == n;
+        }
+    }
+    ok = (std::fclose(f) == 0) && ok;
+    if (!ok) return fail(h, ACP_ERR_INVALID, "writing %s failed", path);
+    return ACP_OK;
+}
+
+int acp_checkpoint_load(acp_handle* h, const char* path) {
+    if (!h || !path) return ACP_ERR_INVALID;
+    if (!h->inited) return fail(h, ACP_ERR_STATE, "restore before acp_init");
+    if (h->batch) return fail(h, ACP_ERR_STATE, "the case belongs to a batch");
+    CU(h, cudaSetDevice(h->device));
+    CU(h, cudaStreamSynchronize(h->stream));
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return fail(h, ACP_ERR_INVALID, "cannot read %s", path);
+    CheckpointHeader hd;
+    if (std::fread(&hd, sizeof hd, 1, f) != 1 || std::memcmp(hd.magic, kCheckpointMagic, sizeof hd.magic) != 0) {
+        std::fclose(f);
+        return fail(h, ACP_ERR_INVALID, "%s is not a checkpoint of this engine", path);
+    }
+    const CheckpointHeader mine = checkpointHeader(h);
+    if (hd.abi != mine.abi || hd.storage != mine.storage || hd.levels != mine.levels ||
+        std::memcmp(hd.dims, mine.dims, sizeof hd.dims) != 0 || std::memcmp(hd.slots, mine.slots, sizeof hd.slots) != 0 ||
+        (hd.cur != 0 && hd.cur != 1) || hd.steps < 0) {
+        std::fclose(f);
+        return fail(h, ACP_ERR_INVALID, "%s holds a case of another storage form or level shape", path);
+    }
+    std::vector<char> buf;
+    for (const auto& reg : checkpointRegions(h)) {
+        for (size_t o = 0; o < reg.second; o += kCheckpointChunk) {
+            const size_t n = std::min(kCheckpointChunk, reg.second - o);
+            buf.resize(n);
+            if (std::fread(buf.data(), 1, n, f) != n) {
+                std::fclose(f);
+                return fail(h, ACP_ERR_INVALID, "%s is truncated", path);
+            }
+            CU(h, cudaMemcpy((char*)reg.first + o, buf.data(), n, cudaMemcpyHostToDevice));
+        }
+    }
+    std::fclose(f);
+    h->cur = hd.cur;
+    h->steps = hd.steps;
+    if (h->dCounter) CU(h, cudaMemset(h->dCounter, 0, sizeof(int)));
+    CU(h, cudaMemset(h->dErr, 0, sizeof(int)));
     return ACP_OK;
 }
 

@@ -45,6 +45,8 @@ def lib():
         L.acp_set_probes.argtypes = [vp, C.c_int, vp]
         L.acp_read_probes.argtypes = [vp, vp, C.c_int, C.POINTER(C.c_int)]
         L.acp_steps_done.argtypes = [vp, C.POINTER(C.c_longlong)]
+        L.acp_checkpoint_save.argtypes = [vp, C.c_char_p]
+        L.acp_checkpoint_load.argtypes = [vp, C.c_char_p]
         L.acp_set_stream.argtypes = [vp, vp]
         L.acp_device_bytes.argtypes = [vp, C.POINTER(C.c_size_t)]
         L.acp_estimate_bytes.argtypes = [C.POINTER(CaseDesc), C.POINTER(C.c_size_t)]
@@ -150,6 +152,15 @@ class Lattice:
         s = C.c_longlong()
         self._check(lib().acp_steps_done(self._h, C.byref(s)))
         return s.value
+
+    def save_checkpoint(self, path):
+        """Write the case's complete device state to `path` (acp_checkpoint_save)."""
+        self._check(lib().acp_checkpoint_save(self._h, os.fsencode(path)))
+
+    def load_checkpoint(self, path):
+        """Restore a state written by save_checkpoint into this initialised case."""
+        self._check(lib().acp_checkpoint_load(self._h, os.fsencode(path)))
+        return self
 
     def device_bytes(self):
         b = C.c_size_t()

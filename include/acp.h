@@ -158,6 +158,21 @@ int acp_active_updates(acp_handle* h, long long* coarse_nodes, long long* fine_n
 int acp_read_populations(acp_handle* h, int level, double* host_out);
 /* Overwrite a level's populations (both ping-pong arrays) from FP64 f_i. */
 int acp_write_populations(acp_handle* h, int level, const double* host_in);
+/* Checkpoint / restart of a case's device state.  The reference keeps no
+ * restart state: main.cpp:37-121 builds and initialises every run from
+ * BoundaryConditions.txt.  A checkpoint file holds the complete state a
+ * coarse step reads: both ping-pong population arrays of every level in
+ * their storage form (bit-exact), the partner-strain records of the coupling
+ * nodes, the ping-pong parity and the number of coarse steps done.
+ * acp_checkpoint_save waits for the case's queued steps first.
+ * acp_checkpoint_load needs a handle created from a case of the same storage
+ * form and level shapes and initialised (acp_init); it then continues bit-for-
+ * bit as the saved run would have.  A mismatched file gives ACP_ERR_INVALID,
+ * a file that cannot be read or written ACP_ERR_INVALID with the reason in
+ * acp_last_error.  Probe series restart empty.  Cases stepped by a batch are
+ * refused (ACP_ERR_STATE). */
+int acp_checkpoint_save(acp_handle* h, const char* path);
+int acp_checkpoint_load(acp_handle* h, const char* path);
 /* A macroscopic field of a level (SI: kg/m^3, m/s, Pa), host buffer of nodes doubles. */
 int acp_read_field(acp_handle* h, int level, int field, double* host_out);
 /* Pressure probes: n probes at (level, i, j, k) quadruples, i j k in the
