@@ -773,10 +773,13 @@ dim3 gridOf(const LevelHost& L, int bx) { return dim3((L.nx + bx - 1) / bx, L.ny
 
 // enqueue one step of a single level, reading array src
 template <typename S, typename R>
-int enqueueLevelStep(acp_handle* h, int l, int src, PhaseTimer* tm = nullptr, cudaStream_t st = nullptr) {
+int enqueueLevelLodi(acp_handle* h, int l, int src, PhaseTimer* tm, cudaStream_t st);
+
+template <typename S, typename R>
+int enqueueLevelStep(acp_handle* h, int l, int src, PhaseTimer* tm = nullptr, cudaStream_t st = nullptr,
+                     bool lodi = true) {
     if (!st) st = h->stream;
     const LevelHost& L = h->host[l];
-    const LevelDev& D = h->dev[l];
     LevelArgs<S> a = levelArgs<S>(h, l, src);
     const int bx = 128;
     if (tm) tm->mark(-1);
@@ -788,6 +791,15 @@ int enqueueLevelStep(acp_handle* h, int l, int src, PhaseTimer* tm = nullptr, cu
         pickCollide<S, R>(h->d)<<<gridOf(L, bx), bx, 0, st>>>(a);
     }
     if (tm) tm->mark(ACP_K_COLLIDE);
+    return lodi ? enqueueLevelLodi<S, R>(h, l, src, tm, st) : ACP_OK;
+}
+
+// the LODI passes of a level after its collide + push (reading array src)
+template <typename S, typename R>
+int enqueueLevelLodi(acp_handle* h, int l, int src, PhaseTimer* tm, cudaStream_t st) {
+    if (!st) st = h->stream;
+    const LevelDev& D = h->dev[l];
+    LevelArgs<S> a = levelArgs<S>(h, l, src);
     const LodiArgs p = lodiArgsOf(h, l);
     LodiFn<S> lf = pickLodi<S>(h->d.eq_order);
     // eight lanes per boundary node (one per stencil member) and small blocks
@@ -840,14 +852,29 @@ int enqueueStepT(acp_handle* h, int src, PhaseTimer* tm) {
     } else {
         LevelArgs<S> lc = levelArgs<S>(h, 0, src);
         const CouplingArgs c = couplingArgs(h);
-        // the coarse step (with the saving of the coupling sources) and the first
-        // fine sub-step touch different arrays: in a graph they run side by side
+        // in a captured graph three branches run side by side where the kernels
+        // touch disjoint data: the coarse step (with the saving of the coupling
+        // sources) beside the first fine sub-step; the fine level's LODI passes
+        // (domain-face nodes and their normal neighbours) beside the coupling
+        // kernels (coupling nodes: a coupling node on a LODI face is refused at
+        // set-up); F2C (coarse coupling nodes from a fine cube two cells inside
+        // the box) beside the last C2F (fine coupling nodes from regular coarse
+        // nodes).  Timed runs (tm) keep one stream.
         const bool fork = tm == nullptr;
-        cudaStream_t cs = h->stream;
+        cudaStream_t cs = h->stream, ls = h->stream, fs = h->stream;
+        auto branch = [h](cudaStream_t to, cudaEvent_t ev) {
+            cudaEventRecord(ev, h->stream);
+            cudaStreamWaitEvent(to, ev, 0);
+        };
+        auto join = [h](cudaStream_t from, cudaEvent_t ev) {
+            cudaEventRecord(ev, from);
+            cudaStreamWaitEvent(h->stream, ev, 0);
+        };
         if (fork) {
-            cudaEventRecord(h->forkEv, h->stream);
-            cudaStreamWaitEvent(h->side, h->forkEv, 0);
+            branch(h->side, h->forkEv);
             cs = h->side;
+            ls = h->side2;
+            fs = h->side;
         }
         if (tm) tm->mark(-1);
         if (h->nCoinc)
@@ -855,29 +882,36 @@ int enqueueStepT(acp_handle* h, int src, PhaseTimer* tm) {
                 lc.A, h->dC2F, h->nCoinc, (R*)h->dPre, lc, c);
         if (tm) tm->mark(ACP_K_COUPLING);
         enqueueLevelStep<S, R>(h, 0, src, tm, cs);  // coarse t -> t+1
-        enqueueLevelStep<S, R>(h, 1, 0, tm);        // fine t -> t+1/2
-        if (fork) {
-            cudaEventRecord(h->joinEv, h->side);
-            cudaStreamWaitEvent(h->stream, h->joinEv, 0);
-        }
+        enqueueLevelStep<S, R>(h, 1, 0, tm, h->stream, false);  // fine t -> t+1/2
+        if (fork) branch(ls, h->branchEv[0]);
+        enqueueLevelLodi<S, R>(h, 1, 0, tm, ls);
+        if (fork) join(h->side, h->joinEv);
         if (tm) tm->mark(-1);
         enqueueC2F<S, R>(h, 1 - src, 1, R(0.5));  // C2F at t+1/2
         if (tm) tm->mark(ACP_K_COUPLING);
-        enqueueLevelStep<S, R>(h, 1, 1, tm);    // fine t+1/2 -> t+1
+        if (fork) join(ls, h->branchEv[1]);
+        enqueueLevelStep<S, R>(h, 1, 1, tm, h->stream, false);  // fine t+1/2 -> t+1
+        if (fork) branch(ls, h->branchEv[2]);
+        enqueueLevelLodi<S, R>(h, 1, 1, tm, ls);
         if (tm) tm->mark(-1);
         if (!h->f2cHost.empty()) {  // STD only: the direct coupling does F2C in its t+1 pass
+            if (fork) branch(fs, h->branchEv[3]);
             LevelArgs<S> lf = levelArgs<S>(h, 1, 0);
             const unsigned g = ((unsigned)h->f2cHost.size() * 32 + 127) / 128;  // a warp per coarse node
             const S* Ff = (const S*)h->dev[1].f[0];
             S* Bc = (S*)h->dev[0].f[1 - src];
             const int n = (int)h->f2cHost.size();
             const int o = h->d.eq_order;
-            if (o == 2) k_f2c<S, R, 2><<<g, 128, 0, h->stream>>>(Ff, Bc, h->dF2C, n, c, lf);
-            else if (o == 3) k_f2c<S, R, 3><<<g, 128, 0, h->stream>>>(Ff, Bc, h->dF2C, n, c, lf);
-            else k_f2c<S, R, 4><<<g, 128, 0, h->stream>>>(Ff, Bc, h->dF2C, n, c, lf);
+            if (o == 2) k_f2c<S, R, 2><<<g, 128, 0, fs>>>(Ff, Bc, h->dF2C, n, c, lf);
+            else if (o == 3) k_f2c<S, R, 3><<<g, 128, 0, fs>>>(Ff, Bc, h->dF2C, n, c, lf);
+            else k_f2c<S, R, 4><<<g, 128, 0, fs>>>(Ff, Bc, h->dF2C, n, c, lf);
         }
         enqueueC2F<S, R>(h, 1 - src, 0, R(1.0));  // C2F at t+1
         if (tm) tm->mark(ACP_K_COUPLING);
+        if (fork) {
+            if (!h->f2cHost.empty()) join(fs, h->branchEv[4]);
+            join(ls, h->branchEv[5]);
+        }
     }
     if (h->nProbes) {
         launchProbes<S>(h, h->stream, 1 - src);
@@ -1122,6 +1156,8 @@ int acp_create(const acp_case_desc* d, int device, acp_handle** out) {
     CU(h, cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
     CU(h, cudaEventCreateWithFlags(&h->forkEv, cudaEventDisableTiming));
     CU(h, cudaEventCreateWithFlags(&h->joinEv, cudaEventDisableTiming));
+    CU(h, cudaStreamCreateWithFlags(&h->side2, cudaStreamNonBlocking));
+    for (cudaEvent_t& e : h->branchEv) CU(h, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     if ((s = devAlloc(h, (void**)&h->dErr, sizeof(int)))) return s;
     CU(h, cudaMemsetAsync(h->dErr, 0, sizeof(int), h->stream));
     h->dev.resize(h->host.size());
@@ -1643,6 +1679,9 @@ int acp_destroy(acp_handle* h) {
     if (h->side) cudaStreamDestroy(h->side);
     if (h->forkEv) cudaEventDestroy(h->forkEv);
     if (h->joinEv) cudaEventDestroy(h->joinEv);
+    if (h->side2) cudaStreamDestroy(h->side2);
+    for (cudaEvent_t e : h->branchEv)
+        if (e) cudaEventDestroy(e);
     delete h;
     return ACP_OK;
 }

@@ -59,6 +59,10 @@ struct acp_handle {
     bool ownStream = false;
     cudaStream_t side = nullptr;  // second branch of a captured step (coarse level beside the fine sub-step)
     cudaEvent_t forkEv = nullptr, joinEv = nullptr;
+    // third branch of a captured step: the fine level's LODI passes beside the
+    // coupling kernels, F2C beside the last C2F (disjoint node sets)
+    cudaStream_t side2 = nullptr;
+    cudaEvent_t branchEv[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     cudaGraphExec_t graph[2] = {nullptr, nullptr};  // one step starting from cur == 0 / cur == 1
     // two-level coupling (fine state always in array 0 between coarse steps)
     std::vector<acp::C2FDev> c2fHost;
