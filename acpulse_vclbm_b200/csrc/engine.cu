@@ -1467,6 +1467,81 @@ int acp_checkpoint_load(acp_handle* h, const char* path) {
     return ACP_OK;
 }
 
+int acp_write_vtk(acp_handle* h, const char* prefix, int binary) {
+    if (!h || !prefix || (binary != 0 && binary != 1)) return ACP_ERR_INVALID;
+    if (h->dev.empty()) return ACP_ERR_STATE;
+    CU(h, cudaSetDevice(h->device));
+    joinBatch(h);
+    const acp_case_desc& d = h->d;
+    const double cs2 = d.speed_of_sound * d.speed_of_sound;
+    for (size_t l = 0; l < h->host.size(); ++l) {
+        const LevelHost& L = h->host[l];
+        const size_t N = (size_t)L.N;
+        const int arr = l == 0 ? h->cur : 0;
+        double* tmp = nullptr;
+        CU(h, cudaMallocAsync((void**)&tmp, N * 4 * sizeof(double), h->stream));
+        const unsigned grid = (unsigned)((N + 255) / 256);
+        switch (d.storage) {
+            case ACP_STORE_F64:
+                k_fields4<double><<<grid, 256, 0, h->stream>>>((const double*)h->dev[l].f[arr], tmp, L.N, h->shift, h->c,
+                                                                levelArgs<double>(h, (int)l, 0));
+                break;
+            case ACP_STORE_F32_DEV:
+                k_fields4<float><<<grid, 256, 0, h->stream>>>((const float*)h->dev[l].f[arr], tmp, L.N, h->shift, h->c,
+                                                               levelArgs<float>(h, (int)l, 0));
+                break;
+            default:
+                k_fields4<__half><<<grid, 256, 0, h->stream>>>((const __half*)h->dev[l].f[arr], tmp, L.N, h->shift, h->c,
+                                                                levelArgs<__half>(h, (int)l, 0));
+                break;
+        }
+        std::vector<double> v(N * 4);
+        cudaError_t e = cudaMemcpyAsync(v.data(), tmp, N * 4 * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+        cudaFreeAsync(tmp, h->stream);
+        if (e != cudaSuccess) return fail(h, ACP_ERR_CUDA, "copy: %s", cudaGetErrorString(e));
+        CU(h, cudaStreamSynchronize(h->stream));
+        const double* rho = v.data();
+        const double* u[3] = {v.data() + N, v.data() + 2 * N, v.data() + 3 * N};
+        const std::string path = std::string(prefix) + (h->host.size() > 1 ? "_level" + std::to_string(l) : "") + ".vtk";
+        FILE* f = std::fopen(path.c_str(), "wb");
+        if (!f) return fail(h, ACP_ERR_INVALID, "cannot write %s", path.c_str());
+        const double sp = d.spacing / std::pow(2.0, (double)l);
+        std::fprintf(f, "# vtk DataFile Version 3.0\nacPulse_vcLBM level %d\n%s\nDATASET STRUCTURED_POINTS\n", (int)l,
+                     binary ? "BINARY" : "ASCII");
+        std::fprintf(f, "DIMENSIONS %d %d %d\n", L.nx, L.ny, L.nz);
+        std::fprintf(f, "ORIGIN %.8g %.8g %.8g\n", L.off[0] * sp, L.off[1] * sp, L.off[2] * sp);
+        std::fprintf(f, "SPACING %.8g %.8g %.8g\nPOINT_DATA %zu\n", sp, sp, sp, N);
+        // values in file order: big-endian FP64 (binary) or %.8g text
+        std::vector<unsigned char> be;
+        auto put = [&](const double* x, size_t n, size_t stride, int per) {
+            if (binary) {
+                be.resize(n * per * 8);
+                for (size_t m = 0; m < n; ++m)
+                    for (int k = 0; k < per; ++k) {
+                        uint64_t w;
+                        std::memcpy(&w, x + m + k * stride, 8);
+                        for (int b = 0; b < 8; ++b) be[(m * per + k) * 8 + b] = (unsigned char)(w >> (56 - 8 * b));
+                    }
+                std::fwrite(be.data(), 1, be.size(), f);
+                std::fputc('\n', f);
+            } else {
+                for (size_t m = 0; m < n; ++m)
+                    for (int k = 0; k < per; ++k) std::fprintf(f, k + 1 < per ? "%.8g " : "%.8g\n", x[m + k * stride]);
+            }
+        };
+        std::vector<double> p(N);
+        for (size_t m = 0; m < N; ++m) p[m] = rho[m] * cs2;
+        std::fprintf(f, "SCALARS Pressure double 1\nLOOKUP_TABLE default\n");
+        put(p.data(), N, 0, 1);
+        std::fprintf(f, "SCALARS Density double 1\nLOOKUP_TABLE default\n");
+        put(rho, N, 0, 1);
+        std::fprintf(f, "VECTORS Velocity double\n");
+        put(u[0], N, N, 3);
+        if (std::fclose(f) != 0) return fail(h, ACP_ERR_INVALID, "writing %s failed", path.c_str());
+    }
+    return ACP_OK;
+}
+
 int acp_read_field(acp_handle* h, int level, int field, double* out) {
     if (!h || !out || level < 0 || level >= (int)h->host.size() || field < 0 || field > 4) return ACP_ERR_INVALID;
     CU(h, cudaSetDevice(h->device));

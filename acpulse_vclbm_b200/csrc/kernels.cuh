@@ -951,6 +951,27 @@ __global__ void k_field(const S* __restrict__ src, double* dst, long long N, dou
     }
     dst[n] = r;
 }
+// density and the three velocity components of every node, out[4][N], with
+// the arithmetic of k_field
+template <typename S>
+__global__ void k_fields4(const S* __restrict__ src, double* out, long long N, double shift, double c,
+                          LevelArgs<S> la) {
+    const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    double rho = 0, jx = 0, jy = 0, jz = 0;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const double v = (double)Store<S>::load(src + q * N + n, la.hscale[q]) + wq(q) * shift;
+        rho += v;
+        jx += ex(q) * v;
+        jy += ey(q) * v;
+        jz += ez(q) * v;
+    }
+    out[n] = rho;
+    out[N + n] = c * jx / rho;
+    out[2 * N + n] = c * jy / rho;
+    out[3 * N + n] = c * jz / rho;
+}
 // storage -> absolute FP64 populations of the node window [begin, begin+count)
 template <typename S>
 __global__ void k_to_f64_window(const S* __restrict__ src, double* dst, long long N, long long begin, int count,

@@ -47,6 +47,7 @@ def lib():
         L.acp_steps_done.argtypes = [vp, C.POINTER(C.c_longlong)]
         L.acp_checkpoint_save.argtypes = [vp, C.c_char_p]
         L.acp_checkpoint_load.argtypes = [vp, C.c_char_p]
+        L.acp_write_vtk.argtypes = [vp, C.c_char_p, C.c_int]
         L.acp_set_stream.argtypes = [vp, vp]
         L.acp_device_bytes.argtypes = [vp, C.POINTER(C.c_size_t)]
         L.acp_estimate_bytes.argtypes = [C.POINTER(CaseDesc), C.POINTER(C.c_size_t)]
@@ -152,6 +153,10 @@ class Lattice:
         s = C.c_longlong()
         self._check(lib().acp_steps_done(self._h, C.byref(s)))
         return s.value
+
+    def write_vtk(self, prefix, binary=False):
+        """Legacy VTK files of every level (acp_write_vtk): ASCII as the reference writes them, or binary."""
+        self._check(lib().acp_write_vtk(self._h, os.fsencode(prefix), 1 if binary else 0))
 
     def save_checkpoint(self, path):
         """Write the case's complete device state to `path` (acp_checkpoint_save)."""

@@ -71,28 +71,6 @@ double Lattice::getDistribution(bool& alternating, int& dir, int& level, int& i,
 }
 
 void Lattice::writeResultsVTK(std::string filename, bool&, bool&) {
-    const acp_case_desc& d = bc_.caseDescription();
-    for (int l = 0; l <= d.max_level; ++l) {
-        const int* n = dims_[l];
-        const size_t N = (size_t)n[0] * n[1] * n[2];
-        std::vector<double> rho(N), ux(N), uy(N), uz(N);
-        check(acp_read_field(h_, l, ACP_FIELD_RHO, rho.data()), "writeResultsVTK");
-        check(acp_read_field(h_, l, ACP_FIELD_UX, ux.data()), "writeResultsVTK");
-        check(acp_read_field(h_, l, ACP_FIELD_UY, uy.data()), "writeResultsVTK");
-        check(acp_read_field(h_, l, ACP_FIELD_UZ, uz.data()), "writeResultsVTK");
-        const double sp = d.spacing / std::pow(2., l);
-        std::ofstream out(filename + (d.max_level ? "_level" + std::to_string(l) : std::string()) + ".vtk");
-        out << "# vtk DataFile Version 3.0\nacPulse_vcLBM level " << l << "\nASCII\nDATASET STRUCTURED_POINTS\n";
-        out << "DIMENSIONS " << n[0] << " " << n[1] << " " << n[2] << "\n";
-        out << "ORIGIN " << origin_[l][0] * sp << " " << origin_[l][1] * sp << " " << origin_[l][2] * sp << "\n";
-        out << "SPACING " << sp << " " << sp << " " << sp << "\nPOINT_DATA " << N << "\n";
-        out << std::setprecision(8);
-        const double cs2 = d.speed_of_sound * d.speed_of_sound;
-        out << "SCALARS Pressure double 1\nLOOKUP_TABLE default\n";
-        for (size_t m = 0; m < N; ++m) out << rho[m] * cs2 << "\n";
-        out << "SCALARS Density double 1\nLOOKUP_TABLE default\n";
-        for (size_t m = 0; m < N; ++m) out << rho[m] << "\n";
-        out << "VECTORS Velocity double\n";
-        for (size_t m = 0; m < N; ++m) out << ux[m] << " " << uy[m] << " " << uz[m] << "\n";
-    }
+    // the reference's ASCII form; acp_write_vtk(h, prefix, 1) writes the binary form of the same files
+    check(acp_write_vtk(h_, filename.c_str(), 0), "writeResultsVTK");
 }

@@ -173,6 +173,14 @@ int acp_write_populations(acp_handle* h, int level, const double* host_in);
  * refused (ACP_ERR_STATE). */
 int acp_checkpoint_save(acp_handle* h, const char* path);
 int acp_checkpoint_load(acp_handle* h, const char* path);
+/* Legacy structured-points VTK of every level with the fields the reference
+ * writes (Lattice::writeResultsVTK, Lattice.cpp:2212-4352: Pressure,
+ * Density, Velocity): `<prefix>.vtk` for one level, `<prefix>_level<l>.vtk`
+ * for two.  binary = 0 writes ASCII with 8 significant digits (the
+ * reference's form); binary = 1 the BINARY form of the same format
+ * (big-endian FP64), about a third of the size and read without parsing
+ * text.  The four fields of a level are formed on the device in one pass. */
+int acp_write_vtk(acp_handle* h, const char* prefix, int binary);
 /* A macroscopic field of a level (SI: kg/m^3, m/s, Pa), host buffer of nodes doubles. */
 int acp_read_field(acp_handle* h, int level, int field, double* host_out);
 /* Pressure probes: n probes at (level, i, j, k) quadruples, i j k in the
