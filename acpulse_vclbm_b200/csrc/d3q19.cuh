@@ -304,6 +304,19 @@ __device__ __forceinline__ void gsBackAll(const R* x, F&& f, std::integer_sequen
     (f(q, gsBackRow<R, q, skipConserved>(x, std::make_integer_sequence<int, 19>{})), ...);
 }
 
+// sum_m Minv[q][m] * x[m] over the moments m in the bit set `mask`, zero
+// coefficients dropped at compile time
+template <typename R, int q, unsigned mask, int... m>
+__device__ __forceinline__ R gsBackRowMasked(const R* x, std::integer_sequence<int, m...>) {
+    R acc = R(-0.0);
+    ((GsInv<q, m>::v != 0.0 && ((mask >> m) & 1u) ? (void)(acc += R(GsInv<q, m>::v) * x[m]) : (void)0), ...);
+    return acc;
+}
+template <typename R, unsigned mask, typename F, int... q>
+__device__ __forceinline__ void gsBackAllMasked(const R* x, F&& f, std::integer_sequence<int, q...>) {
+    (f(q, gsBackRowMasked<R, q, mask>(x, std::make_integer_sequence<int, 19>{})), ...);
+}
+
 // raw-moment basis rows 5..9: the deviatoric second-order moments relaxed with
 // omega (Node.cpp:2720-2733, 2580-2584)
 __host__ __device__ constexpr int rmRow2(int m, int q) {

@@ -276,32 +276,40 @@ struct Collider {
         const R kappa = R(a.kappa);
 
         if (OP == OP_MRT_GS) {
-            R dm[Q];
+            // post-collision moments, back-transformed at once: the conserved
+            // ones (drho, j), the six viscous ones relaxed at omega towards
+            // their equilibria, every other one at its equilibrium, which is
+            // zero (Node.cpp:2838-2931).  The moments of the rest state
+            // w_q rho0 vanish except the density's, so in the deviation form
+            // only moment 0 carries drho instead of rho.
+            R mp[Q];
+            const R om1 = R(1) - omega;
 #pragma unroll
             for (int mm = 0; mm < Q; ++mm) {
-                R m = R(a.shift) * R(c_gsMw[mm]);
+                const bool visc = mm == 1 || mm == 9 || mm == 11 || mm == 13 || mm == 14 || mm == 15;
+                if (!visc) continue;
+                R m = R(-0.0);
 #pragma unroll
                 for (int q = 0; q < Q; ++q)
                     if (gsRow(mm, q) != 0) m += R(gsRow(mm, q)) * g[q];
-                R meq = 0;
+                R meq;
                 switch (mm) {
-                    case 0: meq = rho; break;
                     case 1: meq = (jx * jx + jy * jy + jz * jz) * inv; break;
-                    case 3: meq = jx; break;
-                    case 5: meq = jy; break;
-                    case 7: meq = jz; break;
                     case 9: meq = (R(2) * jx * jx - jy * jy - jz * jz) * inv; break;
                     case 11: meq = (jy * jy - jz * jz) * inv; break;
                     case 13: meq = jx * jy * inv; break;
                     case 14: meq = jy * jz * inv; break;
-                    case 15: meq = jx * jz * inv; break;
-                    default: meq = 0;
+                    default: meq = jx * jz * inv; break;
                 }
-                const bool conserved = mm == 0 || mm == 3 || mm == 5 || mm == 7;
-                const bool visc = mm == 1 || mm == 9 || mm == 11 || mm == 13 || mm == 14 || mm == 15;
-                dm[mm] = conserved ? R(0) : (visc ? omega : R(1)) * (meq - m);
+                mp[mm] = meq + om1 * (m - meq);
             }
-            gsBackAll<R, true>(dm, [&](int q, R back) { emit(q, g[q] + back); }, std::make_integer_sequence<int, Q>{});
+            mp[0] = drho;
+            mp[3] = jx;
+            mp[5] = jy;
+            mp[7] = jz;
+            constexpr unsigned kPost = (1u << 0) | (1u << 1) | (1u << 3) | (1u << 5) | (1u << 7) | (1u << 9) |
+                                       (1u << 11) | (1u << 13) | (1u << 14) | (1u << 15);
+            gsBackAllMasked<R, kPost>(mp, [&](int q, R back) { emit(q, back); }, std::make_integer_sequence<int, Q>{});
             return;
         }
 
