@@ -19,6 +19,7 @@
 #include <cuda_runtime.h>
 #include <cuda_fp16.h>
 
+#include <type_traits>
 #include <utility>
 
 namespace acp {
@@ -251,11 +252,13 @@ struct Mat19 {
     double a[19][19];
 };
 constexpr double cabs(double x) { return x < 0 ? -x : x; }
-constexpr Mat19 gsInverse() {
+// inverse of the 19 x 19 integer basis row(m, q) by Gauss-Jordan elimination
+// with partial pivoting, evaluated by the compiler
+constexpr Mat19 basisInverse(int (*row)(int, int)) {
     double m[19][38] = {};
     for (int r = 0; r < 19; ++r)
         for (int c = 0; c < 19; ++c) {
-            m[r][c] = gsRow(r, c);
+            m[r][c] = row(r, c);
             m[r][19 + c] = r == c ? 1.0 : 0.0;
         }
     for (int c = 0; c < 19; ++c) {
@@ -281,12 +284,46 @@ constexpr Mat19 gsInverse() {
         for (int c = 0; c < 19; ++c) out.a[r][c] = m[r][19 + c];
     return out;
 }
+constexpr Mat19 gsInverse() { return basisInverse(gsRow); }
 constexpr Mat19 kGsInverse = gsInverse();
 template <int q, int m>
 struct GsInv {
     static constexpr double v = kGsInverse.a[q][m];
 };
 __host__ __device__ constexpr bool gsConserved(int m) { return m == 0 || m == 3 || m == 5 || m == 7; }
+
+// raw-moment basis (Node.cpp:2607-2795): 1, x, y, z, |e|^2, x^2-z^2, y^2-z^2,
+// xy, xz, yz, x^2 z, x z^2, y^2 z, y z^2, x^2 y, x y^2, x^2 z^2, x^2 y^2, y^2 z^2
+__host__ __device__ constexpr int rmRow(int m, int q) {
+    const int x = ex(q), y = ey(q), z = ez(q);
+    switch (m) {
+        case 0: return 1;
+        case 1: return x;
+        case 2: return y;
+        case 3: return z;
+        case 4: return x * x + y * y + z * z;
+        case 5: return x * x - z * z;
+        case 6: return y * y - z * z;
+        case 7: return x * y;
+        case 8: return x * z;
+        case 9: return y * z;
+        case 10: return x * x * z;
+        case 11: return x * z * z;
+        case 12: return y * y * z;
+        case 13: return y * z * z;
+        case 14: return x * x * y;
+        case 15: return x * y * y;
+        case 16: return x * x * z * z;
+        case 17: return x * x * y * y;
+        default: return y * y * z * z;
+    }
+}
+constexpr Mat19 kRmInverse = basisInverse(rmRow);
+template <int q, int m>
+struct RmInv {
+    static constexpr double v = kRmInverse.a[q][m];
+};
+
 
 // sum_m Minv[q][m] * x[m] over the moments (the conserved ones skipped when
 // `skipConserved`), zero coefficients dropped at compile time

@@ -255,6 +255,18 @@ __device__ __forceinline__ void regularisedEmit(R drho, const R* u, const R* s2,
     forEachDirection<R, ORDER>(mc, kappa, [&](int q, R poly) { emit(q, R(wq(q)) * (drho + poly)); });
 }
 
+// acc + Minv_RM[q][m] * d[m - 5], the term left out when the coefficient is zero
+template <typename R, int q, int m>
+__device__ __forceinline__ R rmBack(R acc, const R* d) {
+    if constexpr (RmInv<q, m>::v != 0.0) return acc + R(RmInv<q, m>::v) * d[m - 5];
+    else return acc;
+}
+// f(std::integral_constant<int, q>) for q = 0 .. 18
+template <typename F, int... q>
+__device__ __forceinline__ void forEachQ(F&& f, std::integer_sequence<int, q...>) {
+    (f(std::integral_constant<int, q>{}), ...);
+}
+
 template <typename R, int OP, int ORDER, bool CUBIC, bool MRTWB>
 struct Collider {
     // nb: as for regularisedEmit
@@ -346,13 +358,19 @@ struct Collider {
                     if (rmRow2(mm, q) != 0) d[mm] += R(rmRow2(mm, q)) * gn;
             }
             const R om1 = R(1) - omega;
-#pragma unroll
-            for (int q = 0; q < Q; ++q) {
-                R acc = 0;
-#pragma unroll
-                for (int mm = 0; mm < 5; ++mm) acc += RT<R>::rmTinv(q, mm) * d[mm];
+            // back transform of the five relaxed moments (raw-moment basis rows
+            // 5..9), its inverse's coefficients compile-time constants
+            auto back = [&](auto qc) {
+                constexpr int q = decltype(qc)::value;
+                R acc = R(-0.0);
+                acc = rmBack<R, q, 5>(acc, d);
+                acc = rmBack<R, q, 6>(acc, d);
+                acc = rmBack<R, q, 7>(acc, d);
+                acc = rmBack<R, q, 8>(acc, d);
+                acc = rmBack<R, q, 9>(acc, d);
                 emit(q, geqRM(q) + om1 * acc);
-            }
+            };
+            forEachQ(back, std::make_integer_sequence<int, Q>{});
             return;
         }
 

@@ -3,6 +3,8 @@ timing.  Prints the per-kernel device times of acp_step_timed.
 
 usage: python -m acpulse_vclbm_b200.profile_case [--op HRR] [--storage FP32-DEV]
            [--nx 1024 --ny 512 --nz 3] [--steps 3] [--levels 1]
+       python -m acpulse_vclbm_b200.profile_case --batched 64 [--steps 3]
+           (the seeded batched workload, workloads.batched_cases(seed=2024), in one batch)
 """
 import argparse
 import ctypes as C
@@ -25,7 +27,19 @@ def main():
                     help="2: refine the right half 2:1 (the sweep configuration's layout)")
     ap.add_argument("--filter", default="LAG")
     ap.add_argument("--coupling", default="STD", choices=["STD", "DC1", "DC2"])
+    ap.add_argument("--batched", type=int, default=0, help="run N seeded batched cases in one batch instead")
     a = ap.parse_args()
+    if a.batched:
+        from . import workloads
+        Ls = [engine.Lattice(d).init() for d in workloads.batched_cases(seed=2024, n=a.batched)]
+        B = engine.Batch(Ls)
+        B.step(a.steps)
+        B.sync()
+        print(B.info())
+        B.close()
+        for L in Ls:
+            L.close()
+        return
     d = lattice_units_case(a.nx, a.ny, a.nz, op=a.op, nu_lu=1e-4, order=a.order, periodic=(False, True, True),
                            eps=1e-3, b=24.0, center=(a.nx / 4.0, a.ny / 2.0, 1.0), storage=a.storage)
     d.mrt_writeback = 1
