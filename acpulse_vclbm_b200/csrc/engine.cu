@@ -39,48 +39,11 @@ int uploadConstants(int device) {
     return ACP_OK;
 }
 
-// MRT bases on the host: inverse of the Gram-Schmidt basis and the
-// raw-moment back transform, uploaded once per process.
-bool invert(const double* m, double* inv, int n) {
-    std::vector<double> a(n * 2 * n);
-    for (int r = 0; r < n; ++r)
-        for (int c = 0; c < n; ++c) {
-            a[r * 2 * n + c] = m[r * n + c];
-            a[r * 2 * n + n + c] = r == c;
-        }
-    for (int c = 0; c < n; ++c) {
-        int p = c;
-        for (int r = c + 1; r < n; ++r)
-            if (std::fabs(a[r * 2 * n + c]) > std::fabs(a[p * 2 * n + c])) p = r;
-        if (std::fabs(a[p * 2 * n + c]) < 1e-12) return false;
-        for (int k = 0; k < 2 * n; ++k) std::swap(a[p * 2 * n + k], a[c * 2 * n + k]);
-        double piv = a[c * 2 * n + c];
-        for (int k = 0; k < 2 * n; ++k) a[c * 2 * n + k] /= piv;
-        for (int r = 0; r < n; ++r) {
-            if (r == c) continue;
-            double f = a[r * 2 * n + c];
-            if (f == 0) continue;
-            for (int k = 0; k < 2 * n; ++k) a[r * 2 * n + k] -= f * a[c * 2 * n + k];
-        }
-    }
-    for (int r = 0; r < n; ++r)
-        for (int c = 0; c < n; ++c) inv[r * n + c] = a[r * 2 * n + n + c];
-    return true;
-}
-
-int rmRowFull(int m, int q) {
-    const int x = ex(q), y = ey(q), z = ez(q);
-    const int v[Q] = {1, x, y, z, x * x + y * y + z * z, x * x - z * z, y * y - z * z, x * y, x * z, y * z,
-                      x * x * z, x * z * z, y * y * z, y * z * z, x * x * y, x * y * y, x * x * z * z,
-                      x * x * y * y, y * y * z * z};
-    return v[m];
-}
-
 }  // namespace
 
 namespace acp {
 
-// the lattice constant tables (push masks, MRT bases)
+// the lattice constant table (push masks)
 int makeConstTables(ConstTables& t) {
     uint32_t* masks = t.masks;
     for (int c = 0; c < 54; ++c) masks[c] = 0;
@@ -103,25 +66,6 @@ int makeConstTables(ConstTables& t) {
         masks[faceCode(b.fx, b.fy, b.fz)] = m;
     }
     masks[CODE_FLUID] = 0x3FFFFu;
-    double gs[Q * Q], rm[Q * Q], rmi[Q * Q];
-    double* gsi = t.gsi;
-    double* mw = t.mw;
-    double(*rm2)[5] = t.rm2;
-    for (int m = 0; m < Q; ++m)
-        for (int q = 0; q < Q; ++q) {
-            gs[m * Q + q] = gsRow(m, q);
-            rm[m * Q + q] = rmRowFull(m, q);
-        }
-    if (!invert(gs, gsi, Q) || !invert(rm, rmi, Q)) return ACP_ERR_INVALID;
-    for (int m = 0; m < Q; ++m) {
-        mw[m] = 0;
-        for (int q = 0; q < Q; ++q) mw[m] += gs[m * Q + q] * wq(q);
-    }
-    for (int q = 0; q < Q; ++q)
-        for (int m = 0; m < 5; ++m) rm2[q][m] = rmi[q * Q + 5 + m];
-    for (int k = 0; k < Q * Q; ++k) t.gsiF[k] = (float)gsi[k];
-    for (int q = 0; q < Q; ++q)
-        for (int m = 0; m < 5; ++m) t.rm2F[q][m] = (float)rm2[q][m];
     return ACP_OK;
 }
 

@@ -32,31 +32,17 @@ __host__ __device__ constexpr bool collides(uint8_t c) { return c == CODE_FLUID 
 
 // pushed-direction mask of each node class
 __constant__ uint32_t c_pushMask[54];
-// MRT bases: inverse of the Gram-Schmidt basis, the basis applied to w_q, and
-// the raw-moment back-transform columns of the five relaxed moments
-__constant__ double c_gsMinv[Q][Q];
-__constant__ double c_gsMw[Q];
-__constant__ double c_rmTinv2[Q][5];
-__constant__ float c_gsMinvF[Q][Q];
-__constant__ float c_rmTinv2F[Q][5];
 
-// host copies of those tables.  Without relocatable device code every
+// host copy of that table.  Without relocatable device code every
 // translation unit that includes this header owns its own __constant__
-// copies, so each one uploads them (uploadTables is static per unit), once
-// per device.
+// copy, so each one uploads it (uploadTables is static per unit), once per
+// device.  (The MRT bases' inverses are compile-time constants: GsInv, RmInv.)
 struct ConstTables {
     uint32_t masks[54];
-    double gsi[Q * Q], mw[Q], rm2[Q][5];
-    float gsiF[Q * Q], rm2F[Q][5];
 };
 int makeConstTables(ConstTables& t);
 static inline int uploadTables(const ConstTables& t) {
     if (cudaMemcpyToSymbol(c_pushMask, t.masks, sizeof t.masks) != cudaSuccess) return -2;
-    if (cudaMemcpyToSymbol(c_gsMinv, t.gsi, sizeof t.gsi) != cudaSuccess) return -2;
-    if (cudaMemcpyToSymbol(c_gsMw, t.mw, sizeof t.mw) != cudaSuccess) return -2;
-    if (cudaMemcpyToSymbol(c_rmTinv2, t.rm2, sizeof t.rm2) != cudaSuccess) return -2;
-    if (cudaMemcpyToSymbol(c_gsMinvF, t.gsiF, sizeof t.gsiF) != cudaSuccess) return -2;
-    if (cudaMemcpyToSymbol(c_rmTinv2F, t.rm2F, sizeof t.rm2F) != cudaSuccess) return -2;
     return 0;
 }
 
@@ -107,18 +93,6 @@ __device__ __forceinline__ float scaleOf(const LevelArgs<S>& a, int q) {
 // post-collision populations are handed to `emit(q, value)` as they are
 // formed, so the regularised operators never hold the old populations and
 // the equilibrium at the same time (the equilibrium is formed twice instead).
-template <typename R>
-struct RT;
-template <>
-struct RT<double> {
-    __device__ __forceinline__ static double gsMinv(int q, int m) { return c_gsMinv[q][m]; }
-    __device__ __forceinline__ static double rmTinv(int q, int m) { return c_rmTinv2[q][m]; }
-};
-template <>
-struct RT<float> {
-    __device__ __forceinline__ static float gsMinv(int q, int m) { return c_gsMinvF[q][m]; }
-    __device__ __forceinline__ static float rmTinv(int q, int m) { return c_rmTinv2F[q][m]; }
-};
 
 // second-order sums {xx, yy, zz, xy, xz, yz} of a node's deviations g:
 // sum over the directions with a nonzero component (diagonal) or of the
