@@ -757,9 +757,10 @@ __device__ __forceinline__ void absMoments(const S* arr, long long N, long long 
         if (ez(q)) jz += ez(q) * g;
     }
     rho = shift + d;
-    uSI[0] = c * jx / rho;
-    uSI[1] = c * jy / rho;
-    uSI[2] = c * jz / rho;
+    const double cr = c / rho;  // one division for the three components
+    uSI[0] = cr * jx;
+    uSI[1] = cr * jy;
+    uSI[2] = cr * jz;
 }
 
 // threads per LODI boundary node: lane m of a node's group forms the moments
@@ -799,19 +800,22 @@ __device__ __forceinline__ void lodiBody(const S* __restrict__ A, S* B, const BN
     const double* veloB = su[0];
     const double* vN = su[1];
     const double* v2N = su[2];
+    // reciprocals formed once: the gradients' 1 / (2 dx), 1 / density, and
+    // the level constants dt / (2 cs^2), dt / (2 cs), 1 / c
     const double ls = p.localSpacing;
-    double dG = (4. * dN - d2N - 3. * densB) / (-2. * ls);
+    const double inv2ls = 1. / (2. * ls);
+    double dG = -(4. * dN - d2N - 3. * densB) * inv2ls;
     double vG[3];
-    for (int c = 0; c < 3; ++c) vG[c] = (4. * vN[c] - v2N[c] - 3. * veloB[c]) / (-2. * ls);
+    for (int c = 0; c < 3; ++c) vG[c] = -(4. * vN[c] - v2N[c] - 3. * veloB[c]) * inv2ls;
     double dGT[2] = {0, 0}, vGT[2][3] = {{0, 0, 0}, {0, 0, 0}};
     if (b.transverse) {
         const double* dT = sr + 3;
         const double(*vT)[3] = su + 3;
-        dGT[0] = (dT[0] - dT[1]) / (2. * ls);
-        dGT[1] = (dT[2] - dT[3]) / (2. * ls);
+        dGT[0] = (dT[0] - dT[1]) * inv2ls;
+        dGT[1] = (dT[2] - dT[3]) * inv2ls;
         for (int c = 0; c < 3; ++c) {
-            vGT[0][c] = (vT[0][c] - vT[1][c]) / (2. * ls);
-            vGT[1][c] = (vT[2][c] - vT[3][c]) / (2. * ls);
+            vGT[0][c] = (vT[0][c] - vT[1][c]) * inv2ls;
+            vGT[1][c] = (vT[2][c] - vT[3][c]) * inv2ls;
         }
     }
     const int nd = b.normalDir;
@@ -847,16 +851,19 @@ __device__ __forceinline__ void lodiBody(const S* __restrict__ A, S* B, const BN
         L5 = (sVB[0] + cs) * cs * (cs * dG + densB * sVG[0]);
     }
     const double L3 = sVB[0] * sVG[1], L4 = sVB[0] * sVG[2];
-    const double T3 = -(sVB[1] * sT[0][1] + sVB[2] * sT[1][1]) - (cs2 / densB) * dGT[0];
-    const double T4 = -(sVB[1] * sT[0][2] + sVB[2] * sT[1][2]) - (cs2 / densB) * dGT[1];
+    const double invDens = 1. / densB;
+    const double T3 = -(sVB[1] * sT[0][1] + sVB[2] * sT[1][1]) - (cs2 * invDens) * dGT[0];
+    const double T4 = -(sVB[1] * sT[0][2] + sVB[2] * sT[1][2]) - (cs2 * invDens) * dGT[1];
     const double dt = p.dt;
-    const double rho = densB - dt / (2. * cs2) * (L5 + L1) + dt / (2. * cs2) * (T5 + T1);
+    const double kr = dt / (2. * cs2), kv = dt / (2. * cs) * invDens;
+    const double rho = densB - kr * (L5 + L1) + kr * (T5 + T1);
     double v[3];
-    v[0] = sVB[0] - dt / (2. * densB * cs) * (L5 - L1) + dt / (2. * densB * cs) * (T5 - T1);
+    v[0] = sVB[0] - kv * (L5 - L1) + kv * (T5 - T1);
     v[1] = sVB[1] - dt * L3 + dt * T3;
     v[2] = sVB[2] - dt * L4 + dt * T4;
     double u[3];
-    for (int c = 0; c < 3; ++c) u[perm[c]] = v[c] / p.c;
+    const double invc = 1. / p.c;
+    for (int c = 0; c < 3; ++c) u[perm[c]] = v[c] * invc;
     if (!(rho > 0.5 * p.rho0 && rho < 1.5 * p.rho0)) atomicOr(p.errorFlag, 1);
     EqCoef<double, ORDER> ec;
     ec.set(u, p.kappa);
