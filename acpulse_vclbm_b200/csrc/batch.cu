@@ -103,7 +103,7 @@ __global__ void __launch_bounds__(TX * TY, TiledMinBlocks<R>::value)
 }
 
 template <typename S, int ORDER>
-__global__ void __launch_bounds__(32) kb_lodi(const BatchCase<S>* __restrict__ cases,
+__global__ void __launch_bounds__(128) kb_lodi(const BatchCase<S>* __restrict__ cases,
                                                const WorkItem* __restrict__ items, int n, int level, int fineSrc,
                                                int flip, int zy) {
     __shared__ LevelArgs<S> sa;
@@ -435,8 +435,8 @@ int buildGroup(acp_batch* b, Group& g) {
         phase(g.collide[l], [&](int c, const acp_handle* h) {
             collideItems(h->host[l], c, g.tiled, recs[c].lv[l].zChunk, items);
         });
-        phase(g.lodiX[l], [&](int c, const acp_handle* h) { blockItems(c, h->dev[l].nLodiX * LODI_TPN, 32, items); });
-        phase(g.lodiZY[l], [&](int c, const acp_handle* h) { blockItems(c, h->dev[l].nLodiZY * LODI_TPN, 32, items); });
+        phase(g.lodiX[l], [&](int c, const acp_handle* h) { blockItems(c, h->dev[l].nLodiX * LODI_TPN, 128, items); });
+        phase(g.lodiZY[l], [&](int c, const acp_handle* h) { blockItems(c, h->dev[l].nLodiZY * LODI_TPN, 128, items); });
     }
     if (g.levels == 2) {
         phase(g.save, [&](int c, const acp_handle* h) {
@@ -479,7 +479,7 @@ int occupancy(Group& g, const acp_case_desc& d) {
     };
     const int o = d.eq_order;
     g.resident[0] = occ((const void*)pickBatchCollide<S, R>(d), g.tiled ? TX * TY : 128);
-    g.resident[1] = occ((const void*)pickBatchLodi<S>(o), 32);
+    g.resident[1] = occ((const void*)pickBatchLodi<S>(o), 128);
     g.resident[2] = occ((const void*)kb_c2f_save<S, R>, 128);
     g.resident[3] = occ((const void*)pickBatchCoinc<S, R>(o), 128);
     g.resident[4] = occ((const void*)kb_c2f_interp<S, R>, 256);
@@ -505,10 +505,10 @@ void enqueueGroup(acp_batch* b, Group& g, int flip) {
                                                                                      g.collide[l].count, l, fineSrc,
                                                                                      flip);
         if (g.lodiX[l].count)
-            lodi<<<gridFor(b, g.lodiX[l].count, g.resident[1]), 32, 0, ls>>>(cs, it + g.lodiX[l].off,
+            lodi<<<gridFor(b, g.lodiX[l].count, g.resident[1]), 128, 0, ls>>>(cs, it + g.lodiX[l].off,
                                                                              g.lodiX[l].count, l, fineSrc, flip, 0);
         if (g.lodiZY[l].count)
-            lodi<<<gridFor(b, g.lodiZY[l].count, g.resident[1]), 32, 0, ls>>>(cs, it + g.lodiZY[l].off,
+            lodi<<<gridFor(b, g.lodiZY[l].count, g.resident[1]), 128, 0, ls>>>(cs, it + g.lodiZY[l].off,
                                                                               g.lodiZY[l].count, l, fineSrc, flip, 1);
     };
     if (g.levels == 1) {
