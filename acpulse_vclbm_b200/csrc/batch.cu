@@ -443,8 +443,8 @@ int buildGroup(acp_batch* b, Group& g) {
             blockItems(c, (long long)h->nCoinc * coincidentThreadsPerNode(couplingArgs(h)), 128, items);
         });
         phase(g.coinc, [&](int c, const acp_handle* h) {
-            blockItems(c, (long long)h->nCoinc * (h->dcHost.empty() ? coincidentThreadsPerNode(couplingArgs(h)) : 1), 128,
-                       items);
+            blockItems(c, (long long)h->nCoinc * (h->dcHost.empty() ? coincidentThreadsPerNode(couplingArgs(h)) : DC_TPN),
+                       128, items);
         });
         phase(g.mid, [&](int c, const acp_handle* h) {
             blockItems(c, (long long)h->nMid * interpComponents(h), 256, items);

@@ -766,7 +766,7 @@ void enqueueC2F(acp_handle* h, int cnew, int fdst, R th) {
     const R* pre = (const R*)h->dPre;
     const int o = h->d.eq_order;
     if (h->nCoinc && !h->dcHost.empty()) {
-        const unsigned g = (h->nCoinc + 127) / 128;
+        const unsigned g = (h->nCoinc * DC_TPN + 127) / 128;  // a warp per shared node
         S* Bw = (S*)h->dev[0].f[cnew];
         const int dc2 = h->d.coupling == ACP_COUPLING_DC2;
         if (o == 2) k_dc_couple<S, R, 2><<<g, 128, 0, h->stream>>>(Bw, Ff, h->dDC, h->nCoinc, pre, th, dc2, c, la);

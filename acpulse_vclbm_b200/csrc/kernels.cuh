@@ -1371,51 +1371,58 @@ __device__ __forceinline__ void regulariseNeq(const R* neq, R* out) {
     for (int q = 0; q < Q; ++q) out[q] = R(4.5) * R(wq(q)) * h2dot<R>(q, P);
 }
 
+// threads per shared node of the direct coupling: lane q gathers population
+// q (coarse state, time blend, the fine plane filter over up to nine
+// members), shuffles give every lane all nineteen, and lane q stores q
+constexpr int DC_TPN = 32;
+
 // th < 1: the fine side at t+1/2 (coarse state blended in time with the
-// saved pre-step state); th == 1: both sides at t+1.  One thread per shared node.
+// saved pre-step state); th == 1: both sides at t+1.  One warp per shared node.
 template <typename S, typename R, int ORDER>
 __device__ __forceinline__ void dcCoupleBody(S* Bc, S* Ff, const DCDev* __restrict__ nodes, int count, const R* __restrict__ pre,
                                              R th, int dc2, const CouplingArgs& c, const LevelArgs<S>& la, int bx) {
-    const int t = bx * blockDim.x + threadIdx.x;
-    if (t >= count) return;
+    const int tg = bx * blockDim.x + threadIdx.x;
+    const int t = tg / DC_TPN, lane = tg % DC_TPN;
+    if (t >= count) return;  // whole warps: DC_TPN is the warp size
     const DCDev& nd = nodes[t];
     const bool full = th == R(1);
-    R cp[Q], X[Q], eq[Q];
-#pragma unroll
-    for (int q = 0; q < Q; ++q) cp[q] = R(Store<S>::load(Bc + (long long)q * c.Nc + nd.nc, la.hscale[q]));
     // populations whose source node is live on neither level keep the coarse
     // state of t (complete after the previous exchange): no population that a
-    // level leaves unwritten is ever read
-#pragma unroll
-    for (int q = 0; q < Q; ++q) {
+    // level leaves unwritten is read.  At t+1 the fine populations are
+    // filtered over the interface plane, gathered before this warp overwrites
+    // the shared node's fine populations (the stencil's other nodes are
+    // hanging fine nodes, which this kernel does not write), each population's
+    // weights renormalised over the stencil nodes where it is valid.
+    R xm = 0, fm = 0;
+    if (lane < Q) {
+        const int q = lane;
         if (nd.vc >> q & 1u) {
-            X[q] = (R(1) - th) * pre[(long long)q * count + t] + th * cp[q];
+            const R cq = R(Store<S>::load(Bc + (long long)q * c.Nc + nd.nc, la.hscale[q]));
+            xm = (R(1) - th) * pre[(long long)q * count + t] + th * cq;
         } else if (full && (nd.vf >> q & 1u)) {
-            X[q] = R(Store<S>::load(Ff + (long long)q * c.Nf + nd.nf, la.hscale[q]));
+            xm = R(Store<S>::load(Ff + (long long)q * c.Nf + nd.nf, la.hscale[q]));
         } else {
-            X[q] = pre[(long long)q * count + t];
+            xm = pre[(long long)q * count + t];
         }
-    }
-    eqSplit<R, ORDER>(X, R(c.shiftC), R(c.kappa), eq);
-    const R aF2C = R(c.alphaF2C), aC2F = R(c.alphaC2F);
-    // t+1: the fine populations filtered over the interface plane, gathered
-    // before this thread overwrites the shared node's fine populations (the
-    // stencil's other nodes are hanging fine nodes, which this kernel does
-    // not write), and the weights of each population are renormalised over the
-    // stencil nodes where it is valid (no slot that a level leaves unwritten is read)
-    R ff[Q];
-    if (full) {
-#pragma unroll
-        for (int q = 0; q < Q; ++q) {
+        if (full) {
             R acc = 0, ws = 0;
+#pragma unroll
             for (int m = 0; m < 9; ++m)
                 if (nd.plane[m] >= 0 && (nd.pv[m] >> q & 1u)) {
                     acc += R(nd.w[m]) * R(Store<S>::load(Ff + (long long)q * c.Nf + nd.plane[m], la.hscale[q]));
                     ws += R(nd.w[m]);
                 }
-            ff[q] = ws > R(0) ? acc / ws : R(0);
+            fm = ws > R(0) ? acc / ws : R(0);
         }
     }
+    R X[Q], eq[Q], ff[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        X[q] = __shfl_sync(0xffffffffu, xm, q);
+        ff[q] = __shfl_sync(0xffffffffu, fm, q);
+    }
+    eqSplit<R, ORDER>(X, R(c.shiftC), R(c.kappa), eq);
+    const R aF2C = R(c.alphaF2C), aC2F = R(c.alphaC2F);
     // fine side
     {
         R neq[Q], sc[Q];
@@ -1428,14 +1435,14 @@ __device__ __forceinline__ void dcCoupleBody(S* Bc, S* Ff, const DCDev* __restri
             regulariseNeq<R>(neq, sc);
 #pragma unroll
             for (int q = 0; q < Q; ++q)
-                if (nd.rf >> q & 1u) Store<S>::store(Ff + (long long)q * c.Nf + nd.nf, eq[q] + aC2F * sc[q], la.hscale[q]);
+                if (q == lane && (nd.rf >> q & 1u)) Store<S>::store(Ff + (long long)q * c.Nf + nd.nf, eq[q] + aC2F * sc[q], la.hscale[q]);
         } else {
 #pragma unroll
             for (int q = 0; q < Q; ++q) neq[q] = X[q] - eq[q];
             rescaleNeq<R>(neq, c, true);
 #pragma unroll
             for (int q = 0; q < Q; ++q)
-                if (nd.rf >> q & 1u)
+                if (q == lane && (nd.rf >> q & 1u))
                     Store<S>::store(Ff + (long long)q * c.Nf + nd.nf, (nd.vc >> q & 1u) ? eq[q] + neq[q] : eq[q],
                                     la.hscale[q]);
         }
@@ -1453,12 +1460,12 @@ __device__ __forceinline__ void dcCoupleBody(S* Bc, S* Ff, const DCDev* __restri
         regulariseNeq<R>(neq, sc);
 #pragma unroll
         for (int q = 0; q < Q; ++q)
-            if (nd.rc >> q & 1u) Store<S>::store(Bc + (long long)q * c.Nc + nd.nc, eq[q] + sc[q], la.hscale[q]);
+            if (q == lane && (nd.rc >> q & 1u)) Store<S>::store(Bc + (long long)q * c.Nc + nd.nc, eq[q] + sc[q], la.hscale[q]);
     } else {
         rescaleNeq<R>(neq, c, false);
 #pragma unroll
         for (int q = 0; q < Q; ++q)
-            if (nd.rc >> q & 1u)
+            if (q == lane && (nd.rc >> q & 1u))
                 Store<S>::store(Bc + (long long)q * c.Nc + nd.nc, (nd.vf >> q & 1u) ? eq[q] + neq[q] : eq[q],
                                 la.hscale[q]);
     }
