@@ -988,20 +988,17 @@ size_t estimateBytes(const acp_case_desc& d) {
 static __device__ __align__(256) double g_windowScratch[(size_t)ACP_WINDOW_MAX_NODES * Q];
 
 namespace {
-std::mutex g_windowMutex;
-double* g_windowPtr[64] = {nullptr};
-
-// device address of g_windowScratch on `device` (current), looked up once per device
-int windowScratch(acp_handle* h, int device, double** out) {
-    if (device < 0 || device >= 64) return fail(h, ACP_ERR_UNSUPPORTED, "device index %d beyond 63", device);
-    std::lock_guard<std::mutex> lock(g_windowMutex);
-    if (!g_windowPtr[device]) {
-        double* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress((void**)&p, g_windowScratch);
-        if (e != cudaSuccess) return fail(h, ACP_ERR_CUDA, "cudaGetSymbolAddress: %s", cudaGetErrorString(e));
-        g_windowPtr[device] = p;
-    }
-    *out = g_windowPtr[device];
+// device address of g_windowScratch in the current context (the handle's
+// device is current).  It is looked up on every call rather than cached: the
+// address belongs to the context the module was loaded into, so after the
+// application destroys and recreates a device's context (cudaDeviceReset)
+// the next call gets the new address instead of a stale one.  The lookup
+// allocates nothing.
+int windowScratch(acp_handle* h, double** out) {
+    double* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress((void**)&p, g_windowScratch);
+    if (e != cudaSuccess) return fail(h, ACP_ERR_CUDA, "cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+    *out = p;
     return ACP_OK;
 }
 
@@ -1259,13 +1256,14 @@ int acp_read_populations_window(acp_handle* h, int level, long long begin, int c
     if (count < 0 || count > ACP_WINDOW_MAX_NODES)
         return fail(h, ACP_ERR_INVALID, "window of %d nodes: at most %d (ACP_WINDOW_MAX_NODES) per call", count,
                     ACP_WINDOW_MAX_NODES);
-    if (begin < 0 || begin + count > L.N)
-        return fail(h, ACP_ERR_INVALID, "window [%lld, %lld) outside the level's %lld nodes", begin, begin + count, L.N);
+    // count is in [0, ACP_WINDOW_MAX_NODES], so L.N - count cannot overflow
+    if (begin < 0 || begin > L.N - count)
+        return fail(h, ACP_ERR_INVALID, "window of %d nodes at %lld outside the level's %lld nodes", count, begin, L.N);
     if (count == 0) return ACP_OK;
     CU(h, cudaSetDevice(h->device));
     joinBatch(h);
     double* scratch = nullptr;
-    int s = windowScratch(h, h->device, &scratch);
+    int s = windowScratch(h, &scratch);
     if (s) return s;
     const int arr = level == 0 ? h->cur : 0;
     switch (h->d.storage) {
@@ -1302,15 +1300,21 @@ int acp_write_populations(acp_handle* h, int level, const double* in) {
 
 namespace {
 // checkpoint file: header, then per level both population arrays (storage
-// bytes) and the partner-strain records
+// bytes) and the partner-strain records.  The header names everything that
+// gives the stored values their meaning: the storage form with its shift and
+// FP16 scales, the operator and its options, the coupling and layout.
 struct CheckpointHeader {
     char magic[8];
     int abi, storage, levels, cur;
     long long steps;
     long long dims[2][3];
     long long slots[2];
+    int op, eqOrder, cubic, mrtWriteback, coupling, layout, scalingStyle, f2cFilter;
+    double shift;
+    float hscale[Q];
+    int pad;
 };
-constexpr char kCheckpointMagic[8] = {'A', 'C', 'P', 'C', 'K', 'P', 'T', '1'};
+constexpr char kCheckpointMagic[8] = {'A', 'C', 'P', 'C', 'K', 'P', 'T', '2'};
 
 CheckpointHeader checkpointHeader(const acp_handle* h) {
     CheckpointHeader c;
@@ -1327,7 +1331,26 @@ CheckpointHeader checkpointHeader(const acp_handle* h) {
         c.dims[l][2] = h->host[l].nz;
         c.slots[l] = h->dev[l].sg ? h->host[l].nSlots : 0;
     }
+    c.op = h->d.op;
+    c.eqOrder = h->d.eq_order;
+    c.cubic = h->d.cubic_mach;
+    c.mrtWriteback = h->d.mrt_writeback;
+    c.coupling = h->d.coupling;
+    c.layout = h->d.max_level == 1 ? h->d.layout : -1;
+    c.scalingStyle = h->d.scaling_style;
+    c.f2cFilter = h->d.f2c_filter;
+    c.shift = h->shift;
+    for (int q = 0; q < Q; ++q) c.hscale[q] = h->hscale[q];
     return c;
+}
+
+// the case fields of two headers agree (everything but parity and step count)
+bool sameCase(const CheckpointHeader& a, const CheckpointHeader& b) {
+    return a.abi == b.abi && a.storage == b.storage && a.levels == b.levels &&
+           std::memcmp(a.dims, b.dims, sizeof a.dims) == 0 && std::memcmp(a.slots, b.slots, sizeof a.slots) == 0 &&
+           a.op == b.op && a.eqOrder == b.eqOrder && a.cubic == b.cubic && a.mrtWriteback == b.mrtWriteback &&
+           a.coupling == b.coupling && a.layout == b.layout && a.scalingStyle == b.scalingStyle &&
+           a.f2cFilter == b.f2cFilter && a.shift == b.shift && std::memcmp(a.hscale, b.hscale, sizeof a.hscale) == 0;
 }
 
 // device regions of the state, in file order
@@ -1385,27 +1408,39 @@ int acp_checkpoint_load(acp_handle* h, const char* path) {
         return fail(h, ACP_ERR_INVALID, "%s is not a checkpoint of this engine", path);
     }
     const CheckpointHeader mine = checkpointHeader(h);
-    if (hd.abi != mine.abi || hd.storage != mine.storage || hd.levels != mine.levels ||
-        std::memcmp(hd.dims, mine.dims, sizeof hd.dims) != 0 || std::memcmp(hd.slots, mine.slots, sizeof hd.slots) != 0 ||
-        (hd.cur != 0 && hd.cur != 1) || hd.steps < 0) {
+    if (!sameCase(hd, mine) || (hd.cur != 0 && hd.cur != 1) || hd.steps < 0) {
         std::fclose(f);
-        return fail(h, ACP_ERR_INVALID, "%s holds a case of another storage form or level shape", path);
+        return fail(h, ACP_ERR_INVALID,
+                    "%s holds another case (storage form, shift, level shape, operator, coupling or layout)", path);
+    }
+    // the file must hold exactly the state regions: checked before any device write
+    const auto regions = checkpointRegions(h);
+    long long want = (long long)sizeof hd;
+    for (const auto& reg : regions) want += (long long)reg.second;
+    if (std::fseek(f, 0, SEEK_END) != 0 || std::ftell(f) != want || std::fseek(f, (long)sizeof hd, SEEK_SET) != 0) {
+        std::fclose(f);
+        return fail(h, ACP_ERR_INVALID, "%s is truncated or too long (%lld bytes expected)", path, want);
     }
     std::vector<char> buf;
-    for (const auto& reg : checkpointRegions(h)) {
+    for (const auto& reg : regions) {
         for (size_t o = 0; o < reg.second; o += kCheckpointChunk) {
             const size_t n = std::min(kCheckpointChunk, reg.second - o);
             buf.resize(n);
             if (std::fread(buf.data(), 1, n, f) != n) {
                 std::fclose(f);
-                return fail(h, ACP_ERR_INVALID, "%s is truncated", path);
+                return fail(h, ACP_ERR_INVALID, "reading %s failed; the case's state is undefined", path);
             }
-            CU(h, cudaMemcpy((char*)reg.first + o, buf.data(), n, cudaMemcpyHostToDevice));
+            const cudaError_t e = cudaMemcpy((char*)reg.first + o, buf.data(), n, cudaMemcpyHostToDevice);
+            if (e != cudaSuccess) {
+                std::fclose(f);
+                return fail(h, ACP_ERR_CUDA, "restore copy: %s; the case's state is undefined", cudaGetErrorString(e));
+            }
         }
     }
     std::fclose(f);
     h->cur = hd.cur;
     h->steps = hd.steps;
+    // probe series restart empty: the counter is reset, the step count continues
     if (h->dCounter) CU(h, cudaMemset(h->dCounter, 0, sizeof(int)));
     CU(h, cudaMemset(h->dErr, 0, sizeof(int)));
     return ACP_OK;

@@ -19,7 +19,26 @@ launches on, W warm-up steps, K timed steps, max over ranks.  The working set
 `--impl reference` times the CPU FP64 oracle (the restated reference, all
 host threads) on the same workload and prints the same JSON line shape.
 
+Two further modes reproduce the measurements behind the committed profiles
+and results (they print their own lines, not the bench JSON):
+
+  --profile   run --steps coarse steps of one case of the workload (flags
+              --op --storage --order --nx --ny --nz --levels --filter
+              --coupling; --batched N: the seeded batched cases in one batch
+              instead), for ncu; --timed N adds N steps kernel by kernel with
+              CUDA events and prints each kernel kind's device time
+  --study S   sweep: the operator and scheme sweep (1024 x 512 x 3, right half
+              refined, every operator x {STD, DC1} x {LAG, TOU} x nu in
+              {1e-5, 1e-4, 1e-3}, 3200 steps, reflection coefficient, FP32 errors
+              at nu = 1e-4); precision: the 256^3 precision form (HRR, centred
+              128^3-cell patch, transverse LODI, eps in {1e-2, 1e-4}, FP32 and
+              FP16 against FP64); convergence: the reflection coefficient of the
+              reference-sized pulse scaled to b = 6, 12, 24, 48 cells; --out
+              writes the JSON
+
 usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+       python bench.py --profile [--levels 1|2] [--op OP] [--storage S] [--steps K] [--timed N]
+       python bench.py --study sweep|precision|convergence [--steps K] [--out file.json]
 """
 import argparse
 import json
@@ -33,6 +52,9 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
+
+from acpulse_vclbm_b200 import analysis  # noqa: E402  (pure Python; loads no library)
+from acpulse_vclbm_b200.capi import F2C_FILTER, LAYOUT_BOX, lattice_units_case  # noqa: E402
 
 METRIC = "MLUPS & %HBM peak: FP32-shifted vs FP64 at ≤1e-5 rel err; p99 solve latency"
 
@@ -54,12 +76,19 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batched-cases", type=int, default=64, help="cases of the batched form (0: skip)")
     ap.add_argument("--serve-requests", type=int, default=16, help="requests of the serving form (0: skip)")
+    ap.add_argument("--order", type=int, default=3)
+    ap.add_argument("--storage", default="FP32-DEV")
+    ap.add_argument("--profile", action="store_true", help="profiling run of one case (see the module docstring)")
+    ap.add_argument("--timed", type=int, default=0, help="--profile: N steps kernel by kernel with CUDA events")
+    ap.add_argument("--batched", type=int, default=0, help="--profile: N seeded batched cases in one batch")
+    ap.add_argument("--study", default="", choices=["", "sweep", "precision", "convergence"])
+    ap.add_argument("--out", default="")
     return ap.parse_args()
 
 
 def workload(args, storage):
     from acpulse_vclbm_b200.capi import lattice_units_case
-    d = lattice_units_case(args.nx, args.ny, args.nz, op=args.op, nu_lu=args.nu, order=3,
+    d = lattice_units_case(args.nx, args.ny, args.nz, op=args.op, nu_lu=args.nu, order=args.order,
                            periodic=(False, True, True), eps=1e-3, b=24.0,
                            center=(args.nx / 4.0, args.ny / 2.0, 1.0), storage=storage)
     d.hybrid_sigma = 0.98
@@ -396,9 +425,210 @@ def run_engine(args):
         replicas.finish(dist)
 
 
+def run_profile(args):
+    """A few coarse steps of one case (or of the seeded batched cases), for
+    ncu; with --timed, per-kernel-kind device times by CUDA events."""
+    import ctypes as C
+    from acpulse_vclbm_b200 import engine
+    if args.batched:
+        from acpulse_vclbm_b200 import workloads
+        Ls = [engine.Lattice(d).init() for d in workloads.batched_cases(seed=2024, n=args.batched)]
+        B = engine.Batch(Ls)
+        B.step(args.steps)
+        B.sync()
+        print(B.info())
+        B.close()
+        for L in Ls:
+            L.close()
+        return
+    d = workload(args, args.storage)
+    L = engine.Lattice(d).init()
+    L.step(args.steps)
+    L.sync()
+    if args.timed:
+        km = (C.c_double * 5)()
+        engine.lib().acp_step_timed.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        engine.lib().acp_step_timed(L._h, args.timed, C.cast(km, C.c_void_p))
+        c, f = L.active_updates()
+        nodes = c + 2 * f
+        b = {"FP64": 8, "FP32-DEV": 4, "FP16-DEV": 2}[args.storage] * 38
+        print(f"{args.op} {args.storage} order {args.order} {args.nx}x{args.ny}x{args.nz} levels {args.levels}: "
+              f"collide {km[1]*1e3:.1f} us ({nodes * b / (km[1] * 1e-3) / 1e9:.0f} GB/s algorithmic), "
+              f"lodi {km[2]*1e3:.1f} us, coupling {km[3]*1e3:.1f} us, updates/step {nodes}", flush=True)
+    L.close()
+
+
+# ---------------------------------------------------------------------------
+# studies of the pulse configurations (--study), GPU, FP64 unless stated
+
+OPS5 = ["SRT", "MRT-GS", "MRT-RM", "RR", "HRR"]
+
+
+def _study_run(d, steps, probes):
+    from acpulse_vclbm_b200 import engine
+    L = engine.Lattice(d).init()
+    L.set_probes(probes)
+    L.step(steps)
+    L.sync()
+    s = L.probes()
+    p = [L.field(4, l) for l in range(d.max_level + 1)]
+    L.close()
+    return s, p
+
+
+def study_sweep(steps=3200, nx=1024, ny=512):
+    from acpulse_vclbm_b200.engine import AcpError
+    rows = []
+    uni = {}
+    p0 = None
+    for op in OPS5:
+        for nu in (1e-5, 1e-4, 1e-3):
+            du = analysis.interface_case(nx, ny, 3, op=op, nu=nu, eps=1e-3, b=24.0,
+                                         center=(nx / 4.0, ny / 2.0, 1.0), refined=False)
+            try:
+                uni[(op, nu)], _ = _study_run(du, steps, analysis.interface_probes(du))
+            except AcpError as e:
+                rows.append({"op": op, "nu": nu, "uniform_error": str(e)})
+                continue
+            p0 = du.density * du.speed_of_sound ** 2
+            for coupling in ("STD", "DC1"):
+                for filt in ("LAG", "TOU"):
+                    t0 = time.perf_counter()
+                    d = analysis.interface_case(nx, ny, 3, op=op, nu=nu, eps=1e-3, b=24.0,
+                                                center=(nx / 4.0, ny / 2.0, 1.0), filt=filt, coupling=coupling)
+                    try:
+                        s64, f64 = _study_run(d, steps, analysis.interface_probes(d))
+                    except AcpError as e:  # a numerical blow-up is a result of the sweep
+                        row = {"op": op, "nu": nu, "coupling": coupling, "filter": filt, "R": None,
+                               "error": str(e)}
+                        rows.append(row)
+                        print(json.dumps(row), flush=True)
+                        continue
+                    w = min(steps, analysis.window_steps(d))
+                    r = analysis.reflection_coefficient(s64[:, 0], uni[(op, nu)][:, 0], p0, w)
+                    row = {"op": op, "nu": nu, "coupling": coupling, "filter": filt, "R": r, "window_steps": w}
+                    if nu == 1e-4:
+                        d32 = analysis.interface_case(nx, ny, 3, op=op, nu=nu, eps=1e-3, b=24.0,
+                                                      center=(nx / 4.0, ny / 2.0, 1.0), filt=filt,
+                                                      coupling=coupling, storage="FP32-DEV")
+                        try:
+                            s32, f32 = _study_run(d32, steps, analysis.interface_probes(d32))
+                        except AcpError as e:
+                            row["fp32_error"] = str(e)
+                            rows.append(row)
+                            continue
+                        amp = d.ic_eps * d.density * d.speed_of_sound ** 2
+                        live = slice(0, nx // 2 + 1 + d.overlap)
+                        e = [f32[0][..., live] - f64[0][..., live], f32[1] - f64[1]]
+                        n = sum(x.size for x in e)
+                        row["fp32_l2_err_rel_amp"] = float(np.sqrt(sum((x ** 2).sum() for x in e) / n) / amp)
+                        row["fp32_max_err_rel_amp"] = float(max(np.abs(x).max() for x in e) / amp)
+                        row["fp32_probe_err_rel_amp"] = float(np.abs(s32 - s64).max() / amp)
+                        r32 = analysis.reflection_coefficient(s32[:, 0], uni[(op, nu)][:, 0], p0, w)
+                        row["fp32_R_rel_err"] = abs(r32 - r) / r
+                    row["seconds"] = time.perf_counter() - t0
+                    rows.append(row)
+                    print(json.dumps(row), flush=True)
+    return {"study": "operator and scheme sweep", "nx": nx, "ny": ny, "nz": 3, "steps": steps, "rows": rows}
+
+
+def study_precision_case(eps, storage, n=256):
+    lo, hi = n // 4, n // 4 + n // 2
+    d = lattice_units_case(n, n, n, op="HRR", nu_lu=1e-4, order=3, periodic=(False, False, False), eps=eps,
+                           b=12.0, center=(n / 2.0, n / 2.0, n / 2.0), storage=storage, ic_dims=3)
+    d.hybrid_sigma = 0.98
+    d.transverse = 1
+    d.max_level = 1
+    d.layout = LAYOUT_BOX
+    d.box_lo[:] = [lo, lo, lo]
+    d.box_hi[:] = [hi, hi, hi]
+    d.f2c_filter = F2C_FILTER["LAG"]
+    return d
+
+
+def study_precision(steps=300, n=256):
+    rows = []
+    c = n // 2
+    lo = n // 4
+    probes = [(1, 2 * (lo + 10), 2 * c, 2 * c), (0, lo - 10, c, c)]  # 10 cells inside and outside the patch face
+    for eps in (1e-2, 1e-4):
+        ref = None
+        for storage in ("FP64", "FP32-DEV", "FP16-DEV"):
+            d = study_precision_case(eps, storage, n)
+            t0 = time.perf_counter()
+            from acpulse_vclbm_b200 import engine
+            L = engine.Lattice(d).init()
+            L.set_probes(probes)
+            L.step(steps)
+            L.sync()
+            ms = (time.perf_counter() - t0) * 1e3 / steps
+            s = L.probes()
+            f = [L.field(4, l) for l in range(2)]
+            c_, fi = L.active_updates()
+            L.close()
+            amp = eps * d.density * d.speed_of_sound ** 2
+            row = {"eps": eps, "storage": storage, "steps": steps, "ms_per_step_incl_setup": ms,
+                   "updates_per_step": c_ + 2 * fi}
+            if ref is None:
+                ref = (s, f)
+            else:
+                live = np.ones(f[0].shape, dtype=bool)
+                live[lo + 1:lo + n // 2, lo + 1:lo + n // 2, lo + 1:lo + n // 2] = False  # covered coarse nodes
+                row["probe_err_rel_amp"] = float(np.abs(s - ref[0]).max() / amp)
+                row["field_max_err_rel_amp"] = float(max(np.abs(f[0] - ref[1][0])[live].max(),
+                                                         np.abs(f[1] - ref[1][1]).max()) / amp)
+            rows.append(row)
+            print(json.dumps(row), flush=True)
+    return {"study": "precision form", "n": n, "steps": steps, "rows": rows}
+
+
+
+
+def study_convergence(bs=(6.0, 12.0, 24.0, 48.0), ops=("SRT", "MRT-RM"), couplings=("STD", "DC1")):
+    """Reflection coefficient of the reference-sized pulse (128 x 64 x 3, b = 6)
+    scaled to b cells: grid, pulse, centre and steps times b / 6, lattice
+    viscosity 1e-3 x b / 6 (a physically similar refinement), FP64; the
+    observed order between successive b."""
+    rows = []
+    for op in ops:
+        for coupling in couplings:
+            prev = None
+            for b in bs:
+                s = b / 6.0
+                nx, ny = int(128 * s), int(64 * s)
+                kw = dict(op=op, nu=1e-3 * s, eps=1e-3, b=b, center=(32.0 * s, 32.0 * s, 1.0))
+                d = analysis.interface_case(nx, ny, 3, coupling=coupling, **kw)
+                du = analysis.interface_case(nx, ny, 3, refined=False, **kw)
+                w = analysis.window_steps(d)
+                s_ref, _ = _study_run(d, w, analysis.interface_probes(d)[:1])
+                s_uni, _ = _study_run(du, w, analysis.interface_probes(du)[:1])
+                r = analysis.reflection_coefficient(s_ref[:, 0], s_uni[:, 0], d.density * d.speed_of_sound ** 2, w)
+                row = {"op": op, "coupling": coupling, "b": b, "nx": nx, "ny": ny, "steps": w, "R": r}
+                if prev:
+                    row["order"] = float(np.log(prev / r) / np.log(2.0))
+                prev = r
+                rows.append(row)
+                print(json.dumps(row), flush=True)
+    return {"study": "reflection coefficient under refinement", "rows": rows}
+
+def run_study(args):
+    if args.study == "sweep":
+        res = study_sweep(steps=args.steps if args.steps != 200 else 3200)
+    elif args.study == "precision":
+        res = study_precision(steps=args.steps if args.steps != 200 else 300)
+    else:
+        res = study_convergence()
+    if args.out:
+        json.dump(res, open(args.out, "w"), indent=1)
+
+
 if __name__ == "__main__":
     a = parse()
-    if a.impl == "reference":
+    if a.profile:
+        run_profile(a)
+    elif a.study:
+        run_study(a)
+    elif a.impl == "reference":
         run_reference(a)
     else:
         run_engine(a)

@@ -167,10 +167,15 @@ int acp_write_populations(acp_handle* h, int level, const double* host_in);
  * acp_checkpoint_save waits for the case's queued steps first.
  * acp_checkpoint_load needs a handle created from a case of the same storage
  * form and level shapes and initialised (acp_init); it then continues bit-for-
- * bit as the saved run would have.  A mismatched file gives ACP_ERR_INVALID,
- * a file that cannot be read or written ACP_ERR_INVALID with the reason in
- * acp_last_error.  Probe series restart empty.  Cases stepped by a batch are
- * refused (ACP_ERR_STATE). */
+ * bit as the saved run would have.  The file names the case it belongs to
+ * (storage form with its density shift and FP16 scales, level shapes,
+ * operator, equilibrium order, cubic-Mach and MRT options, coupling, layout,
+ * restriction and scaling style); a file of another case, or one whose length
+ * is not exactly the state's, gives ACP_ERR_INVALID before anything on the
+ * device is overwritten.  A read or copy that fails after that point leaves
+ * the case's state undefined (ACP_ERR_INVALID / ACP_ERR_CUDA).  Probe series
+ * restart empty after a load while the step count continues.  Cases stepped
+ * by a batch are refused (ACP_ERR_STATE). */
 int acp_checkpoint_save(acp_handle* h, const char* path);
 int acp_checkpoint_load(acp_handle* h, const char* path);
 /* Legacy structured-points VTK of every level with the fields the reference
@@ -228,11 +233,13 @@ int acp_boundary_wiring(const acp_case_desc* d, long long* rows, long long max_r
  * ACP_WINDOW_MAX_NODES x 19 doubles (about 5 MB) built into the library; every
  * device that loads the library holds it until the process exits.  Larger
  * windows are rejected (ACP_ERR_INVALID): read a large level window by window.
- * The first call on a device looks up that array's device address (once per
- * device), so make the first call before any stream capture on the device.
- * All calls share the array: calls that overlap on the GPU (other threads or
- * streams) race and must be serialised by the caller.  Nothing in it needs to
- * start at zero; each call overwrites the part it reads back. */
+ * Every call looks up that array's device address in the device's current
+ * context (with the handle's device current), so the address stays valid if
+ * the application destroys and recreates the context (cudaDeviceReset); the
+ * call synchronises the handle's stream, so it is not made inside a stream
+ * capture.  All calls share the array: calls that overlap on the GPU (other
+ * threads or streams) race and must be serialised by the caller.  Nothing in
+ * it needs to start at zero; each call overwrites the part it reads back. */
 int acp_read_populations_window(acp_handle* h, int level, long long node_begin, int node_count, double* host_out);
 /* ---- batched form --------------------------------------------------------
  * Many initialised cases of uneven sizes, operators, storage forms and

@@ -16,11 +16,15 @@ _LIB = None
 
 
 def build():
-    """Compile oracle/liboracle.so (and, where the reference checkout exists,
-    the reference's single-level binary oracle/_ref/acp_ref)."""
+    """Compile oracle/liboracle.so (and, where the reference's sources are
+    present, its single-level binary oracle/_ref/acp_ref).  The sources are
+    found at the recipe's default location (oracle/ref_build/Makefile, REF) or
+    at $ACP_REFERENCE_SRC."""
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
-    if os.path.isdir("/root/reference/acPulse_vcLBM"):
-        subprocess.run(["make", "-s", "-C", os.path.join(_HERE, "ref_build")], check=True)
+    ref = os.environ.get("ACP_REFERENCE_SRC")
+    cmd = ["make", "-s", "-C", os.path.join(_HERE, "ref_build")] + ([f"REF={ref}"] if ref else [])
+    if subprocess.run(cmd + ["have-ref"], capture_output=True).returncode == 0:
+        subprocess.run(cmd, check=True)
 
 
 def lib():

@@ -94,3 +94,59 @@ def test_restart_refuses_another_level_shape(tmp_path):
         c.load_checkpoint(str(tmp_path / "missing.ckpt"))
     b.close()
     c.close()
+
+
+def test_restart_refuses_another_case_and_a_truncated_file(tmp_path):
+    """A file of another operator, or a cut-off file, is refused before the
+    device state is touched: the handle keeps stepping as before."""
+    path = str(tmp_path / "case.ckpt")
+    a = engine.Lattice(two_level("HRR", "FP32-DEV")).init()
+    a.step(3)
+    a.save_checkpoint(path)
+    a.close()
+    b = engine.Lattice(two_level("RR", "FP32-DEV")).init()  # same shapes, another operator
+    b.step(2)
+    b.sync()
+    before = b.populations(0)
+    with pytest.raises(engine.AcpError) as e:
+        b.load_checkpoint(path)
+    assert e.value.status == -1
+    cut = str(tmp_path / "cut.ckpt")
+    with open(path, "rb") as src, open(cut, "wb") as dst:
+        data = src.read()
+        dst.write(data[:len(data) - 100])
+    c = engine.Lattice(two_level("HRR", "FP32-DEV")).init()
+    c.step(2)
+    c.sync()
+    keep = c.populations(1)
+    with pytest.raises(engine.AcpError):
+        c.load_checkpoint(cut)
+    assert np.array_equal(c.populations(1), keep) and c.steps_done() == 2
+    assert np.array_equal(b.populations(0), before)
+    b.close()
+    c.close()
+
+
+def test_probe_series_restart_after_load(tmp_path):
+    """Probe series restart empty after a load; the step count continues."""
+    path = str(tmp_path / "case.ckpt")
+    d = two_level("SRT", "FP64")
+    a = engine.Lattice(d).init()
+    a.set_probes([(0, 8, 10, 1)])
+    a.step(5)
+    a.save_checkpoint(path)
+    a.step(4)
+    a.sync()
+    ref = a.probes()
+    a.close()
+    b = engine.Lattice(d).init()
+    b.set_probes([(0, 8, 10, 1)])
+    b.step(1)
+    b.load_checkpoint(path)
+    b.step(4)
+    b.sync()
+    got = b.probes()
+    assert b.steps_done() == 9
+    b.close()
+    assert got.shape == (4, 1)
+    assert np.array_equal(got, ref[5:9])

@@ -29,20 +29,37 @@ def _bind():
     return lib
 
 
-@pytest.mark.parametrize("storage", ["FP32-DEV", "FP64"])
-def test_window_read_matches_full_read_twice(storage):
+def _two_level(storage):
+    from acpulse_vclbm_b200.capi import F2C_FILTER, LAYOUT_BOX
+    d = lattice_units_case(32, 12, 3, op="HRR", nu_lu=1e-3, order=3, periodic=(False, True, True), eps=1e-3, b=3.0,
+                           center=(14.0, 6.0, 1.0), storage=storage)
+    d.hybrid_sigma = 0.98
+    d.max_level = 1
+    d.layout = LAYOUT_BOX
+    d.box_lo[:] = [16, 0, 0]
+    d.box_hi[:] = [31, 11, 2]
+    d.f2c_filter = F2C_FILTER["LAG"]
+    return d
+
+
+@pytest.mark.parametrize("storage,level", [("FP32-DEV", 0), ("FP64", 0), ("FP16-DEV", 0),
+                                           ("FP32-DEV", 1), ("FP16-DEV", 1)])
+def test_window_read_matches_full_read_twice(storage, level):
     lib = _bind()
-    d = lattice_units_case(40, 24, 3, op="HRR", nu_lu=1e-3, order=3, eps=1e-3, b=4.0, center=(14.0, 12.0, 1.0),
-                           storage=storage)
+    if level == 0:
+        d = lattice_units_case(40, 24, 3, op="HRR", nu_lu=1e-3, order=3, eps=1e-3, b=4.0, center=(14.0, 12.0, 1.0),
+                               storage=storage)
+    else:  # the fine level of a two-level case, whose state sits in its first array between coarse steps
+        d = _two_level(storage)
     L = engine.Lattice(d).init()
     L.step(7)
     L.sync()
-    full = L.populations().reshape(19, -1)
+    full = L.populations(level).reshape(19, -1)
     n = full.shape[1]
     windows = [(5, 1000), (n - 777, 777)]  # two calls in a row, the second at the end of the level
     for begin, count in windows:
         out = np.full((19, count), np.nan)
-        s = lib.acp_read_populations_window(L._h, 0, begin, count, out.ctypes.data)
+        s = lib.acp_read_populations_window(L._h, level, begin, count, out.ctypes.data)
         assert s == ACP_OK, lib.acp_last_error(L._h)
         np.testing.assert_allclose(out, full[:, begin:begin + count], rtol=0, atol=1e-14)
     L.close()
@@ -56,4 +73,7 @@ def test_window_limits_are_enforced():
     assert lib.acp_read_populations_window(L._h, 0, 0, WINDOW_MAX + 1, out.ctypes.data) == ACP_ERR_INVALID
     assert b"ACP_WINDOW_MAX_NODES" in lib.acp_last_error(L._h)
     assert lib.acp_read_populations_window(L._h, 0, 40 * 24 * 3 - 2, 4, out.ctypes.data) == ACP_ERR_INVALID
+    # a begin near the largest 64-bit value is refused, not wrapped around
+    assert lib.acp_read_populations_window(L._h, 0, (1 << 63) - 2, 4, out.ctypes.data) == ACP_ERR_INVALID
+    assert lib.acp_read_populations_window(L._h, 0, -1, 4, out.ctypes.data) == ACP_ERR_INVALID
     L.close()
