@@ -38,7 +38,7 @@ def up_to_date():
 def build_host():
     """The drop-in C++ Control/Lattice and the reference-style driver, linked to libacp_cuda.so."""
     host = os.path.join(HERE, "host")
-    srcs = [os.path.join(host, f) for f in ("Control.cpp", "Lattice.cpp", "acp_main.cpp")]
+    srcs = [os.path.join(host, f) for f in ("Control.cpp", "Lattice.cpp", "Node.cpp", "acp_main.cpp")]
     subprocess.run([HOSTCXX, "-O2", "-std=c++17", "-o", MAIN, *srcs, "-L" + HERE, "-lacp_cuda",
                     "-Wl,-rpath,$ORIGIN"], check=True)
     return MAIN

@@ -102,6 +102,41 @@ __global__ void __launch_bounds__(TX * TY, TiledMinBlocks<R>::value)
     }
 }
 
+// the y-marching collide (periodic z of at most MARCH_MAX_NZ planes) over
+// (case, x tile, y chunk) items; every case of the group has the same number
+// of z planes on the level (blockDim.y)
+template <typename S, typename R, int OP, int ORDER, bool CUBIC>
+__device__ __forceinline__ void kbMarchBody(const BatchCase<S>* __restrict__ cases, const WorkItem* __restrict__ items,
+                                            int n, int level, int fineSrc, int flip) {
+    __shared__ LevelArgs<S> sa;
+    extern __shared__ __align__(16) unsigned char marchSmem[];
+    for (int w = blockIdx.x; w < n; w += gridDim.x) {
+        const WorkItem it = items[w];
+        const BatchCase<S>& bc = cases[it.c];
+        stage(&sa, &bc.lv[level].a[srcOf(bc, level, fineSrc, flip)]);
+        __syncthreads();
+        if (MarchPrefetch<R>::value)
+            marchBodyPrefetch<S, R, OP, ORDER, CUBIC>(sa, bc.lv[level].zChunk, it.bx, it.by,
+                                                      reinterpret_cast<MomR<R>*>(marchSmem));
+        else
+            marchBody<S, R, OP, ORDER, CUBIC>(sa, bc.lv[level].zChunk, it.bx, it.by,
+                                              reinterpret_cast<MomR<R>*>(marchSmem));
+        __syncthreads();
+    }
+}
+template <typename S, typename R, int OP, int ORDER, bool CUBIC>
+__global__ void __launch_bounds__(MARCH_TX * MARCH_MAX_NZ, TiledMinBlocks<R>::value)
+    kb_march(const BatchCase<S>* __restrict__ cases, const WorkItem* __restrict__ items, int n, int level, int fineSrc,
+             int flip) {
+    kbMarchBody<S, R, OP, ORDER, CUBIC>(cases, items, n, level, fineSrc, flip);
+}
+template <typename S, typename R, int OP, int ORDER, bool CUBIC>
+__global__ void __maxnreg__(ACP_MARCH_REGS_F32)
+    kb_march_f32(const BatchCase<S>* __restrict__ cases, const WorkItem* __restrict__ items, int n, int level,
+                 int fineSrc, int flip) {
+    kbMarchBody<S, R, OP, ORDER, CUBIC>(cases, items, n, level, fineSrc, flip);
+}
+
 template <typename S, int ORDER>
 __global__ void __launch_bounds__(128) kb_lodi(const BatchCase<S>* __restrict__ cases,
                                                const WorkItem* __restrict__ items, int n, int level, int fineSrc,
@@ -244,6 +279,28 @@ KbCollide<S> pickBatchCollide(const acp_case_desc& d) {
     }
 }
 
+template <typename S, typename R, int OP, int ORDER, bool CUBIC>
+KbCollide<S> batchMarchKernel() {
+    if constexpr (sizeof(R) == 8) return kb_march<S, R, OP, ORDER, CUBIC>;
+    else return kb_march_f32<S, R, OP, ORDER, CUBIC>;
+}
+template <typename S, typename R>
+KbCollide<S> pickBatchMarch(const acp_case_desc& d) {
+    const bool cubic = d.cubic_mach != 0;
+    if (d.op == OP_RR) {
+        switch (d.eq_order) {
+            case 2: return batchMarchKernel<S, R, OP_RR, 2, true>();
+            case 3: return batchMarchKernel<S, R, OP_RR, 3, true>();
+            default: return batchMarchKernel<S, R, OP_RR, 4, true>();
+        }
+    }
+    switch (d.eq_order) {
+        case 2: return cubic ? batchMarchKernel<S, R, OP_HRR, 2, true>() : batchMarchKernel<S, R, OP_HRR, 2, false>();
+        case 3: return cubic ? batchMarchKernel<S, R, OP_HRR, 3, true>() : batchMarchKernel<S, R, OP_HRR, 3, false>();
+        default: return cubic ? batchMarchKernel<S, R, OP_HRR, 4, true>() : batchMarchKernel<S, R, OP_HRR, 4, false>();
+    }
+}
+
 template <typename S>
 KbLodi<S> pickBatchLodi(int o) { return o == 2 ? kb_lodi<S, 2> : (o == 3 ? kb_lodi<S, 3> : kb_lodi<S, 4>); }
 template <typename S, typename R>
@@ -253,12 +310,24 @@ KbCoinc<S, R> pickBatchCoinc(int o) {
 template <typename S, typename R>
 KbF2C<S> pickBatchF2C(int o) { return o == 2 ? kb_f2c<S, R, 2> : (o == 3 ? kb_f2c<S, R, 3> : kb_f2c<S, R, 4>); }
 
+// z planes of a level when its neighbour-moment collide is the y-marching
+// one (those planes are the block's second dimension), else 0
+int marchPlanes(const acp_handle* h, int l) {
+    const LevelHost& L = h->host[l];
+    return needsMoments(h->d) && marchesY(L) ? L.nz : 0;
+}
+
+using GroupKey = std::tuple<int, int, int, int, int, int, int, int, int>;
+
 // the kernel-template key of a case: cases with equal keys form one group
-std::tuple<int, int, int, int, int, int, int> groupKey(const acp_case_desc& d, int levels) {
+GroupKey groupKey(const acp_handle* h) {
+    const acp_case_desc& d = h->d;
+    const int levels = (int)h->host.size();
     const bool mrt = d.op == OP_MRT_GS || d.op == OP_MRT_RM;
     const int op = (mrt && !d.mrt_writeback) ? -1 : d.op;  // the reference's MRT no-op forms share a kernel
     return std::make_tuple(d.storage, op, mrt ? 0 : d.eq_order, d.cubic_mach && (d.op == OP_RR || d.op == OP_HRR),
-                           mrt ? d.mrt_writeback : 0, levels, levels == 2 ? (d.coupling != ACP_COUPLING_STD) : 0);
+                           mrt ? d.mrt_writeback : 0, levels, levels == 2 ? (d.coupling != ACP_COUPLING_STD) : 0,
+                           marchPlanes(h, 0), levels == 2 ? marchPlanes(h, 1) : 0);
 }
 
 struct Range {
@@ -277,6 +346,7 @@ struct Group {
     int levels = 1;
     bool direct = false;
     bool tiled = false;
+    int marchNz[2] = {0, 0};  // per level: z planes of the y-marching collide (0: not marching)
     void* dCases = nullptr;
     WorkItem* dItems = nullptr;
     // item ranges per phase
@@ -285,7 +355,7 @@ struct Group {
     cudaEvent_t joined = nullptr;
     cudaStream_t side = nullptr;  // the coarse step beside the first fine sub-step
     cudaEvent_t sideFork = nullptr, sideJoin = nullptr;
-    int resident[9] = {0};  // resident blocks per SM of each batch kernel (occupancy)
+    int resident[9] = {0};  // resident blocks per SM of each batch kernel (occupancy; 6, 7: march per level)
 };
 
 }  // namespace acp
@@ -346,7 +416,11 @@ BatchCase<S> caseRecord(const acp_handle* h, int chunkScale, int base) {
         L.nLodiX = h->dev[l].nLodiX;
         L.nLodiZY = h->dev[l].nLodiZY;
         const LevelHost& H = h->host[l];
-        L.zChunk = (H.per[2] && H.nz <= 3) ? H.nz : std::min(H.nz, tiledChunk(H) * chunkScale);
+        // the y-marching collide takes its y chunk in the same field
+        if (marchPlanes(h, (int)l))
+            L.zChunk = std::min(H.ny, marchChunkFor(H, h->d.storage == ACP_STORE_F64 ? 8 : 4) * chunkScale);
+        else
+            L.zChunk = (H.per[2] && H.nz <= 3) ? H.nz : std::min(H.nz, tiledChunk(H) * chunkScale);
     }
     if (h->host.size() == 2) {
         r.cpl = couplingArgs(h);
@@ -365,7 +439,7 @@ BatchCase<S> caseRecord(const acp_handle* h, int chunkScale, int base) {
 }
 
 // blocks of a level's collide launch that hold at least one live node
-void collideItems(const LevelHost& L, int c, bool tiled, int zChunk, std::vector<WorkItem>& out) {
+void collideItems(const LevelHost& L, int c, bool tiled, bool march, int zChunk, std::vector<WorkItem>& out) {
     auto live = [&](int i0, int i1, int j0, int j1, int k0, int k1) {
         for (int k = k0; k < k1; ++k)
             for (int j = j0; j < j1; ++j) {
@@ -375,7 +449,15 @@ void collideItems(const LevelHost& L, int c, bool tiled, int zChunk, std::vector
             }
         return false;
     };
-    if (tiled) {
+    if (march) {
+        // x tiles of MARCH_STEP collided nodes, y chunks of zChunk rows, whole z columns
+        const int gx = (L.nx + MARCH_STEP - 1) / MARCH_STEP, gy = (L.ny + zChunk - 1) / zChunk;
+        for (int by = 0; by < gy; ++by)
+            for (int bx = 0; bx < gx; ++bx)
+                if (live(bx * MARCH_STEP, std::min(L.nx, bx * MARCH_STEP + MARCH_STEP), by * zChunk,
+                         std::min(L.ny, by * zChunk + zChunk), 0, L.nz))
+                    out.push_back({c, bx, by, 0});
+    } else if (tiled) {
         const int gx = (L.nx + TX - 1) / TX, gy = (L.ny + TY - 1) / TY, gz = (L.nz + zChunk - 1) / zChunk;
         for (int bz = 0; bz < gz; ++bz)
             for (int by = 0; by < gy; ++by)
@@ -433,7 +515,7 @@ int buildGroup(acp_batch* b, Group& g) {
     };
     for (int l = 0; l < g.levels; ++l) {
         phase(g.collide[l], [&](int c, const acp_handle* h) {
-            collideItems(h->host[l], c, g.tiled, recs[c].lv[l].zChunk, items);
+            collideItems(h->host[l], c, g.tiled, g.marchNz[l] > 0, recs[c].lv[l].zChunk, items);
         });
         phase(g.lodiX[l], [&](int c, const acp_handle* h) { blockItems(c, h->dev[l].nLodiX * LODI_TPN, 128, items); });
         phase(g.lodiZY[l], [&](int c, const acp_handle* h) { blockItems(c, h->dev[l].nLodiZY * LODI_TPN, 128, items); });
@@ -484,6 +566,15 @@ int occupancy(Group& g, const acp_case_desc& d) {
     g.resident[3] = occ((const void*)pickBatchCoinc<S, R>(o), 128);
     g.resident[4] = occ((const void*)kb_c2f_interp<S, R>, 256);
     g.resident[5] = occ((const void*)pickBatchF2C<S, R>(o), 128);
+    for (int l = 0; l < 2; ++l)
+        if (g.marchNz[l]) {
+            int m = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&m, (const void*)pickBatchMarch<S, R>(d),
+                                                              MARCH_TX * g.marchNz[l],
+                                                              marchSmemBytes<R>(g.marchNz[l])) != cudaSuccess)
+                m = 1;
+            g.resident[6 + l] = std::max(1, m);
+        }
     return ACP_OK;
 }
 
@@ -500,7 +591,11 @@ void enqueueGroup(acp_batch* b, Group& g, int flip) {
     KbLodi<S> lodi = pickBatchLodi<S>(o);
     const dim3 cblock = g.tiled ? dim3(TX, TY) : dim3(128);
     auto levelStep = [&](int l, int fineSrc, cudaStream_t ls) {
-        if (g.collide[l].count)
+        if (g.collide[l].count && g.marchNz[l])
+            pickBatchMarch<S, R>(d)<<<gridFor(b, g.collide[l].count, g.resident[6 + l]), dim3(MARCH_TX, g.marchNz[l]),
+                                      marchSmemBytes<R>(g.marchNz[l]), ls>>>(cs, it + g.collide[l].off,
+                                                                             g.collide[l].count, l, fineSrc, flip);
+        else if (g.collide[l].count)
             collide<<<gridFor(b, g.collide[l].count, g.resident[0]), cblock, 0, ls>>>(cs, it + g.collide[l].off,
                                                                                      g.collide[l].count, l, fineSrc,
                                                                                      flip);
@@ -665,13 +760,13 @@ int acp_batch_create(acp_handle* const* cases, int n, acp_batch** out) {
     BCU(b, cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
     BCU(b, cudaEventCreateWithFlags(&b->forked, cudaEventDisableTiming));
     BCU(b, cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming));
-    std::map<std::tuple<int, int, int, int, int, int, int>, int> index;
+    std::map<GroupKey, int> index;
     for (int i = 0; i < n; ++i) {
         acp_handle* h = cases[i];
         BCU(b, cudaStreamSynchronize(h->stream));  // the case's own pending work
         b->cases.push_back(h);
         const int levels = (int)h->host.size();
-        auto key = groupKey(h->d, levels);
+        auto key = groupKey(h);
         auto f = index.find(key);
         if (f == index.end()) {
             Group g;
@@ -679,6 +774,7 @@ int acp_batch_create(acp_handle* const* cases, int n, acp_batch** out) {
             g.levels = levels;
             g.direct = levels == 2 && h->d.coupling != ACP_COUPLING_STD;
             g.tiled = needsMoments(h->d);
+            for (int l = 0; l < levels; ++l) g.marchNz[l] = marchPlanes(h, l);
             index[key] = (int)b->groups.size();
             b->groups.push_back(g);
             f = index.find(key);

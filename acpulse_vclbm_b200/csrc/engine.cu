@@ -207,10 +207,29 @@ int wireLevel(acp_handle* h, LevelHost& L, int level) {
         for (int a = 0; a < 3; ++a) fc[a] = (lodiLo[a] && c[a] == 0) ? -1 : ((lodiHi[a] && c[a] == dims[a] - 1) ? 1 : 0);
         return fc[0] || fc[1] || fc[2];
     };
-    const std::vector<long long> faceNodes = scanNodes(L, [&](long long n, int i, int j, int k) {
-        int fc[3];
-        return L.code[n] != CODE_DEAD && faceOf(i, j, k, fc);
-    });
+    // live nodes on the LODI faces, in node order: a row on a y or z face is
+    // scanned whole, any other row holds at most its two x-face nodes
+    std::vector<long long> faceNodes;
+    {
+        const int T = std::max(1, std::min(16, (int)std::thread::hardware_concurrency()));
+        std::vector<std::vector<long long>> part(T);
+        forRows((long long)L.ny * L.nz, [&](long long r0, long long r1, int t) {
+            for (long long r = r0; r < r1; ++r) {
+                const int j = (int)(r % L.ny), k = (int)(r / L.ny);
+                const bool whole = (lodiLo[1] && j == 0) || (lodiHi[1] && j == L.ny - 1) || (lodiLo[2] && k == 0) ||
+                                   (lodiHi[2] && k == L.nz - 1);
+                const long long row = r * L.nx;
+                if (whole) {
+                    for (int i = 0; i < L.nx; ++i)
+                        if (L.code[row + i] != CODE_DEAD) part[t].push_back(row + i);
+                    continue;
+                }
+                if (lodiLo[0] && L.code[row] != CODE_DEAD) part[t].push_back(row);
+                if (lodiHi[0] && L.nx > 1 && L.code[row + L.nx - 1] != CODE_DEAD) part[t].push_back(row + L.nx - 1);
+            }
+        });
+        for (auto& v : part) faceNodes.insert(faceNodes.end(), v.begin(), v.end());
+    }
     for (const long long n : faceNodes) {
                 const int i = (int)(n % L.nx), j = (int)((n / L.nx) % L.ny), k = (int)(n / ((long long)L.nx * L.ny));
                 int fc[3];
@@ -283,42 +302,55 @@ struct CouplingGeom {
         const int sg = inside ? 1 : -1;
         for (int a = 0; a < 3; ++a) f[a] = (loIf[a] && c[a] == cl[a]) ? -sg : ((hiIf[a] && c[a] == ch[a]) ? sg : 0);
     }
-    bool dead(const int* c) const {
-        if (inside) return false;
-        for (int a = 0; a < 3; ++a) {
-            const int lo = loIf[a] ? cl[a] + 1 : cl[a], hi = hiIf[a] ? ch[a] - 1 : ch[a];
-            if (c[a] < lo || c[a] > hi) return false;
-        }
-        return true;
-    }
-    bool coupling(const int* c) const {
-        bool within = true, face = false;
-        for (int a = 0; a < 3; ++a) {
-            if (c[a] < cl[a] || c[a] > ch[a]) within = false;
-            if ((loIf[a] && c[a] == cl[a]) || (hiIf[a] && c[a] == ch[a])) face = true;
-        }
-        return within && face && !dead(c);
-    }
 };
 
 // node classes of a level from its coupling geometry: dead nodes, coupling
 // nodes (pushing everywhere when the level lies outside its box, where the
-// covered nodes exist in the array, else only within the level)
+// covered nodes exist in the array, else only within the level).  Row by row
+// (j, k): a row crossing the box's interior holds at most one dead segment and
+// a coupling node at each interface x face; a row on a y or z interface face
+// is coupling over the whole x extent of the box; classes are then set per
+// segment instead of testing every node.
 void markLevel(LevelHost& L, const CouplingGeom& g) {
     L.code.assign(L.N, CODE_FLUID);
+    auto setCoupling = [&](long long n, const int* c) {
+        int f[3];
+        g.normal(c, f);
+        L.code[n] = (uint8_t)(CODE_IFACE0 + (g.inside ? faceCode(f[0], f[1], f[2]) : CODE_FLUID));
+    };
+    // strictly-inside range of an axis (the covered nodes of a level outside its box)
+    int dlo[3], dhi[3];
+    for (int a = 0; a < 3; ++a) {
+        dlo[a] = g.loIf[a] ? g.cl[a] + 1 : g.cl[a];
+        dhi[a] = g.hiIf[a] ? g.ch[a] - 1 : g.ch[a];
+    }
     forRows((long long)L.ny * L.nz, [&](long long r0, long long r1, int) {
-        for (long long r = r0; r < r1; ++r)
-            for (int i = 0; i < L.nx; ++i) {
-                const int c[3] = {i, (int)(r % L.ny), (int)(r / L.ny)};
-                const long long n = r * L.nx + i;
-                if (g.dead(c)) {
-                    L.code[n] = CODE_DEAD;
-                } else if (g.coupling(c)) {
-                    int f[3];
-                    g.normal(c, f);
-                    L.code[n] = (uint8_t)(CODE_IFACE0 + (g.inside ? faceCode(f[0], f[1], f[2]) : CODE_FLUID));
+        for (long long r = r0; r < r1; ++r) {
+            const int j = (int)(r % L.ny), k = (int)(r / L.ny);
+            if (j < g.cl[1] || j > g.ch[1] || k < g.cl[2] || k > g.ch[2]) continue;  // row misses the box
+            const long long row = r * L.nx;
+            const bool faceRow = (g.loIf[1] && j == g.cl[1]) || (g.hiIf[1] && j == g.ch[1]) ||
+                                 (g.loIf[2] && k == g.cl[2]) || (g.hiIf[2] && k == g.ch[2]);
+            const bool innerRow = j >= dlo[1] && j <= dhi[1] && k >= dlo[2] && k <= dhi[2];
+            if (faceRow) {
+                // a face coordinate lies outside the strictly-inside range: nothing dead
+                for (int i = std::max(0, g.cl[0]); i <= std::min(L.nx - 1, g.ch[0]); ++i) {
+                    const int c[3] = {i, j, k};
+                    setCoupling(row + i, c);
                 }
+                continue;
             }
+            if (!g.inside && innerRow && dlo[0] <= dhi[0])
+                std::fill(L.code.begin() + row + std::max(0, dlo[0]), L.code.begin() + row + std::min(L.nx - 1, dhi[0]) + 1,
+                          CODE_DEAD);
+            const int xs[2] = {g.loIf[0] ? g.cl[0] : -1, g.hiIf[0] ? g.ch[0] : -1};
+            for (int e = 0; e < 2; ++e) {
+                const int i = xs[e];
+                if (i < 0 || i >= L.nx || (e == 1 && i == xs[0])) continue;
+                const int c[3] = {i, j, k};
+                setCoupling(row + i, c);
+            }
+        }
     });
 }
 
@@ -546,11 +578,9 @@ int buildTwoLevel(acp_handle* h) {
     h->partner = !direct && (d.op == OP_HRR || (d.op == OP_RR && d.cubic_mach));
     h->nbHost.clear();
     if (h->partner) {
-        F.slot.assign(F.N, -1);
-        for (size_t i = 0; i < h->c2fHost.size(); ++i) F.slot[h->c2fHost[i].n] = (int)i;
+        // record t of a level's coupling list is the partner strain of its node
+        // (the node -> record map is scattered on the device, k_scatter_slots)
         F.nSlots = (int)h->c2fHost.size();
-        C.slot.assign(C.N, -1);
-        for (size_t i = 0; i < h->f2cHost.size(); ++i) C.slot[h->f2cHost[i].n] = (int)i;
         C.nSlots = (int)h->f2cHost.size();
         auto regular = [](const LevelHost& L, long long n) { return L.code[n] < CODE_IFACE0; };
         for (int t = 0; t < h->nCoinc; ++t) {
@@ -689,6 +719,30 @@ TiledFn<S> pickTiled(const acp_case_desc& d) {
     }
 }
 
+// the march kernel of a case: FP64 compute with its launch bound, FP32
+// compute (FP32 and FP16 storage) with its direct register cap
+template <typename S, typename R, int OP, int ORDER, bool CUBIC>
+TiledFn<S> marchKernel() {
+    if constexpr (sizeof(R) == 8) return k_collide_push_march<S, R, OP, ORDER, CUBIC>;
+    else return k_collide_push_march_f32<S, R, OP, ORDER, CUBIC>;
+}
+template <typename S, typename R>
+TiledFn<S> pickMarch(const acp_case_desc& d) {
+    const bool cubic = d.cubic_mach != 0;
+    if (d.op == OP_RR) {
+        switch (d.eq_order) {
+            case 2: return marchKernel<S, R, OP_RR, 2, true>();
+            case 3: return marchKernel<S, R, OP_RR, 3, true>();
+            default: return marchKernel<S, R, OP_RR, 4, true>();
+        }
+    }
+    switch (d.eq_order) {
+        case 2: return cubic ? marchKernel<S, R, OP_HRR, 2, true>() : marchKernel<S, R, OP_HRR, 2, false>();
+        case 3: return cubic ? marchKernel<S, R, OP_HRR, 3, true>() : marchKernel<S, R, OP_HRR, 3, false>();
+        default: return cubic ? marchKernel<S, R, OP_HRR, 4, true>() : marchKernel<S, R, OP_HRR, 4, false>();
+    }
+}
+
 template <typename S>
 using LodiFn = void (*)(const S*, S*, const BNodeDev*, int, LodiArgs, LevelArgs<S>);
 
@@ -727,7 +781,11 @@ int enqueueLevelStep(acp_handle* h, int l, int src, PhaseTimer* tm = nullptr, cu
     LevelArgs<S> a = levelArgs<S>(h, l, src);
     const int bx = 128;
     if (tm) tm->mark(-1);
-    if (needsMoments(h->d)) {
+    if (needsMoments(h->d) && marchesY(L)) {
+        const int chunk = marchChunkFor(L, sizeof(R));
+        dim3 grid((L.nx + MARCH_STEP - 1) / MARCH_STEP, (L.ny + chunk - 1) / chunk);
+        pickMarch<S, R>(h->d)<<<grid, dim3(MARCH_TX, L.nz), marchSmemBytes<R>(L.nz), st>>>(a, chunk);
+    } else if (needsMoments(h->d)) {
         const int chunk = tiledChunkFor(L, TiledMinBlocks<R>::value);
         dim3 grid((L.nx + TX - 1) / TX, (L.ny + TY - 1) / TY, (L.nz + chunk - 1) / chunk);
         pickTiled<S, R>(h->d)<<<grid, dim3(TX, TY), 0, st>>>(a, chunk);
@@ -944,6 +1002,14 @@ void launchInit(acp_handle* h, int l) {
     k_init<S><<<gridOf(L, 128), 128, 0, h->stream>>>(a, ia);
 }
 
+// node -> coupling record map of a level: slot[recs[t].n] = t (the map is
+// -1 elsewhere, set by a memset before)
+template <typename Rec>
+__global__ void k_scatter_slots(int* slot, const Rec* recs, int n) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) slot[recs[t].n] = t;
+}
+
 int devAlloc(acp_handle* h, void** p, size_t bytes) {
     cudaError_t e = cudaMalloc(p, bytes);
     if (e != cudaSuccess) return fail(h, ACP_ERR_NOMEM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
@@ -1136,7 +1202,7 @@ int acp_create(const acp_case_desc* d, int device, acp_handle** out) {
                 LevelHost& L = h->host[l];
                 LevelDev& D = h->dev[l];
                 if ((s = devAlloc(h, (void**)&D.slot, (size_t)L.N * sizeof(int)))) return s;
-                CU(h, cudaMemcpyAsync(D.slot, L.slot.data(), (size_t)L.N * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+                CU(h, cudaMemsetAsync(D.slot, 0xFF, (size_t)L.N * sizeof(int), h->stream));  // -1: no record
                 if ((s = devAlloc(h, (void**)&D.sg, std::max<size_t>(1, (size_t)L.nSlots) * 12 * sizeof(double)))) return s;
                 CU(h, cudaMemsetAsync(D.sg, 0, std::max<size_t>(1, (size_t)L.nSlots) * 12 * sizeof(double), h->stream));
             }
@@ -1156,6 +1222,12 @@ int acp_create(const acp_case_desc* d, int device, acp_handle** out) {
             if ((s = devAlloc(h, (void**)&h->dF2C, h->f2cHost.size() * sizeof(F2CDev)))) return s;
             CU(h, cudaMemcpyAsync(h->dF2C, h->f2cHost.data(), h->f2cHost.size() * sizeof(F2CDev),
                                   cudaMemcpyHostToDevice, h->stream));
+        }
+        if (h->partner) {
+            const int nf = (int)h->c2fHost.size(), nc = (int)h->f2cHost.size();
+            if (nf) k_scatter_slots<C2FDev><<<(nf + 255) / 256, 256, 0, h->stream>>>(h->dev[1].slot, h->dC2F, nf);
+            if (nc) k_scatter_slots<F2CDev><<<(nc + 255) / 256, 256, 0, h->stream>>>(h->dev[0].slot, h->dF2C, nc);
+            CU(h, cudaGetLastError());
         }
     }
     CU(h, cudaStreamSynchronize(h->stream));
@@ -1231,23 +1303,54 @@ int acp_active_updates(acp_handle* h, long long* coarse, long long* fine) {
     return ACP_OK;
 }
 
-int acp_read_populations(acp_handle* h, int level, double* out) {
-    if (!h || !out || level < 0 || level >= (int)h->host.size()) return ACP_ERR_INVALID;
+// FP64 populations of ping-pong array `arr` of a level into host memory
+static int readArray(acp_handle* h, int level, int arr, double* out) {
     CU(h, cudaSetDevice(h->device));
     joinBatch(h);
     const LevelHost& L = h->host[level];
     double* tmp = nullptr;
     CU(h, cudaMallocAsync((void**)&tmp, (size_t)L.N * Q * sizeof(double), h->stream));
     switch (h->d.storage) {
-        case ACP_STORE_F64: launchToF64<double>(h, level, level == 0 ? h->cur : 0, tmp); break;
-        case ACP_STORE_F32_DEV: launchToF64<float>(h, level, level == 0 ? h->cur : 0, tmp); break;
-        default: launchToF64<__half>(h, level, level == 0 ? h->cur : 0, tmp); break;
+        case ACP_STORE_F64: launchToF64<double>(h, level, arr, tmp); break;
+        case ACP_STORE_F32_DEV: launchToF64<float>(h, level, arr, tmp); break;
+        default: launchToF64<__half>(h, level, arr, tmp); break;
     }
     cudaError_t e = cudaMemcpyAsync(out, tmp, (size_t)L.N * Q * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
     cudaFreeAsync(tmp, h->stream);
     if (e != cudaSuccess) return fail(h, ACP_ERR_CUDA, "copy: %s", cudaGetErrorString(e));
     CU(h, cudaStreamSynchronize(h->stream));
     return ACP_OK;
+}
+
+int acp_read_populations(acp_handle* h, int level, double* out) {
+    if (!h || !out || level < 0 || level >= (int)h->host.size()) return ACP_ERR_INVALID;
+    return readArray(h, level, level == 0 ? h->cur : 0, out);
+}
+
+int acp_node_kind(acp_handle* h, int level, int i, int j, int k, int* id, int* face_class) {
+    if (!h || !id || !face_class || level < 0 || level >= (int)h->host.size()) return ACP_ERR_INVALID;
+    const LevelHost& L = h->host[level];
+    const int c[3] = {i - L.off[0], j - L.off[1], k - L.off[2]};
+    *id = -1;
+    *face_class = CODE_FLUID;
+    if (c[0] < 0 || c[1] < 0 || c[2] < 0 || c[0] >= L.nx || c[1] >= L.ny || c[2] >= L.nz) return ACP_OK;
+    const uint8_t code = L.code[((long long)c[2] * L.ny + c[1]) * L.nx + c[0]];
+    if (code == CODE_DEAD) return ACP_OK;
+    if (code == CODE_FLUID) {
+        *id = 0;
+    } else if (code < CODE_IFACE0) {
+        *id = 1;
+        *face_class = code;
+    } else {
+        *id = 2;
+        *face_class = code - CODE_IFACE0;
+    }
+    return ACP_OK;
+}
+
+int acp_read_populations_other(acp_handle* h, int level, double* out) {
+    if (!h || !out || level < 0 || level >= (int)h->host.size()) return ACP_ERR_INVALID;
+    return readArray(h, level, level == 0 ? (h->cur ^ 1) : 1, out);
 }
 
 int acp_read_populations_window(acp_handle* h, int level, long long begin, int count, double* out) {

@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <string>
 #include <vector>
 
@@ -25,8 +26,7 @@ struct LevelHost {
     int per[3] = {0, 0, 0};  // periodic axes of this level
     std::vector<uint8_t> code;
     std::vector<BNodeDev> lodiX, lodiZY;
-    std::vector<int> slot;  // coupling node -> partner-strain record (empty: none kept)
-    int nSlots = 0;
+    int nSlots = 0;  // partner-strain records kept (the device map LevelDev::slot; 0: none)
     long long active = 0;
     double omega = 0, dt = 0, spacing = 0;
 };
@@ -226,6 +226,26 @@ inline int tiledChunkFor(const LevelHost& L, int perSM) {
     int chunk = 8;
     while (chunk > 6 && bxy * ((L.nz + chunk - 1) / chunk) < (long long)perSM * 148) --chunk;
     return std::min(chunk, L.nz);
+}
+
+// The y-marching form of the neighbour-moment collide (k_collide_push_march)
+// takes levels whose z axis is periodic and at most MARCH_MAX_NZ planes deep.
+inline bool marchesY(const LevelHost& L) { return L.per[2] && L.nz <= MARCH_MAX_NZ; }
+
+// y rows per march block.  Every block reloads two rows at its chunk's ends,
+// yet short chunks win: a block's rows are serial (load, barrier, collide),
+// so the SM hides latency only across blocks, and many short-lived blocks
+// also balance the tail.  Measured on the fine level of the 1024 x 512 x 3
+// two-level HRR workload (collide time per coarse step): FP32 (alternating
+// march directions, 56 registers) 2 rows 562 us, 3 rows 536, 4 rows 528,
+// 8 rows 545, 16 rows 599; FP64 (prefetch) 4 rows 1104 us, 8 rows 1087.
+// ACP_MARCH_YCHUNK overrides the choice.
+inline int marchChunkFor(const LevelHost& L, size_t realBytes) {
+    if (const char* e = std::getenv("ACP_MARCH_YCHUNK")) {
+        const int v = std::atoi(e);
+        if (v > 0) return std::min(v, L.ny);
+    }
+    return std::min(realBytes == 8 ? 8 : 4, L.ny);
 }
 
 // z chunk of the batched engine's persistent tiled work items: a periodic z

@@ -725,6 +725,228 @@ __global__ void __launch_bounds__(TX * TY, TiledMinBlocks<R>::value) k_collide_p
     tiledBody<S, R, OP, ORDER, CUBIC>(a, zChunk, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
+// ---------------------------------------------------------------------------
+// The same collide + push for lattices whose z axis is periodic and at most
+// MARCH_MAX_NZ planes deep (the quasi-2D pulse cases): a block holds MARCH_TX
+// x-nodes by the whole periodic z column and marches along y.  The moments of
+// a row (every x and z of the block) are formed once and roll through four
+// shared-memory row slots, so the y neighbours cost no extra loads and the z
+// neighbours wrap inside the block; the first and last x lane of the block are
+// halo lanes that only form moments (the x neighbours of the block's edge
+// nodes), so x tiles advance by MARCH_TX - 2 nodes.  Per collided node the
+// loads are 19 x (MARCH_TX / (MARCH_TX - 2)) x (rows + 2) / rows instead of the
+// 19 x (1 + ring / tile) of the x-y tile.  Thread (tx, tz) owns the node at x =
+// x0 - 1 + tx, z = tz of every row.
+#ifndef ACP_MARCH_TX
+#define ACP_MARCH_TX 32
+#endif
+constexpr int MARCH_TX = ACP_MARCH_TX;
+constexpr int MARCH_MAX_NZ = 8;
+constexpr int MARCH_STEP = MARCH_TX - 2;  // collided x-nodes per block
+#ifndef ACP_MARCH_PREFETCH_F64
+#define ACP_MARCH_PREFETCH_F64 1
+#endif
+
+// dynamic shared memory of a march block: four row slots of nz x MARCH_TX moment records
+template <typename R>
+constexpr size_t marchSmemBytes(int nz) {
+    return sizeof(MomR<R>) * 4 * (size_t)nz * MARCH_TX;
+}
+
+template <typename S, typename R, int OP, int ORDER, bool CUBIC>
+__device__ __forceinline__ void marchBody(const LevelArgs<S>& a, int yChunk, int bx, int by, MomR<R>* sm) {
+    const int tx = threadIdx.x, tz = threadIdx.y, nz = a.nz;
+    // slot s, plane z, lane x
+    auto at = [&](int s, int z, int x) -> MomR<R>& { return sm[(s * nz + z) * MARCH_TX + x]; };
+    const int xu = bx * MARCH_STEP - 1 + tx;  // unwrapped x of the lane
+    const int xw = wrapm(xu, a.nx, a.per[0]);
+    const bool collider = tx > 0 && tx < MARCH_TX - 1 && xu < a.nx;
+    const int yBeg = by * yChunk;
+    const int yEnd = min(a.ny, yBeg + yChunk);
+    const int zpl = tz + 1 == nz ? 0 : tz + 1, zmi = tz == 0 ? nz - 1 : tz - 1;
+    // moments of row y (wrapped) into slot s; the lane's second-order sums into s2
+    auto rowPass = [&](int s, int y, R* s2) {
+        if (xw < 0) return;
+        const int n = (tz * a.ny + y) * a.nx + xw;
+        if (a.code[n] == CODE_DEAD) return;
+        R g[Q];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) g[q] = R(Store<S>::load(a.A + (q * a.Ni + n), scaleOf(a, q)));
+        R d, jj[3];
+        pairMoments<R>(g, d, jj, s2);
+        MomR<R> m;
+        m.drho = d;
+        const R inv = rcpRN(R(a.shift) + d);
+        m.ux = jj[0] * inv;
+        m.uy = jj[1] * inv;
+        m.uz = jj[2] * inv;
+        at(s, tz, tx) = m;
+    };
+    // Odd chunks march downwards: two neighbouring chunks then reach the row
+    // they both load (the one past their common end) at about the same time,
+    // so the second load hits L2 instead of DRAM.  Step s visits row
+    // rowAt(s); steps -1 and len load the rows beyond the chunk's ends, and
+    // the row of step s sits in slot (s + 1) mod 4.
+    const int len = yEnd - yBeg;
+    const int dir = (by & 1) ? -1 : 1;
+    auto rowAt = [&](int st) { return dir > 0 ? yBeg + st : yEnd - 1 - st; };
+    auto key = [](int st) { return (st + 1) & 3; };
+    R cur[6], nxt[6];
+    {
+        const int ym = wrapc(rowAt(-1), a.ny, a.per[1]);
+        if (ym >= 0) rowPass(key(-1), ym, nxt);  // moments only
+        rowPass(key(0), rowAt(0), cur);
+    }
+    for (int st = 0; st < len; ++st) {
+        const int y = rowAt(st);
+        const int yn = wrapc(rowAt(st + 1), a.ny, a.per[1]);
+        if (yn >= 0) rowPass(key(st + 1), yn, nxt);
+        __syncthreads();
+        if (collider) {
+            const int n = (tz * a.ny + y) * a.nx + xu;
+            const uint8_t code = a.code[n];
+            const int sc = key(st);
+            const int sp = dir > 0 ? key(st + 1) : key(st - 1);  // row y + 1
+            const int sn = dir > 0 ? key(st - 1) : key(st + 1);  // row y - 1
+            tiledCollide<S, R, OP, ORDER, CUBIC>(a, n, xu, y, tz, code, at(sc, tz, tx), at(sc, tz, tx + 1),
+                                                 at(sc, tz, tx - 1), at(sp, tz, tx), at(sn, tz, tx), at(sc, zpl, tx),
+                                                 at(sc, zmi, tx), cur);
+        }
+#pragma unroll
+        for (int c = 0; c < 6; ++c) cur[c] = nxt[c];
+    }
+}
+
+// The same march with the loads of row y+2 issued before row y collides and
+// reduced to moments after it, so their latency hides behind the collision;
+// the node classes run one row further ahead (a dead node's populations are
+// not loaded).  Row slots as above: during step st the block writes the slot
+// of step st+2 while slower threads may still read those of steps st-1..st+1.
+template <typename S, typename R, int OP, int ORDER, bool CUBIC>
+__device__ __forceinline__ void marchBodyPrefetch(const LevelArgs<S>& a, int yChunk, int bx, int by, MomR<R>* sm) {
+    const int tx = threadIdx.x, tz = threadIdx.y, nz = a.nz;
+    auto at = [&](int s, int z, int x) -> MomR<R>& { return sm[(s * nz + z) * MARCH_TX + x]; };
+    const int xu = bx * MARCH_STEP - 1 + tx;
+    const int xw = wrapm(xu, a.nx, a.per[0]);
+    const bool collider = tx > 0 && tx < MARCH_TX - 1 && xu < a.nx;
+    const int yBeg = by * yChunk;
+    const int yEnd = min(a.ny, yBeg + yChunk);
+    const int zpl = tz + 1 == nz ? 0 : tz + 1, zmi = tz == 0 ? nz - 1 : tz - 1;
+    // steps, rows and slots as in marchBody, every chunk marching upwards:
+    // with the prefetch (FP64) alternating directions measured slower, 1237
+    // against 1087 us per coarse step on the 1024 x 512 x 3 HRR workload
+    const int len = yEnd - yBeg;
+    const int dir = 1;
+    auto rowAt = [&](int st) { return dir > 0 ? yBeg + st : yEnd - 1 - st; };
+    auto key = [](int st) { return (st + 1) & 3; };
+    // node index of the lane in the row of step st, or -1 outside a LODI y axis
+    auto nodeOf = [&](int st) -> int {
+        const int y = wrapc(rowAt(st), a.ny, a.per[1]);
+        return (xw < 0 || y < 0) ? -1 : (tz * a.ny + y) * a.nx + xw;
+    };
+    auto codeOf = [&](int n) -> uint8_t { return n < 0 ? CODE_DEAD : a.code[n]; };
+    auto loadRow = [&](int n, uint8_t c, R* g) {
+        if (c == CODE_DEAD) return;
+#pragma unroll
+        for (int q = 0; q < Q; ++q) g[q] = R(Store<S>::load(a.A + (q * a.Ni + n), scaleOf(a, q)));
+    };
+    auto reduceRow = [&](int s, uint8_t c, const R* g, R* s2) {
+        if (c == CODE_DEAD) return;
+        R d, jj[3];
+        pairMoments<R>(g, d, jj, s2);
+        MomR<R> m;
+        m.drho = d;
+        const R inv = rcpRN(R(a.shift) + d);
+        m.ux = jj[0] * inv;
+        m.uy = jj[1] * inv;
+        m.uz = jj[2] * inv;
+        at(s, tz, tx) = m;
+    };
+    R g[Q];
+    R s2c[6], s2n[6], s2p[6];
+    int nC, nN, nP;
+    uint8_t cC, cN, cP, cA;
+    {
+        const int nM = nodeOf(-1);
+        const uint8_t cM = codeOf(nM);
+        loadRow(nM, cM, g);
+        reduceRow(key(-1), cM, g, s2p);
+        nC = nodeOf(0);
+        cC = codeOf(nC);
+        loadRow(nC, cC, g);
+        reduceRow(key(0), cC, g, s2c);
+        nN = nodeOf(1);
+        cN = codeOf(nN);
+        loadRow(nN, cN, g);
+        reduceRow(key(1), cN, g, s2n);
+        nP = 2 <= len ? nodeOf(2) : -1;
+        cP = codeOf(nP);
+    }
+    __syncthreads();
+    for (int st = 0; st < len; ++st) {
+        // step st+2 in flight, the class of step st+3 behind it
+        loadRow(nP, cP, g);
+        const int nA = st + 3 <= len ? nodeOf(st + 3) : -1;
+        cA = codeOf(nA);
+        if (collider) {
+            const int y = rowAt(st);
+            const int sc = key(st);
+            const int sp = dir > 0 ? key(st + 1) : key(st - 1);  // row y + 1
+            const int sn = dir > 0 ? key(st - 1) : key(st + 1);  // row y - 1
+            tiledCollide<S, R, OP, ORDER, CUBIC>(a, nC, xu, y, tz, cC, at(sc, tz, tx), at(sc, tz, tx + 1),
+                                                 at(sc, tz, tx - 1), at(sp, tz, tx), at(sn, tz, tx), at(sc, zpl, tx),
+                                                 at(sc, zmi, tx), s2c);
+        }
+        reduceRow(key(st + 2), cP, g, s2p);
+        __syncthreads();
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+            s2c[c] = s2n[c];
+            s2n[c] = s2p[c];
+        }
+        nC = nN;
+        cC = cN;
+        nN = nP;
+        cN = cP;
+        nP = nA;
+        cP = cA;
+    }
+}
+
+// Measured on the 1024 x 512 x 3 two-level HRR workload (collide time per
+// coarse step): FP64 1087 us with the prefetch against 1093 us without; FP32
+// 568 us without it at 64 registers (five blocks of 32 x 6 per SM) against
+// 597 us with it at 80 registers (four blocks), the lost block costing more
+// than the hidden latency gains.
+template <typename R>
+struct MarchPrefetch {
+    static constexpr bool value = sizeof(R) == 8 && ACP_MARCH_PREFETCH_F64;
+};
+
+template <typename S, typename R, int OP, int ORDER, bool CUBIC>
+__global__ void __launch_bounds__(MARCH_TX * MARCH_MAX_NZ, TiledMinBlocks<R>::value)
+    k_collide_push_march(LevelArgs<S> a, int yChunk) {
+    extern __shared__ __align__(16) unsigned char marchSmem[];
+    if (MarchPrefetch<R>::value)
+        marchBodyPrefetch<S, R, OP, ORDER, CUBIC>(a, yChunk, blockIdx.x, blockIdx.y,
+                                                  reinterpret_cast<MomR<R>*>(marchSmem));
+    else
+        marchBody<S, R, OP, ORDER, CUBIC>(a, yChunk, blockIdx.x, blockIdx.y, reinterpret_cast<MomR<R>*>(marchSmem));
+}
+
+// FP32 compute: the register cap set directly, so that blocks of 32 x 6
+// threads fit six to an SM at 56 registers (a launch bound can only express
+// caps for the 256-thread maximum block).  FP32 collide time per coarse step
+// on the workload above: 528 us at 56 registers, 538 at 64, 555 at 48 (spills).
+#ifndef ACP_MARCH_REGS_F32
+#define ACP_MARCH_REGS_F32 56
+#endif
+template <typename S, typename R, int OP, int ORDER, bool CUBIC>
+__global__ void __maxnreg__(ACP_MARCH_REGS_F32) k_collide_push_march_f32(LevelArgs<S> a, int yChunk) {
+    extern __shared__ __align__(16) unsigned char marchSmem[];
+    marchBody<S, R, OP, ORDER, CUBIC>(a, yChunk, blockIdx.x, blockIdx.y, reinterpret_cast<MomR<R>*>(marchSmem));
+}
+
 
 // ---------------------------------------------------------------------------
 // LODI characteristic pressure boundary (Node::LODIpressureOutlet and

@@ -40,6 +40,7 @@ def lib():
         L.acp_level_dims.argtypes = [vp, C.c_int, C.POINTER(C.c_int)]
         L.acp_active_updates.argtypes = [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
         L.acp_read_populations.argtypes = [vp, C.c_int, vp]
+        L.acp_read_populations_other.argtypes = [vp, C.c_int, vp]
         L.acp_write_populations.argtypes = [vp, C.c_int, vp]
         L.acp_read_field.argtypes = [vp, C.c_int, C.c_int, vp]
         L.acp_set_probes.argtypes = [vp, C.c_int, vp]
@@ -122,19 +123,28 @@ class Lattice:
         self._check(lib().acp_active_updates(self._h, C.byref(c), C.byref(f)))
         return c.value, f.value
 
-    def populations(self, level=0):
+    def populations(self, level=0, other=False):
+        """FP64 f_i of a level, (19, nz, ny, nx): the current state, or with
+        other=True the level's other ping-pong array (acp_read_populations_other)"""
         nx, ny, nz = self.dims(level)
         out = np.empty((19, nz, ny, nx), dtype=np.float64)
-        self._check(lib().acp_read_populations(self._h, level, out.ctypes.data))
+        fn = lib().acp_read_populations_other if other else lib().acp_read_populations
+        self._check(fn(self._h, level, out.ctypes.data))
         return out
 
     def write_populations(self, f, level=0):
         f = np.ascontiguousarray(f, dtype=np.float64)
         self._check(lib().acp_write_populations(self._h, level, f.ctypes.data))
 
-    def field(self, which, level=0):
+    def field(self, which, level=0, out=None):
+        """FP64 field `which` (ACP_FIELD_*) of a level as an (nz, ny, nx)
+        array; `out`, if given, is filled instead (C-contiguous float64 of that
+        shape -- a page-locked buffer makes the copy a direct DMA)"""
         nx, ny, nz = self.dims(level)
-        out = np.empty((nz, ny, nx), dtype=np.float64)
+        if out is None:
+            out = np.empty((nz, ny, nx), dtype=np.float64)
+        elif out.shape != (nz, ny, nx) or out.dtype != np.float64 or not out.flags["C_CONTIGUOUS"]:
+            raise ValueError(f"field output must be C-contiguous float64 of shape {(nz, ny, nx)}")
         self._check(lib().acp_read_field(self._h, level, which, out.ctypes.data))
         return out
 

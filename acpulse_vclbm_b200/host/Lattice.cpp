@@ -7,7 +7,6 @@
 #include <fstream>
 #include <iomanip>
 #include <iostream>
-#include <limits>
 
 void Lattice::check(int status, const char* what) {
     if (status != ACP_OK) {
@@ -33,7 +32,7 @@ void Lattice::initialization(Control&) {
     check(acp_init(h_), "initialization");
     // main.cpp:55-57: both flags start true and the state is in both arrays
     currentFlag_ = true;
-    stepsSeen_[0] = stepsSeen_[1] = -1;
+    for (auto& w : stepsSeen_) w[0] = w[1] = -1;
 }
 
 void Lattice::solve(bool& alternating) {
@@ -48,26 +47,30 @@ void Lattice::solve(bool& alternatingL0, bool&) {
     currentFlag_ = !alternatingL0;
 }
 
-void Lattice::refresh(int level) {
+void Lattice::refresh(int level, int which) {
     long long steps = 0;
     acp_steps_done(h_, &steps);
-    if (stepsSeen_[level] == steps) return;
+    if (stepsSeen_[which][level] == steps) return;
     check(acp_sync(h_), "sync");
     const size_t n = (size_t)dims_[level][0] * dims_[level][1] * dims_[level][2];
-    cache_[level].resize(n * 19);
-    check(acp_read_populations(h_, level, cache_[level].data()), "getDistribution");
-    stepsSeen_[level] = steps;
+    cache_[which][level].resize(n * 19);
+    check(which == 0 ? acp_read_populations(h_, level, cache_[which][level].data())
+                     : acp_read_populations_other(h_, level, cache_[which][level].data()),
+          "getDistribution");
+    stepsSeen_[which][level] = steps;
 }
 
 double Lattice::getDistribution(bool& alternating, int& dir, int& level, int& i, int& j, int& k) {
     if (dir >= 19 || level < 0 || level > bc_.caseDescription().max_level) return 0.;
-    if (alternating != currentFlag_) return std::numeric_limits<double>::quiet_NaN();  // only the current array is kept
-    refresh(level);
+    // the flag naming the current state reads it; the other flag reads the
+    // other ping-pong array (acp_read_populations_other)
+    const int which = alternating == currentFlag_ ? 0 : 1;
+    refresh(level, which);
     const int li = i - origin_[level][0], lj = j - origin_[level][1], lk = k - origin_[level][2];
     const int* n = dims_[level];
     if (li < 0 || lj < 0 || lk < 0 || li >= n[0] || lj >= n[1] || lk >= n[2]) return 0.;
     const size_t N = (size_t)n[0] * n[1] * n[2];
-    return cache_[level][(size_t)dir * N + ((size_t)lk * n[1] + lj) * n[0] + li];
+    return cache_[which][level][(size_t)dir * N + ((size_t)lk * n[1] + lj) * n[0] + li];
 }
 
 void Lattice::writeResultsVTK(std::string filename, bool&, bool&) {

@@ -4,6 +4,10 @@
 // WriteInterval.  Prints the throughput in MLUPS at the end.
 //
 // usage: acp_main <BoundaryConditions.txt> [steps] [--dump-rho file] [--no-vtk]
+//                 [--dump-nodes file level]
+// --dump-nodes writes, for every node of a level (x fastest), the Node view's
+// ID, density, velocity and pressure (six doubles), and prints the count of
+// each GridCoupling tag of that level.
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -12,20 +16,30 @@
 #include <string>
 #include <vector>
 
+#include <map>
+
 #include "Control.h"
 #include "Lattice.h"
+#include "Node.h"
 
 int main(int argc, char* argv[]) {
     if (argc < 2) {
-        std::fprintf(stderr, "usage: %s <BoundaryConditions.txt> [steps] [--dump-rho file] [--no-vtk]\n", argv[0]);
+        std::fprintf(stderr,
+                     "usage: %s <BoundaryConditions.txt> [steps] [--dump-rho file] [--no-vtk] [--dump-nodes file level]\n",
+                     argv[0]);
         return 1;
     }
-    std::string dump;
+    std::string dump, dumpNodes;
+    int nodesLevel = 0;
     bool vtk = true;
     int stepsArg = -1;
     for (int a = 2; a < argc; ++a) {
         if (!std::strcmp(argv[a], "--dump-rho") && a + 1 < argc) dump = argv[++a];
         else if (!std::strcmp(argv[a], "--no-vtk")) vtk = false;
+        else if (!std::strcmp(argv[a], "--dump-nodes") && a + 2 < argc) {
+            dumpNodes = argv[++a];
+            nodesLevel = std::atoi(argv[++a]);
+        }
         else stepsArg = std::atoi(argv[a]);
     }
     Control boundaryConditions(argv[1]);
@@ -68,6 +82,34 @@ int main(int argc, char* argv[]) {
                     std::fwrite(&r, sizeof r, 1, f);
                 }
         std::fclose(f);
+    }
+    if (!dumpNodes.empty()) {
+        int dims[3], origin[3];
+        acp_level_dims(simulationCase.handle(), nodesLevel, dims);
+        acp_level_origin(simulationCase.handle(), nodesLevel, origin);
+        FILE* f = std::fopen(dumpNodes.c_str(), "wb");
+        std::map<std::string, long long> tags;
+        for (int k = origin[2]; k < origin[2] + dims[2]; ++k)
+            for (int j = origin[1]; j < origin[1] + dims[1]; ++j)
+                for (int i = origin[0]; i < origin[0] + dims[0]; ++i) {
+                    Node node(simulationCase, nodesLevel, i, j, k);
+                    double rec[6] = {(double)node.getNodeID(), 0, 0, 0, 0, 0};
+                    if (node.getNodeID() >= 0) {
+                        rec[1] = node.calcDensity(boundaryConditions, alternatingL0);
+                        node.calcVelocity(boundaryConditions, alternatingL0, rec[1], rec + 2);
+                        rec[5] = node.calcPressure(alternatingL0, boundaryConditions);
+                    }
+                    if (node.getNodeID() == 2) ++tags[GridCoupling(simulationCase, nodesLevel, i, j, k).getGridCouplingTag()];
+                    std::fwrite(rec, sizeof rec, 1, f);
+                }
+        std::fclose(f);
+        std::printf("{");
+        const char* sep = "";
+        for (const auto& t : tags) {
+            std::printf("%s\"%s\": %lld", sep, t.first.c_str(), t.second);
+            sep = ", ";
+        }
+        std::printf("}\n");
     }
     return 0;
 }

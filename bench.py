@@ -253,25 +253,33 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def bench_batched(args, engine, torch, device, peak):
-    """The batched form: seeded quasi-2D cases of uneven sizes and operators
-    (FP32 deviation), one CUDA graph per coarse step, schedule chosen by the
-    autotuner; beside it the same cases stepped one after the other."""
-    from acpulse_vclbm_b200 import workloads
-    descs = workloads.batched_cases(seed=2024, n=args.batched_cases)
+def _batched_form(args, engine, torch, device, storage, dist, rank, world):
+    """One storage form of the batched configuration on this rank's share of
+    the seeded cases (largest-first assignment over the ranks): the batch
+    tuned, then K steps timed (max over ranks), then the same cases stepped
+    one after the other for comparison."""
+    from acpulse_vclbm_b200 import replicas, shard, workloads
+    descs_all = workloads.batched_cases(seed=2024, n=args.batched_cases, storage=storage)
+    assign = shard.assign_cases([shard.case_updates(d) for d in descs_all], world)
+    _, descs = shard.my_share(descs_all, assign, rank)
     Ls = [engine.Lattice(d, device=device).init() for d in descs]
-    B = engine.Batch(Ls)
-    report = B.tune(trial_steps=3)
-    info = B.info()
+    B = engine.Batch(Ls) if Ls else None
+    report = B.tune(trial_steps=3) if B else ""
+    info = B.info() if B else {"groups": 0, "launches_per_step": 0, "updates_per_step": 0}
     steps = max(20, args.steps // 2)
-    B.step(3)
-    B.sync()
+    if B:
+        B.step(3)
+        B.sync()
     torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
     t0 = time.perf_counter()
-    B.step(steps)
-    B.sync()
+    if B:
+        B.step(steps)
+        B.sync()
     batched_s = (time.perf_counter() - t0) / steps
-    B.close()
+    if B:
+        B.close()
     # the same cases stepped one by one (each its own CUDA graph), for comparison
     n1 = 10
     for L in Ls:
@@ -285,17 +293,32 @@ def bench_batched(args, engine, torch, device, peak):
     alone_s = (time.perf_counter() - t0) / n1
     for L in Ls:
         L.close()
-    upd = info["updates_per_step"]
-    mlups = upd / batched_s / 1e6
-    achieved = upd * 152 / batched_s / 1e9
-    return {"cases": len(descs), "seed": 2024, "groups": info["groups"],
-            "launches_per_step": info["launches_per_step"], "updates_per_step": upd,
-            "mlups": round(mlups, 1), "ms_per_step": batched_s * 1e3,
-            "hbm_frac_whole_step": round(achieved / peak, 4), "achieved_gbs_whole_step": round(achieved, 1),
+    batched_s, alone_s = replicas.reduce([batched_s, alone_s], dist, "max", device="cuda")
+    upd = replicas.reduce([float(info["updates_per_step"])], dist, "sum", device="cuda")[0]
+    return {"updates_per_step": int(upd), "mlups": round(upd / batched_s / 1e6, 1), "ms_per_step": batched_s * 1e3,
+            "groups_rank0": info["groups"], "launches_per_step_rank0": info["launches_per_step"],
             "alone_sequential_mlups": round(upd / alone_s / 1e6, 1),
             "speedup_over_sequential": round(alone_s / batched_s, 2),
-            "tuner": report.strip().split("\n")[-1],
-            "timing": "host clock around synchronised graph launches"}
+            "tuner_rank0": report.strip().split("\n")[-1] if report else None}
+
+
+def bench_batched(args, engine, torch, device, peak, dist=None, rank=0, world=1):
+    """The batched form: 64 seeded quasi-2D cases of uneven sizes and
+    operators, one CUDA graph per coarse step, schedule chosen by the
+    autotuner, in FP32 deviation and in FP64 storage; with N ranks the cases
+    are sharded over the GPUs (largest-first), each rank one batch of its
+    share, and the rates are whole-job (summed updates over the slowest
+    rank's time)."""
+    out = {"cases": args.batched_cases, "seed": 2024, "ranks": world,
+           "timing": "host clock around synchronised graph launches (K steps, max over ranks)"}
+    for storage, key, b in (("FP32-DEV", "fp32", 152), ("FP64", "fp64", 304)):
+        r = _batched_form(args, engine, torch, device, storage, dist, rank, world)
+        achieved = r["updates_per_step"] * b / (r["ms_per_step"] * 1e-3) / 1e9
+        r["achieved_gbs_whole_step"] = round(achieved, 1)
+        r["hbm_frac_whole_step"] = round(achieved / peak, 4)
+        out[key] = r
+    out["fp32_over_fp64"] = round(out["fp32"]["mlups"] / out["fp64"]["mlups"], 3)
+    return out
 
 
 def bench_serving(args, engine, device):
@@ -327,6 +350,7 @@ def run_engine(args):
     nodes = updates_per_step(d32)
 
     L32 = engine.Lattice(d32, device=local)
+    dims = [L32.dims(l) for l in range(d32.max_level + 1)]
     engine.lib().acp_set_stream(L32._h, stream)
     L32.init()
     L64 = engine.Lattice(d64, device=local)
@@ -369,26 +393,32 @@ def run_engine(args):
     L64.close()
 
     # end to end through the C ABI with host buffers: create (H2D of node
-    # classes and boundary wiring), init, K steps, D2H of the pressure field
+    # classes and boundary wiring), init, K steps, D2H of the pressure field of
+    # every level into the caller's page-locked host buffers (allocated
+    # before the timed region, as a caller keeps its output buffers)
+    outs = [torch.empty((nz, ny, nx), dtype=torch.float64, pin_memory=True).numpy() for nx, ny, nz in dims]
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     Le = engine.Lattice(d32, device=local).init()
     Le.step(args.steps)
     Le.sync()
-    pe = Le.field(4)
-    if d32.max_level == 1:
-        pe = Le.field(4, 1)
+    for l in range(d32.max_level + 1):
+        Le.field(4, l, out=outs[l])
     t1 = time.perf_counter()
-    dims = [Le.dims(l) for l in range(d32.max_level + 1)]
     stored = sum(a * b * c for a, b, c in dims)
     h2d = stored + 2 * (d32.ny * d32.nz) * 80  # node classes + LODI wiring records
     d2h = stored * 8  # the pressure fields (FP64, formed on the device)
     Le.close()
-    e2e = nodes * args.steps / (t1 - t0) / 1e6
+    e2e_s = t1 - t0
+    if dist:
+        from acpulse_vclbm_b200 import replicas
+        e2e_s = replicas.reduce([e2e_s], dist, "max", device="cuda")[0]
+    e2e = nodes * args.steps * args.gpus / e2e_s / 1e6  # every rank runs its own replica end to end
 
     batched = serving = None
-    if rank == 0 and args.batched_cases > 0:
-        batched = bench_batched(args, engine, torch, local, peak)
+    if args.batched_cases > 0:
+        world = args.gpus if dist else 1
+        batched = bench_batched(args, engine, torch, local, peak, dist, rank, world)
     if rank == 0 and args.serve_requests > 0:
         serving = bench_serving(args, engine, local)
     mlups32 = nodes * args.steps / (ms32 * 1e-3) / 1e6 * args.gpus
@@ -524,7 +554,17 @@ def study_sweep(steps=3200, nx=1024, ny=512):
                         row["fp32_l2_err_rel_amp"] = float(np.sqrt(sum((x ** 2).sum() for x in e) / n) / amp)
                         row["fp32_max_err_rel_amp"] = float(max(np.abs(x).max() for x in e) / amp)
                         row["fp32_probe_err_rel_amp"] = float(np.abs(s32 - s64).max() / amp)
-                        r32 = analysis.reflection_coefficient(s32[:, 0], uni[(op, nu)][:, 0], p0, w)
+                        # the FP32 form's R from its own pair of runs (refined and
+                        # uniform, both FP32), against the FP64 pair's
+                        key32 = (op, nu, "FP32-DEV")
+                        if key32 not in uni:
+                            du32 = analysis.interface_case(nx, ny, 3, op=op, nu=nu, eps=1e-3, b=24.0,
+                                                           center=(nx / 4.0, ny / 2.0, 1.0), refined=False,
+                                                           storage="FP32-DEV")
+                            uni[key32], _ = _study_run(du32, steps, analysis.interface_probes(du32))
+                        r32 = analysis.reflection_coefficient(s32[:, 0], uni[key32][:, 0], p0, w)
+                        row["fp32_R"] = r32
+                        row["fp32_R_abs_err"] = abs(r32 - r)
                         row["fp32_R_rel_err"] = abs(r32 - r) / r
                     row["seconds"] = time.perf_counter() - t0
                     rows.append(row)

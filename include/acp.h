@@ -156,6 +156,24 @@ int acp_active_updates(acp_handle* h, long long* coarse_nodes, long long* fine_n
 /* Populations of a level as FP64 f_i (see header comment), host buffer of
  * 19 * nodes doubles; replaces Lattice::getDistribution (Lattice.h:119). */
 int acp_read_populations(acp_handle* h, int level, double* host_out);
+/* The level's other ping-pong array as FP64 f_i, same layout: what the
+ * reference's getDistribution(flag, ...) returns for the flag that does not
+ * name the current state (Lattice.h:119, Node.h:52).  The engine streams by
+ * push from one array into the other, so this array holds the state the last
+ * coarse step started from (coarse level; the fine level: its state at the
+ * half step, after the coarse-to-fine coupling), where the reference keeps
+ * the post-collision values of its in-place collision.  Before the first
+ * step both arrays hold the initial state, as in the reference. */
+int acp_read_populations_other(acp_handle* h, int level, double* host_out);
+/* Kind of node (i, j, k) of a level (level-global node indices, as
+ * getDistribution takes them) in the reference's node IDs: 0 FluidNode,
+ * 1 BoundaryNode (LODI), 2 GridCoupling (FluidNode.h:11, BoundaryNode.h:11,
+ * GridCoupling.h:12), or -1 where the level has no live node (covered by the
+ * other level, or outside it).  *face_class: the face class
+ * (fx+1)*9 + (fy+1)*3 + (fz+1) of a boundary node's domain faces or of a
+ * coupling node's interface faces (outward normals of the level's live
+ * region), 13 otherwise.  Host data only: no device call. */
+int acp_node_kind(acp_handle* h, int level, int i, int j, int k, int* id, int* face_class);
 /* Overwrite a level's populations (both ping-pong arrays) from FP64 f_i. */
 int acp_write_populations(acp_handle* h, int level, const double* host_in);
 /* Checkpoint / restart of a case's device state.  The reference keeps no

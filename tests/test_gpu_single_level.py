@@ -167,6 +167,12 @@ TILE_CASES = [
     ("single-plane", (36, 20, 1), (False, False, True)),
     ("two-planes", (36, 20, 2), (False, False, True)),
     ("periodic-x-small", (9, 13, 5), (True, False, True)),
+    # y-marching blocks (periodic z of at most 8 planes): several x tiles with
+    # halo lanes, y chunks with periodic and LODI ends, the deepest column
+    ("march-six-planes", (70, 21, 6), (False, True, True)),
+    ("march-eight-planes-lodi-y", (65, 19, 8), (False, False, True)),
+    ("march-periodic-x", (61, 17, 4), (True, True, True)),
+    ("nine-planes-tiled", (33, 12, 9), (True, True, True)),
 ]
 
 
