@@ -77,6 +77,7 @@ def parse():
     ap.add_argument("--batched-cases", type=int, default=64, help="cases of the batched form (0: skip)")
     ap.add_argument("--serve-requests", type=int, default=16, help="requests of the serving form (0: skip)")
     ap.add_argument("--order", type=int, default=3)
+    ap.add_argument("--precision-form", type=int, default=1, help="time the 256^3 precision form (0: skip)")
     ap.add_argument("--storage", default="FP32-DEV")
     ap.add_argument("--profile", action="store_true", help="profiling run of one case (see the module docstring)")
     ap.add_argument("--timed", type=int, default=0, help="--profile: N steps kernel by kernel with CUDA events")
@@ -321,18 +322,103 @@ def bench_batched(args, engine, torch, device, peak, dist=None, rank=0, world=1)
     return out
 
 
-def bench_serving(args, engine, device):
-    """The serving form: a seeded Poisson stream of 3-D patch solves, FP32
-    deviation and FP64 side by side, continuous batching under a 40 GB budget."""
-    from acpulse_vclbm_b200 import serve, workloads
-    stream = workloads.request_stream(seed=7, n=args.serve_requests, rate_hz=4.0, size_range=(32, 96),
-                                      steps_range=(200, 2000))
-    reqs = [serve.Request(k, t, d, n) for k, (t, d, n) in enumerate(stream)]
-    s = serve.Server(budget_bytes=40 << 30, tick_steps=50, device=device)
-    rep = s.run(reqs)
-    rep["stream"] = (f"{len(reqs)} requests, Poisson 4/s (seed 7), 3-D boxes 32^3-96^3 with a centred 2:1 patch, "
-                     "200-2000 coarse steps, FP32-DEV / FP64 alternating, 5 operators")
-    return rep
+def bench_precision(args, engine, torch, device, peak):
+    """The precision form, device-timed: a 3-D pulse in a 256^3 coarse box
+    with a centred 128^3-cell patch refined 2:1, HRR (sigma 0.98), nu = 1e-4,
+    eps = 1e-2, b = 12, transverse LODI on all six faces; FP64, FP32 deviation
+    and FP16-scaled storage on the same inputs.  K steps timed with CUDA
+    events after W warm-up steps; the collide kernels' device time per step
+    gives the roofline; each reduced form's pressure error is taken against
+    the FP64 form after the same steps (coarse nodes the patch covers left
+    out)."""
+    import ctypes as C
+    stream = torch.cuda.Stream()
+    out = {"workload": ("3-D pulse, 256^3 coarse nodes, centred 128^3-cell patch refined 2:1, HRR order 3, "
+                        "sigma 0.98, nu=1e-4 lu, eps=1e-2, b=12, transverse LODI on six faces"),
+           "steps": args.steps, "warmup": args.warmup}
+    ref = None
+    n = 256
+    lo = n // 4
+    for storage, key, b in (("FP64", "fp64", 304), ("FP32-DEV", "fp32", 152), ("FP16-DEV", "fp16", 76)):
+        d = study_precision_case(1e-2, storage, n)
+        L = engine.Lattice(d, device=device)
+        engine.lib().acp_set_stream(L._h, stream.cuda_stream)
+        L.init()
+        ms = time_gpu(L, args.steps, args.warmup, torch, stream)
+        c, f = L.active_updates()
+        upd = c + 2 * f
+        km = (C.c_double * 5)()
+        engine.lib().acp_step_timed.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        engine.lib().acp_step_timed(L._h, 10, C.cast(km, C.c_void_p))
+        achieved = upd * b / (km[1] * 1e-3) / 1e9
+        row = {"mlups": round(upd * args.steps / (ms * 1e-3) / 1e6, 1), "ms_per_step": ms / args.steps,
+               "updates_per_step": upd, "collide_ms_per_step": km[1], "lodi_ms_per_step": km[2],
+               "coupling_ms_per_step": km[3],
+               "roofline": {"achieved_gbs": round(achieved, 1), "frac": round(achieved / peak, 4),
+                            "algorithmic_bytes_per_node": b}}
+        p = [L.field(4, l) for l in range(2)]
+        if ref is None:
+            ref = (p, d.ic_eps * d.density * d.speed_of_sound ** 2)
+        else:
+            live = np.ones(p[0].shape, dtype=bool)
+            live[lo + 1:lo + n // 2, lo + 1:lo + n // 2, lo + 1:lo + n // 2] = False
+            err = max(np.abs(p[0] - ref[0][0])[live].max(), np.abs(p[1] - ref[0][1]).max()) / ref[1]
+            row["pressure_err_rel_amplitude_vs_fp64"] = float(err)
+        L.close()
+        out[key] = row
+    return out
+
+
+def _serve_once(args, engine, device, base, scale, dist, rank, world):
+    """serve the seeded stream with its arrival times scaled by `scale` (0:
+    every request at once); requests routed over the ranks; per-request
+    results gathered, whole-job rates over the slowest rank's wall time"""
+    from acpulse_vclbm_b200 import replicas, serve, shard
+    reqs = [serve.Request(k, t * scale, d, n) for k, (t, d, n) in enumerate(base)]
+    route = shard.route_requests(reqs, world)
+    _, mine = shard.my_share(reqs, route, rank)
+    srv = serve.Server(budget_bytes=120 << 30, tick_steps=50, device=device)
+    rep = srv.run(mine) if mine else {"wall_s": 0.0, "batch_rebuilds": 0, "ticks": 0}
+    local = {r.rid: (r.latency, r.updates, r.storage) for r in srv.results}
+    allres = shard.gather_results(local, dist)
+    wall = replicas.reduce([rep["wall_s"]], dist, "max", device="cuda")[0]
+
+    def stats(rows):
+        lat = np.array([x[0] for x in rows])
+        upd = sum(x[1] for x in rows)
+        return {"requests": len(rows), "solves_per_s": round(len(rows) / wall, 3),
+                "aggregate_mlups": round(upd / wall / 1e6, 1),
+                "latency_p50_s": round(float(np.percentile(lat, 50)), 4) if len(lat) else None,
+                "latency_p99_s": round(float(np.percentile(lat, 99)), 4) if len(lat) else None}
+    rows = list(allres.values())
+    out = stats(rows)
+    out.update({"wall_s": round(wall, 3), "batch_rebuilds_rank0": rep["batch_rebuilds"],
+                "fp32": stats([x for x in rows if x[2] == 1]), "fp64": stats([x for x in rows if x[2] == 0])})
+    return out
+
+
+def bench_serving(args, engine, device, dist=None, rank=0, world=1):
+    """The serving form: a seeded Poisson stream of 3-D pulse solves (64^3 to
+    256^3 coarse boxes with a centred 2:1 patch, 200-2000 coarse steps, five
+    operators, FP32 deviation and FP64 alternating) under continuous batching
+    with a 120 GB budget per GPU.  Capacity is measured with every request
+    arriving at once; the same stream is then offered at 50, 80 and 95 % of
+    that capacity (arrival times scaled)."""
+    from acpulse_vclbm_b200 import workloads
+    base = workloads.request_stream(seed=7, n=args.serve_requests, rate_hz=1.0, size_range=(64, 256),
+                                    steps_range=(200, 2000))
+    cap = _serve_once(args, engine, device, base, 0.0, dist, rank, world)
+    capacity = cap["solves_per_s"]
+    out = {"stream": (f"{len(base)} requests (seed 7), 3-D boxes 64^3-256^3 with a centred 2:1 patch, "
+                      "200-2000 coarse steps, FP32-DEV / FP64 alternating, 5 operators"),
+           "ranks": world, "capacity": cap, "loads": []}
+    for frac in (0.5, 0.8, 0.95):
+        rate = frac * capacity  # requests per second offered to the whole job
+        r = _serve_once(args, engine, device, base, 1.0 / rate, dist, rank, world)
+        r["offered_load"] = frac
+        r["offered_rate_per_s"] = round(rate, 3)
+        out["loads"].append(r)
+    return out
 
 
 def run_engine(args):
@@ -415,12 +501,14 @@ def run_engine(args):
         e2e_s = replicas.reduce([e2e_s], dist, "max", device="cuda")[0]
     e2e = nodes * args.steps * args.gpus / e2e_s / 1e6  # every rank runs its own replica end to end
 
-    batched = serving = None
+    batched = serving = precision = None
+    if args.precision_form:
+        precision = bench_precision(args, engine, torch, local, peak)
     if args.batched_cases > 0:
         world = args.gpus if dist else 1
         batched = bench_batched(args, engine, torch, local, peak, dist, rank, world)
-    if rank == 0 and args.serve_requests > 0:
-        serving = bench_serving(args, engine, local)
+    if args.serve_requests > 0:
+        serving = bench_serving(args, engine, local, dist, rank, args.gpus if dist else 1)
     mlups32 = nodes * args.steps / (ms32 * 1e-3) / 1e6 * args.gpus
     mlups64 = nodes * args.steps / (ms64 * 1e-3) / 1e6 * args.gpus
     cpu = None
@@ -447,6 +535,7 @@ def run_engine(args):
                         "d2h_bytes_per_step": d2h // args.steps},
                 "gpu_launches": lps.value * args.steps,
                 "clocks": clk,
+                "precision_form": precision,
                 "batched": batched,
                 "serving": serving}
         print(json.dumps(line), flush=True)

@@ -13,6 +13,9 @@
 // When probe_every > 0 a second file <out.bin>.rho holds the density of every
 // node after every probe_every steps (float64 [n_probe][nx][ny][nz]).
 //
+// usage: acp_ref --vtk <BoundaryConditions.txt> <steps> <prefix>
+// writes the reference's ASCII VTK file <prefix>.vtk after `steps` steps.
+//
 // usage: acp_ref --topo <BoundaryConditions.txt> <out.txt>
 // writes, for every boundary node of level 0, the wiring that setConnectivity
 // (Lattice.cpp:500-1394) gives it: normal direction, the two normal
@@ -70,9 +73,27 @@ static int dumpTopology(const char* bcFile, const char* outPath)
     return 0;
 }
 
+// the reference's own legacy VTK file (Lattice::writeResultsVTK,
+// Lattice.cpp:2212-4352) after `steps` coarse steps, flags as main.cpp keeps them
+static int writeVtk(const char* bcFile, int steps, const char* prefix)
+{
+    Control bc(bcFile);
+    if (bc.getLevelMax() != 0) return 2;
+    Lattice lat(bc);
+    lat.initialization(bc);
+    bool alt = true, altL1 = true;
+    for (int t = 0; t < steps; ++t) {
+        lat.solve(alt);
+        alt = !alt;
+    }
+    lat.writeResultsVTK(prefix, alt, altL1);
+    return 0;
+}
+
 int main(int argc, char** argv)
 {
     if (argc == 4 && std::string(argv[1]) == "--topo") return dumpTopology(argv[2], argv[3]);
+    if (argc == 5 && std::string(argv[1]) == "--vtk") return writeVtk(argv[2], std::atoi(argv[3]), argv[4]);
     if (argc < 4) {
         std::fprintf(stderr, "usage: %s <bc-file> <steps> <out.bin> [probe_every]\n", argv[0]);
         return 1;

@@ -7,7 +7,8 @@ cases and stores, per case:
   * the SHA-256 of the final FP64 population state (structure-of-arrays,
     little endian) -- the CPU oracle must reproduce it bit for bit,
   * the final density field (float64) for tolerance checks of the GPU path,
-  * the reference's boundary wiring (--topo) for two grid sizes.
+  * the reference's boundary wiring (--topo) for two grid sizes,
+  * the reference's legacy VTK file of one small case (--vtk) with its case file.
 This needs /root/reference; the fixtures it writes are committed.
 
 usage: python tests/golden/make_golden.py
@@ -89,9 +90,25 @@ def main():
         write_case_file(d, bc)
         out = os.path.join(HERE, "topo_%dx%dx%d.txt" % dims)
         subprocess.run([REF, "--topo", bc, out], check=True)
+    vtk_golden(tmp)
     for fn in os.listdir(tmp):
         os.remove(os.path.join(tmp, fn))
     os.rmdir(tmp)
+
+
+VTK_STEPS = 12
+
+
+def vtk_golden(tmp):
+    """the reference's own legacy VTK file (Lattice::writeResultsVTK) of a
+    9 x 7 x 5 single-level HRR case after 12 coarse steps, with its case file"""
+    d = small_case(9, 7, 5)
+    bc = os.path.join(tmp, "vtk_case.txt")
+    write_case_file(d, bc, steps=VTK_STEPS)
+    subprocess.run([REF, "--vtk", bc, str(VTK_STEPS), os.path.join(tmp, "ref")], check=True)
+    with open(bc) as src, open(os.path.join(HERE, "vtk_9x7x5_case.txt"), "w") as dst:
+        dst.write(src.read())
+    os.replace(os.path.join(tmp, "ref.vtk"), os.path.join(HERE, "vtk_9x7x5_12steps.vtk"))
 
 
 if __name__ == "__main__":

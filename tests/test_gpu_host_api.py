@@ -46,7 +46,12 @@ def test_driver_writes_vtk(tmp_path):
     r = subprocess.run([MAIN, str(bc), "10"], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr
     vtk = open(tmp_path / "pulse_10.vtk").read()
-    assert "DATASET STRUCTURED_POINTS" in vtk and "SCALARS Pressure" in vtk
+    # the reference's layout: one unstructured grid of every node, voxel cells
+    nx, ny, nz = c["dims"]
+    assert "DATASET UNSTRUCTURED_GRID" in vtk
+    assert f"POINTS {nx * ny * nz} " in vtk and f"CELL_TYPES {(nx - 1) * (ny - 1) * (nz - 1)}" in vtk
+    for field in ("SCALARS Pressure", "SCALARS Density", "SCALARS Omega", "VECTORS Velocity"):
+        assert field in vtk
 
 
 @pytest.mark.parametrize("levels", [1, 2])
@@ -133,3 +138,47 @@ def test_grid_coupling_views_of_a_refined_box(tmp_path):
     assert tags["left"] == tags["right"] == (fx - 2) * (fz - 2)
     assert tags["bottom"] == tags["top"] == (fx - 2) * (fy - 2)
     assert tags["bottomleftfront"] == 1 and tags["toprightback"] == 1
+
+
+def _vtk_parts(text):
+    """(structure lines, {section: numbers}) of a legacy VTK file: every line
+    that holds a keyword or integers verbatim, the floating-point tokens as
+    numbers per section (POINTS and each SCALARS / VECTORS field)"""
+    lines, nums, sec = [], {}, None
+    for line in text.split("\n"):
+        toks = line.split()
+        if toks and all(("e+" in t or "e-" in t) for t in toks):
+            nums.setdefault(sec, []).extend(float(t) for t in toks)
+        else:
+            lines.append(line)
+            if toks and toks[0] in ("POINTS", "SCALARS", "VECTORS"):
+                sec = toks[1] if toks[0] != "POINTS" else "POINTS"
+    return lines, {k: np.array(v) for k, v in nums.items()}
+
+
+def test_writeresultsvtk_reproduces_the_reference_file(tmp_path):
+    """Lattice::writeResultsVTK of the drop-in driver against the reference's
+    own file (tests/golden/vtk_9x7x5_12steps.vtk, written by the reference's
+    Lattice::writeResultsVTK, Lattice.cpp:4095-4352, after 12 steps of the same
+    case): the same header, point and cell counts, connectivity and section
+    order line for line, and every value to the 8 significant digits the file
+    keeps -- 2 units of the last digit, plus 1e-7 of the field's largest
+    value for the velocities: they are sums of +-xi f_q that cancel to about
+    1e-8 of each term, so the last bits in which the GPU's FP64 state differs
+    from the reference's show up at about 1e-8 of the largest velocity"""
+    case = open(os.path.join(HERE, "golden", "vtk_9x7x5_case.txt")).read()
+    case = case.replace("WriteInterval 1000000000", "WriteInterval 12")
+    case = case.replace("Save-as /tmp/acp_unused", "Save-as " + str(tmp_path / "out"))
+    bc = tmp_path / "BoundaryConditions.txt"
+    bc.write_text(case)
+    r = subprocess.run([MAIN, str(bc), "12"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    ref_lines, ref = _vtk_parts(open(os.path.join(HERE, "golden", "vtk_9x7x5_12steps.vtk")).read())
+    got_lines, got = _vtk_parts((tmp_path / "out_12.vtk").read_text())
+    assert got_lines == ref_lines
+    assert sorted(got) == sorted(ref) == sorted(["POINTS", "Pressure", "Density", "Omega", "Velocity"])
+    for sec in ref:
+        assert got[sec].shape == ref[sec].shape, sec
+        tol = 2e-7 * np.abs(ref[sec]) + (1e-7 * np.abs(ref[sec]).max() if sec == "Velocity" else 0.0)
+        bad = np.abs(got[sec] - ref[sec]) > tol
+        assert not bad.any(), (sec, np.flatnonzero(bad)[:5], got[sec][bad][:5], ref[sec][bad][:5])
