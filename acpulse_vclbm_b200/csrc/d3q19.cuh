@@ -38,46 +38,8 @@ __host__ __device__ constexpr int ez(int q) {
 __host__ __device__ constexpr double wq(int q) { return q < 6 ? 1.0 / 18.0 : (q < 18 ? 1.0 / 36.0 : 1.0 / 3.0); }
 
 // correctly rounded reciprocal (the same value as 1 / x under IEEE division)
-
-
-// Two FP32 values computed together with the packed FP32x2 instructions of
-// sm_100 (one FFMA2 / FADD2 / FMUL2 does the work of two scalar ones): the
-// collision of two nodes at once.  Constants and comparisons stay scalar and
-// constexpr, so coefficients known at compile time fold as in the scalar
-// code; every operation on data rounds to nearest like its scalar form.
-struct F2 {
-    float x, y;
-    F2() = default;
-    __host__ __device__ constexpr F2(double v) : x((float)v), y((float)v) {}
-    __host__ __device__ constexpr F2(float a, float b) : x(a), y(b) {}
-    __device__ __forceinline__ float2 f2() const { return make_float2(x, y); }
-    __device__ __forceinline__ static F2 of(float2 v) { return F2(v.x, v.y); }
-};
-__device__ __forceinline__ F2 operator+(F2 a, F2 b) { return F2::of(__fadd2_rn(a.f2(), b.f2())); }
-__device__ __forceinline__ F2 operator*(F2 a, F2 b) { return F2::of(__fmul2_rn(a.f2(), b.f2())); }
-// a - b as a + (-1) b: the product is exact, so this rounds once, like a - b
-__device__ __forceinline__ F2 operator-(F2 a, F2 b) { return F2::of(__ffma2_rn(b.f2(), make_float2(-1.f, -1.f), a.f2())); }
-__device__ __forceinline__ F2 operator-(F2 a) { return F2(-a.x, -a.y); }
-__device__ __forceinline__ F2 operator/(F2 a, F2 b) { return F2(a.x / b.x, a.y / b.y); }
-__device__ __forceinline__ F2& operator+=(F2& a, F2 b) { return a = a + b; }
-__device__ __forceinline__ F2& operator-=(F2& a, F2 b) { return a = a - b; }
-__device__ __forceinline__ F2& operator*=(F2& a, F2 b) { return a = a * b; }
-__host__ __device__ constexpr bool operator!=(F2 a, F2 b) { return a.x != b.x || a.y != b.y; }
-__device__ __forceinline__ F2 fma2(F2 a, F2 b, F2 c) { return F2::of(__ffma2_rn(a.f2(), b.f2(), c.f2())); }
-
-// the scalar type of a compute type (coefficients are formed in it)
-template <typename R>
-struct ScalarOf {
-    using type = R;
-};
-template <>
-struct ScalarOf<F2> {
-    using type = float;
-};
-
 __device__ __forceinline__ float rcpRN(float x) { return __frcp_rn(x); }
 __device__ __forceinline__ double rcpRN(double x) { return __drcp_rn(x); }
-__device__ __forceinline__ F2 rcpRN(F2 x) { return F2(__frcp_rn(x.x), __frcp_rn(x.y)); }
 
 // operator ids (enum acp_op)
 enum { OP_SRT = 0, OP_MRT_GS = 1, OP_MRT_RM = 2, OP_RR = 3, OP_HRR = 4 };
@@ -99,18 +61,14 @@ template <typename R>
 __device__ __forceinline__ void acc(R& s, R c, R x) {
     if (c != R(0)) s += c * x;
 }
-__device__ __forceinline__ void acc(F2& s, F2 c, F2 x) {
-    if (c != F2(0.0)) s = fma2(c, x, s);
-}
 
 // H2 : A for a symmetric tensor A = {xx, yy, zz, xy, xz, yz}
 template <typename R>
 __device__ __forceinline__ R h2dot(int q, const R* A) {
     R d = R(-0.0), o = R(-0.0);
-    using S = typename ScalarOf<R>::type;
-    acc(d, R(h2xx<S>(q)), A[0]);
-    acc(d, R(h2yy<S>(q)), A[1]);
-    acc(d, R(h2zz<S>(q)), A[2]);
+    acc(d, h2xx<R>(q), A[0]);
+    acc(d, h2yy<R>(q), A[1]);
+    acc(d, h2zz<R>(q), A[2]);
     acc(o, R(ex(q) * ey(q)), A[3]);
     acc(o, R(ex(q) * ez(q)), A[4]);
     acc(o, R(ey(q) * ez(q)), A[5]);
@@ -123,18 +81,17 @@ __device__ __forceinline__ R h2dot(int q, const R* A) {
 // yzz-xxy, yyz-xxz, xzz-xyy}
 template <typename R>
 __device__ __forceinline__ R h3dot(int q, const R* a) {
-    using S = typename ScalarOf<R>::type;  // the coefficients are compile-time constants
-    const S hx = S(ex(q)), hy = S(ey(q)), hz = S(ez(q));
-    const S xxy = h2xx<S>(q) * hy, xyy = h2yy<S>(q) * hx, xxz = h2xx<S>(q) * hz;
-    const S xzz = h2zz<S>(q) * hx, yyz = h2yy<S>(q) * hz, yzz = h2zz<S>(q) * hy;
+    const R hx = R(ex(q)), hy = R(ey(q)), hz = R(ez(q));
+    const R xxy = h2xx<R>(q) * hy, xyy = h2yy<R>(q) * hx, xxz = h2xx<R>(q) * hz;
+    const R xzz = h2zz<R>(q) * hx, yyz = h2yy<R>(q) * hz, yzz = h2zz<R>(q) * hy;
     R sym = R(-0.0);
-    acc(sym, R(xxy + yzz), a[0]);
-    acc(sym, R(xxz + yyz), a[1]);
-    acc(sym, R(xyy + xzz), a[2]);
+    acc(sym, xxy + yzz, a[0]);
+    acc(sym, xxz + yyz, a[1]);
+    acc(sym, xyy + xzz, a[2]);
     R t = R(3) * sym;
-    acc(t, R(yzz - xxy), a[3]);
-    acc(t, R(yyz - xxz), a[4]);
-    acc(t, R(xzz - xyy), a[5]);
+    acc(t, yzz - xxy, a[3]);
+    acc(t, yyz - xxz, a[4]);
+    acc(t, xzz - xyy, a[5]);
     return t;
 }
 
@@ -159,9 +116,8 @@ __device__ __forceinline__ void orth4(R pxxyy, R pxxzz, R pyyzz, R sxx, R syy, R
 template <typename R>
 __device__ __forceinline__ R h4dot(int q, const R* a4, R kappa) {
     R h[3];
-    using S = typename ScalarOf<R>::type;
-    orth4<R>(R(h2xx<S>(q) * h2yy<S>(q)), R(h2xx<S>(q) * h2zz<S>(q)), R(h2yy<S>(q) * h2zz<S>(q)), R(h2xx<S>(q)),
-             R(h2yy<S>(q)), R(h2zz<S>(q)), kappa, h);
+    orth4<R>(h2xx<R>(q) * h2yy<R>(q), h2xx<R>(q) * h2zz<R>(q), h2yy<R>(q) * h2zz<R>(q), h2xx<R>(q), h2yy<R>(q),
+             h2zz<R>(q), kappa, h);
     R t = R(-0.0);
     acc(t, R(8.0 / 7.0) * h[0], a4[0]);
     acc(t, R(56.0 / 45.0) * h[1], a4[1]);

@@ -724,7 +724,6 @@ TiledFn<S> pickTiled(const acp_case_desc& d) {
 template <typename S, typename R, int OP, int ORDER, bool CUBIC>
 TiledFn<S> marchKernel() {
     if constexpr (sizeof(R) == 8) return k_collide_push_march<S, R, OP, ORDER, CUBIC>;
-    else if constexpr (marchPairs<R>()) return k_collide_push_march2<S, R, OP, ORDER, CUBIC>;
     else return k_collide_push_march_f32<S, R, OP, ORDER, CUBIC>;
 }
 template <typename S, typename R>
@@ -784,8 +783,8 @@ int enqueueLevelStep(acp_handle* h, int l, int src, PhaseTimer* tm = nullptr, cu
     if (tm) tm->mark(-1);
     if (needsMoments(h->d) && marchesY(L)) {
         const int chunk = marchChunkFor(L, sizeof(R));
-        dim3 grid((L.nx + marchStepOf<R>() - 1) / marchStepOf<R>(), (L.ny + chunk - 1) / chunk);
-        pickMarch<S, R>(h->d)<<<grid, dim3(MARCH_TX, L.nz), marchSmemOf<R>(L.nz), st>>>(a, chunk);
+        dim3 grid((L.nx + MARCH_STEP - 1) / MARCH_STEP, (L.ny + chunk - 1) / chunk);
+        pickMarch<S, R>(h->d)<<<grid, dim3(MARCH_TX, L.nz), marchSmemBytes<R>(L.nz), st>>>(a, chunk);
     } else if (needsMoments(h->d)) {
         const int chunk = tiledChunkFor(L, TiledMinBlocks<R>::value);
         dim3 grid((L.nx + TX - 1) / TX, (L.ny + TY - 1) / TY, (L.nz + chunk - 1) / chunk);

@@ -913,129 +913,6 @@ __device__ __forceinline__ void marchBodyPrefetch(const LevelArgs<S>& a, int yCh
     }
 }
 
-// The y march with two x-adjacent nodes per lane (FP32 compute): lane t holds
-// the nodes x0 - 1 + 2t and x0 + 2t, so a block of 32 lanes covers 62 collided
-// nodes between two halo nodes.  Loads, moments and the neighbour terms of a
-// pair of fluid nodes, and their whole regularised collision, run on the
-// packed FP32x2 type (F2: one FFMA2 / FADD2 / FMUL2 for both nodes); a pair
-// with a boundary, coupling or dead node, or with a halo node, collides node
-// by node as in marchBody.  Row slots, chunks and directions as in marchBody.
-constexpr int MARCH2_NODES = 2 * MARCH_TX;     // node slots per row of a block
-constexpr int MARCH2_STEP = MARCH2_NODES - 2;  // collided x-nodes per block
-
-template <typename R>
-constexpr size_t march2SmemBytes(int nz) {
-    return sizeof(MomR<R>) * 4 * (size_t)nz * MARCH2_NODES;
-}
-
-// push of a pair of fluid nodes: lane x of the packed value to node nA's
-// targets, lane y to node nB's
-template <typename S>
-struct PairPusher {
-    const LevelArgs<S>& a;
-    int nA, nB;
-    NbOffsets oA, oB;
-    __device__ __forceinline__ void operator()(int q, F2 v) const {
-        if (q == 18) {
-            Store<S>::store(a.B + (18 * a.Ni + nA), v.x, scaleOf(a, 18));
-            Store<S>::store(a.B + (18 * a.Ni + nB), v.y, scaleOf(a, 18));
-        } else {
-            const int tA = nA + oA.dx[ex(q) + 1] + oA.dy[ey(q) + 1] + oA.dz[ez(q) + 1];
-            const int tB = nB + oB.dx[ex(q) + 1] + oB.dy[ey(q) + 1] + oB.dz[ez(q) + 1];
-            Store<S>::store(a.B + (q * a.Ni + tA), v.x, scaleOf(a, q));
-            Store<S>::store(a.B + (q * a.Ni + tB), v.y, scaleOf(a, q));
-        }
-    }
-};
-
-__device__ __forceinline__ MomR<F2> pairMom(const MomR<float>& a, const MomR<float>& b) {
-    MomR<F2> m;
-    m.drho = F2(a.drho, b.drho);
-    m.ux = F2(a.ux, b.ux);
-    m.uy = F2(a.uy, b.uy);
-    m.uz = F2(a.uz, b.uz);
-    return m;
-}
-
-template <typename S, int OP, int ORDER, bool CUBIC>
-__device__ __forceinline__ void marchBodyPair(const LevelArgs<S>& a, int yChunk, int bx, int by, MomR<float>* sm) {
-    const int tx = threadIdx.x, tz = threadIdx.y, nz = a.nz;
-    auto at = [&](int s, int z, int x) -> MomR<float>& { return sm[(s * nz + z) * MARCH2_NODES + x]; };
-    const int pA = 2 * tx, pB = 2 * tx + 1;  // the lane's node slots in a row
-    const int xa = bx * MARCH2_STEP - 1 + pA, xb = xa + 1;
-    const int wa = wrapm(xa, a.nx, a.per[0]), wb = wrapm(xb, a.nx, a.per[0]);
-    const bool collA = tx > 0 && xa < a.nx, collB = tx < MARCH_TX - 1 && xb < a.nx;
-    const int yBeg = by * yChunk;
-    const int yEnd = min(a.ny, yBeg + yChunk);
-    const int zpl = tz + 1 == nz ? 0 : tz + 1, zmi = tz == 0 ? nz - 1 : tz - 1;
-    // moments of both nodes of row y (wrapped) into slot s, the pair's
-    // second-order sums into s2 (a node outside the lattice or dead writes
-    // no record)
-    auto rowPass = [&](int s, int y, F2* s2) {
-        const int nA = (tz * a.ny + y) * a.nx + wa, nB = (tz * a.ny + y) * a.nx + wb;
-        const bool lA = wa >= 0 && a.code[nA] != CODE_DEAD, lB = wb >= 0 && a.code[nB] != CODE_DEAD;
-        F2 g[Q];
-#pragma unroll
-        for (int q = 0; q < Q; ++q)
-            g[q] = F2(lA ? float(Store<S>::load(a.A + (q * a.Ni + nA), scaleOf(a, q))) : 0.f,
-                      lB ? float(Store<S>::load(a.A + (q * a.Ni + nB), scaleOf(a, q))) : 0.f);
-        F2 d, jj[3];
-        pairMoments<F2>(g, d, jj, s2);
-        const F2 inv = rcpRN(F2(a.shift) + d);
-        const F2 ux = jj[0] * inv, uy = jj[1] * inv, uz = jj[2] * inv;
-        if (lA) at(s, tz, pA) = MomR<float>{d.x, ux.x, uy.x, uz.x};
-        if (lB) at(s, tz, pB) = MomR<float>{d.y, ux.y, uy.y, uz.y};
-    };
-    const int len = yEnd - yBeg;
-    const int dir = (by & 1) ? -1 : 1;
-    auto rowAt = [&](int st) { return dir > 0 ? yBeg + st : yEnd - 1 - st; };
-    auto key = [](int st) { return (st + 1) & 3; };
-    F2 cur[6], nxt[6];
-    {
-        const int ym = wrapc(rowAt(-1), a.ny, a.per[1]);
-        if (ym >= 0) rowPass(key(-1), ym, nxt);  // moments only
-        rowPass(key(0), rowAt(0), cur);
-    }
-    for (int st = 0; st < len; ++st) {
-        const int y = rowAt(st);
-        const int yn = wrapc(rowAt(st + 1), a.ny, a.per[1]);
-        if (yn >= 0) rowPass(key(st + 1), yn, nxt);
-        __syncthreads();
-        const int sc = key(st);
-        const int sp = dir > 0 ? key(st + 1) : key(st - 1);  // row y + 1
-        const int sn = dir > 0 ? key(st - 1) : key(st + 1);  // row y - 1
-        const int nA = (tz * a.ny + y) * a.nx + xa, nB = nA + 1;
-        const uint8_t cA = collA ? a.code[nA] : CODE_DEAD, cB = collB ? a.code[nB] : CODE_DEAD;
-        if (cA == CODE_FLUID && cB == CODE_FLUID) {
-            const MomR<F2> me = pairMom(at(sc, tz, pA), at(sc, tz, pB));
-            F2 SG[12];
-            neighbourTerms<F2, OP == OP_HRR, CUBIC>(
-                pairMom(at(sc, tz, pA + 1), at(sc, tz, pB + 1)), pairMom(at(sc, tz, pA - 1), at(sc, tz, pB - 1)),
-                pairMom(at(sp, tz, pA), at(sp, tz, pB)), pairMom(at(sn, tz, pA), at(sn, tz, pB)),
-                pairMom(at(sc, zpl, pA), at(sc, zpl, pB)), pairMom(at(sc, zmi, pA), at(sc, zmi, pB)), F2(a.shift), SG);
-            PairPusher<S> emit{a, nA, nB, nbOffsets(a, xa, y, tz), nbOffsets(a, xb, y, tz)};
-            const F2 u[3] = {me.ux, me.uy, me.uz};
-            regularisedEmit<F2, OP, ORDER, CUBIC>(me.drho, u, cur, a, SG, emit);
-        } else {
-            // node by node (boundary, coupling, dead or halo nodes in the pair)
-            if (collA) {
-                const float s2[6] = {cur[0].x, cur[1].x, cur[2].x, cur[3].x, cur[4].x, cur[5].x};
-                tiledCollide<S, float, OP, ORDER, CUBIC>(a, nA, xa, y, tz, cA, at(sc, tz, pA), at(sc, tz, pA + 1),
-                                                         at(sc, tz, pA - 1), at(sp, tz, pA), at(sn, tz, pA),
-                                                         at(sc, zpl, pA), at(sc, zmi, pA), s2);
-            }
-            if (collB) {
-                const float s2[6] = {cur[0].y, cur[1].y, cur[2].y, cur[3].y, cur[4].y, cur[5].y};
-                tiledCollide<S, float, OP, ORDER, CUBIC>(a, nB, xb, y, tz, cB, at(sc, tz, pB), at(sc, tz, pB + 1),
-                                                         at(sc, tz, pB - 1), at(sp, tz, pB), at(sn, tz, pB),
-                                                         at(sc, zpl, pB), at(sc, zmi, pB), s2);
-            }
-        }
-#pragma unroll
-        for (int c = 0; c < 6; ++c) cur[c] = nxt[c];
-    }
-}
-
 // Measured on the 1024 x 512 x 3 two-level HRR workload (collide time per
 // coarse step): FP64 1087 us with the prefetch against 1093 us without; FP32
 // 568 us without it at 64 registers (five blocks of 32 x 6 per SM) against
@@ -1055,32 +932,6 @@ __global__ void __launch_bounds__(MARCH_TX * MARCH_MAX_NZ, TiledMinBlocks<R>::va
                                                   reinterpret_cast<MomR<R>*>(marchSmem));
     else
         marchBody<S, R, OP, ORDER, CUBIC>(a, yChunk, blockIdx.x, blockIdx.y, reinterpret_cast<MomR<R>*>(marchSmem));
-}
-
-#ifndef ACP_MARCH2_REGS
-#define ACP_MARCH2_REGS 112
-#endif
-// single-case FP32-compute levels march with two nodes per lane
-#ifndef ACP_MARCH_PAIRS
-#define ACP_MARCH_PAIRS 1
-#endif
-// collided x-nodes per march block and its dynamic shared memory
-template <typename R>
-constexpr bool marchPairs() {
-    return sizeof(R) == 4 && ACP_MARCH_PAIRS;
-}
-template <typename R>
-constexpr int marchStepOf() {
-    return marchPairs<R>() ? MARCH2_STEP : MARCH_STEP;
-}
-template <typename R>
-constexpr size_t marchSmemOf(int nz) {
-    return marchPairs<R>() ? march2SmemBytes<R>(nz) : marchSmemBytes<R>(nz);
-}
-template <typename S, typename R, int OP, int ORDER, bool CUBIC>
-__global__ void __maxnreg__(ACP_MARCH2_REGS) k_collide_push_march2(LevelArgs<S> a, int yChunk) {
-    extern __shared__ __align__(16) unsigned char marchSmem[];
-    marchBodyPair<S, OP, ORDER, CUBIC>(a, yChunk, blockIdx.x, blockIdx.y, reinterpret_cast<MomR<float>*>(marchSmem));
 }
 
 // FP32 compute: the register cap set directly, so that blocks of 32 x 6
