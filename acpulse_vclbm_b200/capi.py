@@ -52,7 +52,8 @@ class CaseDesc(C.Structure):
         ("ic_center", C.c_double * 3),
         ("ic_dims", C.c_int),
         ("storage", C.c_int),
-        ("reserved", C.c_int * 8),
+        ("lodi_length_nodes", C.c_int * 3),
+        ("reserved", C.c_int * 5),
     ]
 
     def copy(self):

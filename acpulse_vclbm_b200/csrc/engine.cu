@@ -95,6 +95,8 @@ int validate(const acp_case_desc* d, std::string& why) {
             return ACP_ERR_UNSUPPORTED;
         }
     }
+    for (int a = 0; a < 3; ++a)
+        if (d->lodi_length_nodes[a] < 0) { why = "negative LODI length"; return ACP_ERR_INVALID; }
     if (d->max_level != 0 && d->max_level != 1) { why = "MaxLevel must be 0 or 1"; return ACP_ERR_INVALID; }
     if (d->max_level == 1) {
         if (d->layout != ACP_LAYOUT_BOX && d->layout != ACP_LAYOUT_SHELL) { why = "unknown refinement layout"; return ACP_ERR_INVALID; }
@@ -1351,6 +1353,67 @@ int acp_node_kind(acp_handle* h, int level, int i, int j, int k, int* id, int* f
 int acp_read_populations_other(acp_handle* h, int level, double* out) {
     if (!h || !out || level < 0 || level >= (int)h->host.size()) return ACP_ERR_INVALID;
     return readArray(h, level, level == 0 ? (h->cur ^ 1) : 1, out);
+}
+
+// the x-columns [x0, x0 + ncols) of a single-level case's current array in
+// storage form, as one strided copy: the array is 19 * nz * ny rows of nx
+// values, the columns a block of ncols values in every row
+static int columnsCopy(acp_handle* h, int ncols, void* dst, size_t dpitch, const void* src, size_t spitch,
+                       size_t rows) {
+    const size_t sb = storageBytes(h->d.storage);
+    CU(h, cudaMemcpy2DAsync(dst, dpitch, src, spitch, (size_t)ncols * sb, rows, cudaMemcpyDefault, h->stream));
+    CU(h, cudaStreamSynchronize(h->stream));
+    return ACP_OK;
+}
+
+static int columnsCheck(acp_handle* h, int x0, int ncols) {
+    if (!h || h->host.size() != 1) return h ? fail(h, ACP_ERR_UNSUPPORTED, "columns: single-level cases only")
+                                            : ACP_ERR_INVALID;
+    if (!h->inited) return fail(h, ACP_ERR_STATE, "columns: case not initialised");
+    if (h->batch) return fail(h, ACP_ERR_STATE, "columns: the case is stepped by a batch");
+    const LevelHost& L = h->host[0];
+    if (ncols < 0 || x0 < 0 || x0 > L.nx - ncols) return fail(h, ACP_ERR_INVALID, "columns [%d, %d) outside 0..%d", x0,
+                                                               x0 + ncols, L.nx);
+    return ACP_OK;
+}
+
+int acp_get_columns(acp_handle* h, int x0, int ncols, void* buf) {
+    int s = columnsCheck(h, x0, ncols);
+    if (s) return s;
+    if (!buf) return fail(h, ACP_ERR_INVALID, "columns: null buffer");
+    CU(h, cudaSetDevice(h->device));
+    const LevelHost& L = h->host[0];
+    const size_t sb = storageBytes(h->d.storage);
+    const char* arr = (const char*)h->dev[0].f[h->cur] + (size_t)x0 * sb;
+    return columnsCopy(h, ncols, buf, (size_t)ncols * sb, arr, (size_t)L.nx * sb, (size_t)Q * L.ny * L.nz);
+}
+
+int acp_put_columns(acp_handle* h, int x0, int ncols, const void* buf) {
+    int s = columnsCheck(h, x0, ncols);
+    if (s) return s;
+    if (!buf) return fail(h, ACP_ERR_INVALID, "columns: null buffer");
+    CU(h, cudaSetDevice(h->device));
+    const LevelHost& L = h->host[0];
+    const size_t sb = storageBytes(h->d.storage);
+    char* arr = (char*)h->dev[0].f[h->cur] + (size_t)x0 * sb;
+    return columnsCopy(h, ncols, arr, (size_t)L.nx * sb, buf, (size_t)ncols * sb, (size_t)Q * L.ny * L.nz);
+}
+
+int acp_copy_columns(acp_handle* dst, int dst_x0, acp_handle* src, int src_x0, int ncols) {
+    int s = columnsCheck(dst, dst_x0, ncols);
+    if (s) return s;
+    if ((s = columnsCheck(src, src_x0, ncols))) return fail(dst, s, "source: %s", src->err.c_str());
+    const LevelHost& D = dst->host[0];
+    const LevelHost& S = src->host[0];
+    if (D.ny != S.ny || D.nz != S.nz || dst->d.storage != src->d.storage || dst->shift != src->shift)
+        return fail(dst, ACP_ERR_INVALID, "columns: the cases differ in ny, nz or storage form");
+    CU(dst, cudaSetDevice(src->device));
+    CU(dst, cudaStreamSynchronize(src->stream));  // the source's queued steps
+    CU(dst, cudaSetDevice(dst->device));
+    const size_t sb = storageBytes(dst->d.storage);
+    char* d = (char*)dst->dev[0].f[dst->cur] + (size_t)dst_x0 * sb;
+    const char* sp = (const char*)src->dev[0].f[src->cur] + (size_t)src_x0 * sb;
+    return columnsCopy(dst, ncols, d, (size_t)D.nx * sb, sp, (size_t)S.nx * sb, (size_t)Q * D.ny * D.nz);
 }
 
 int acp_read_populations_window(acp_handle* h, int level, long long begin, int count, double* out) {

@@ -181,9 +181,9 @@ inline LodiArgs lodiArgsOf(const acp_handle* h, int l) {
     p.dt = L.dt;
     p.localSpacing = h->d.spacing * std::pow(2.0, -(double)l);
     p.kappa = h->kappa;
-    p.domainLength[0] = h->d.nx * h->d.spacing;
-    p.domainLength[1] = h->d.ny * h->d.spacing;
-    p.domainLength[2] = h->d.nz * h->d.spacing;
+    const int dims[3] = {h->d.nx, h->d.ny, h->d.nz};
+    for (int a = 0; a < 3; ++a)
+        p.domainLength[a] = (h->d.lodi_length_nodes[a] > 0 ? h->d.lodi_length_nodes[a] : dims[a]) * h->d.spacing;
     p.order = h->d.eq_order;
     p.errorFlag = h->dErr;
     return p;

@@ -41,6 +41,9 @@ def lib():
         L.acp_active_updates.argtypes = [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
         L.acp_read_populations.argtypes = [vp, C.c_int, vp]
         L.acp_read_populations_other.argtypes = [vp, C.c_int, vp]
+        L.acp_get_columns.argtypes = [vp, C.c_int, C.c_int, vp]
+        L.acp_put_columns.argtypes = [vp, C.c_int, C.c_int, vp]
+        L.acp_copy_columns.argtypes = [vp, C.c_int, vp, C.c_int, C.c_int]
         L.acp_write_populations.argtypes = [vp, C.c_int, vp]
         L.acp_read_field.argtypes = [vp, C.c_int, C.c_int, vp]
         L.acp_set_probes.argtypes = [vp, C.c_int, vp]

@@ -117,7 +117,11 @@ typedef struct acp_case_desc {
     int ic_dims;               /* 2: r^2 over x,y only (quasi-2D pulse); 3: over x,y,z */
     /* precision */
     int storage;               /* enum acp_storage */
-    int reserved[8];
+    /* LODI relaxation length per axis in coarse nodes: the reference's L =
+     * NumberOfNodes_axis * Spacing (Node.cpp:311); 0 takes the case's own
+     * nx, ny, nz.  A slab of a lattice split in x keeps the whole lattice's. */
+    int lodi_length_nodes[3];
+    int reserved[5];
 } acp_case_desc;
 
 typedef struct acp_handle acp_handle;
@@ -172,8 +176,23 @@ int acp_read_populations_other(acp_handle* h, int level, double* host_out);
  * other level, or outside it).  *face_class: the face class
  * (fx+1)*9 + (fy+1)*3 + (fz+1) of a boundary node's domain faces or of a
  * coupling node's interface faces (outward normals of the level's live
- * region), 13 otherwise.  Host data only: no device call. */
+ * region) on the level that lies inside the refined box (the other level's
+ * coupling nodes keep no face class), 13 otherwise.  Host data only: no
+ * device call. */
 int acp_node_kind(acp_handle* h, int level, int i, int j, int k, int* id, int* face_class);
+/* x-columns of a single-level case's current state in its storage form, for
+ * a lattice split into x slabs over several GPUs (one case per slab; the
+ * reference runs one lattice on one host, Lattice.cpp:1505-1507, and has no
+ * counterpart).  The columns [x0, x0 + ncols) of all 19 populations are
+ * packed as [q][k][j][ncols] values of the storage type (8, 4 or 2 bytes):
+ * acp_get_columns copies them into buf, acp_put_columns writes them back
+ * from buf, and acp_copy_columns copies them from one case straight into
+ * another (same ny, nz and storage form; the cases may be on different
+ * devices of one process).  buf may be host or device memory.  Each call
+ * waits for the cases' queued steps and finishes its copy before returning. */
+int acp_get_columns(acp_handle* h, int x0, int ncols, void* buf);
+int acp_put_columns(acp_handle* h, int x0, int ncols, const void* buf);
+int acp_copy_columns(acp_handle* dst, int dst_x0, acp_handle* src, int src_x0, int ncols);
 /* Overwrite a level's populations (both ping-pong arrays) from FP64 f_i. */
 int acp_write_populations(acp_handle* h, int level, const double* host_in);
 /* Checkpoint / restart of a case's device state.  The reference keeps no

@@ -492,9 +492,11 @@ struct Oracle {
         int perm[3];
         bool neg;
         double L0;
-        if (nd == 0 || nd == 2) { perm[0] = 0; perm[1] = 1; perm[2] = 2; L0 = desc.nx * k.spacing; }
-        else if (nd == 1 || nd == 3) { perm[0] = 1; perm[1] = 0; perm[2] = 2; L0 = desc.ny * k.spacing; }
-        else { perm[0] = 2; perm[1] = 0; perm[2] = 1; L0 = desc.nz * k.spacing; }
+        // L = NumberOfNodes_axis * Spacing (Node.cpp:311), or the case's override
+        auto lodiNodes = [&](int a, int n) { return desc.lodi_length_nodes[a] > 0 ? desc.lodi_length_nodes[a] : n; };
+        if (nd == 0 || nd == 2) { perm[0] = 0; perm[1] = 1; perm[2] = 2; L0 = lodiNodes(0, desc.nx) * k.spacing; }
+        else if (nd == 1 || nd == 3) { perm[0] = 1; perm[1] = 0; perm[2] = 2; L0 = lodiNodes(1, desc.ny) * k.spacing; }
+        else { perm[0] = 2; perm[1] = 0; perm[2] = 1; L0 = lodiNodes(2, desc.nz) * k.spacing; }
         neg = (nd == 0 || nd == 1 || nd == 4);
         if (neg) {
             dG *= -1.;
@@ -1335,6 +1337,18 @@ int orc_write_populations(void* h, int level, const double* in) {
     for (int a = 0; a < 2; ++a)
         for (long n = 0; n < L.N; ++n)
             for (int q = 0; q < orc::Q; ++q) L.f[a][n * orc::Q + q] = in[(long)q * L.N + n];
+    return 0;
+}
+
+// the current array only (the other array keeps what the steps left in it,
+// as the engine's acp_put_columns does)
+int orc_write_current(void* h, int level, const double* in) {
+    Oracle* o = static_cast<Oracle*>(h);
+    if (level < 0 || level >= (int)o->lev.size()) return -1;
+    orc::Level& L = o->lev[level];
+    double* f = L.f[level == 0 ? o->alt : o->altf].data();
+    for (long n = 0; n < L.N; ++n)
+        for (int q = 0; q < orc::Q; ++q) f[n * orc::Q + q] = in[(long)q * L.N + n];
     return 0;
 }
 

@@ -41,6 +41,7 @@ def lib():
         L.orc_dims.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int)]
         L.orc_read_populations.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
         L.orc_write_populations.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        L.orc_write_current.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
         L.orc_steps_done.restype = C.c_longlong
         L.orc_steps_done.argtypes = [C.c_void_p]
         L.orc_destroy.argtypes = [C.c_void_p]
@@ -87,9 +88,11 @@ class OracleLattice:
                 raise ValueError("probe outside its level")
         return out
 
-    def write_populations(self, f, level=0):
+    def write_populations(self, f, level=0, current_only=False):
+        """FP64 f_i of a level into both arrays, or the current one only"""
         f = np.ascontiguousarray(f, dtype=np.float64)
-        lib().orc_write_populations(self._h, level, f.ctypes.data)
+        fn = lib().orc_write_current if current_only else lib().orc_write_populations
+        fn(self._h, level, f.ctypes.data)
 
     def close(self):
         if self._h:
