@@ -151,6 +151,33 @@ struct EqCoef {
         if (ORDER == 4) p += R(20.25) * h4dot<R>(q, a4, kappa);
         return p;
     }
+    // w_q times the even and odd parts below, w_q folded into the constant
+    // coefficients: adds to `even` (which carries w_q drho on entry) and `odd`
+    __device__ __forceinline__ void weightedTerms(int q, R kappa, R& even, R& odd) const {
+        const R w = R(wq(q));
+        const R c2 = w * R(4.5), c3 = w * R(4.5);
+        acc(odd, w * R(3 * ex(q)), u[0]);
+        acc(odd, w * R(3 * ey(q)), u[1]);
+        acc(odd, w * R(3 * ez(q)), u[2]);
+        acc(even, c2 * h2xx<R>(q), uu[0]);
+        acc(even, c2 * h2yy<R>(q), uu[1]);
+        acc(even, c2 * h2zz<R>(q), uu[2]);
+        acc(even, c2 * R(2 * ex(q) * ey(q)), uu[3]);
+        acc(even, c2 * R(2 * ex(q) * ez(q)), uu[4]);
+        acc(even, c2 * R(2 * ey(q) * ez(q)), uu[5]);
+        if (ORDER >= 3) {
+            const R hx = R(ex(q)), hy = R(ey(q)), hz = R(ez(q));
+            const R xxy = h2xx<R>(q) * hy, xyy = h2yy<R>(q) * hx, xxz = h2xx<R>(q) * hz;
+            const R xzz = h2zz<R>(q) * hx, yyz = h2yy<R>(q) * hz, yzz = h2zz<R>(q) * hy;
+            acc(odd, c3 * R(3) * (xxy + yzz), a3[0]);
+            acc(odd, c3 * R(3) * (xxz + yyz), a3[1]);
+            acc(odd, c3 * R(3) * (xyy + xzz), a3[2]);
+            acc(odd, c3 * (yzz - xxy), a3[3]);
+            acc(odd, c3 * (yyz - xxz), a3[4]);
+            acc(odd, c3 * (xzz - xyy), a3[5]);
+        }
+        if (ORDER == 4) even += (w * R(20.25)) * h4dot<R>(q, a4, kappa);
+    }
     // the same polynomial split into its even (second and fourth order) and
     // odd (first and third order) parts: direction q gives even + odd, its
     // opposite even - odd
@@ -179,6 +206,26 @@ __device__ __forceinline__ void forEachDirection(const EqCoef<R, ORDER>& c, R ka
         f(pairB(p), even - odd);
     }
     f(18, c.poly(18, kappa));
+}
+
+// visit (q, w_q (drho + p_q)) for every direction of the polynomial p of the
+// coefficients c: per pair the weighted even sum, started from w_q drho, and
+// the weighted odd sum give w_q (drho + p) = even + odd and, for the opposite
+// direction, even - odd, so no direction needs its own add and multiply
+template <typename R, int ORDER, typename F>
+__device__ __forceinline__ void forEachWeighted(const EqCoef<R, ORDER>& c, R drho, R kappa, F&& f) {
+    const R axis = R(wq(0)) * drho, diag = R(wq(6)) * drho;
+#pragma unroll
+    for (int p = 0; p < 9; ++p) {
+        const int q = pairA(p);
+        R even = q < 6 ? axis : diag, odd = R(-0.0);
+        c.weightedTerms(q, kappa, even, odd);
+        f(q, even + odd);
+        f(pairB(p), even - odd);
+    }
+    R even = R(wq(18)) * drho, odd = R(-0.0);
+    c.weightedTerms(18, kappa, even, odd);
+    f(18, even);
 }
 
 // Recursive off-equilibrium of a second-order coefficient tensor A

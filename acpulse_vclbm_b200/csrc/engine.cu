@@ -14,8 +14,12 @@
 #include <cstring>
 #include <utility>
 #include <algorithm>
+#include <condition_variable>
+#include <functional>
 #include <mutex>
 #include <thread>
+
+#include <pthread.h>
 #include <string>
 #include <vector>
 
@@ -146,38 +150,89 @@ int validate(const acp_case_desc* d, std::string& why) {
     return ACP_OK;
 }
 
+// Host threads of the set-up scans: created on first use and kept for the
+// life of the process (starting threads for every scan cost as much as the
+// scans of a 6 M-node level).  One scan runs at a time; callers on other
+// threads wait for the pool.  A forked child starts a pool of its own.
+class ScanPool {
+  public:
+    static constexpr int kMax = 16;
+    static ScanPool& get() {
+        static std::once_flag once;
+        std::call_once(once, [] { pthread_atfork(nullptr, nullptr, [] { instance() = nullptr; }); });
+        std::lock_guard<std::mutex> g(creation());
+        if (!instance()) instance() = new ScanPool();  // kept until the process exits
+        return *instance();
+    }
+    int threads() const { return T_; }
+    // job(t) for t in [0, threads()), the caller running t = 0
+    void run(const std::function<void(int)>& job) {
+        std::lock_guard<std::mutex> one(busy_);
+        {
+            std::lock_guard<std::mutex> g(m_);
+            job_ = &job;
+            pending_ = T_ - 1;
+            ++gen_;
+        }
+        cv_.notify_all();
+        job(0);
+        std::unique_lock<std::mutex> g(m_);
+        done_.wait(g, [this] { return pending_ == 0; });
+        job_ = nullptr;
+    }
+
+  private:
+    ScanPool() : T_(std::max(1, std::min(kMax, (int)std::thread::hardware_concurrency()))) {
+        for (int t = 1; t < T_; ++t) std::thread([this, t] { work(t); }).detach();
+    }
+    static ScanPool*& instance() {
+        static ScanPool* p = nullptr;
+        return p;
+    }
+    static std::mutex& creation() {
+        static std::mutex m;
+        return m;
+    }
+    void work(int t) {
+        unsigned long long seen = 0;
+        for (;;) {
+            const std::function<void(int)>* job;
+            {
+                std::unique_lock<std::mutex> g(m_);
+                cv_.wait(g, [&] { return gen_ != seen; });
+                seen = gen_;
+                job = job_;
+            }
+            (*job)(t);
+            std::lock_guard<std::mutex> g(m_);
+            if (--pending_ == 0) done_.notify_one();
+        }
+    }
+    const int T_;
+    std::mutex m_, busy_;
+    std::condition_variable cv_, done_;
+    const std::function<void(int)>* job_ = nullptr;
+    int pending_ = 0;
+    unsigned long long gen_ = 0;
+};
+
 // The node scans of the set-up run over the host's cores: rows (j, k) of a
-// level split into contiguous ranges, one per thread, so that per-thread
-// results concatenated in thread order are in node order.
+// level split into contiguous ranges, one per pool thread (index t < 16), so
+// that per-thread results concatenated in thread order are in node order.
 template <typename F>
 void forRows(long long rows, F&& fn) {
-    const int T = std::max(1, std::min(16, (int)std::thread::hardware_concurrency()));
-    if (rows < 256 || T == 1) {
+    if (rows < 256) {
         fn(0LL, rows, 0);
         return;
     }
-    std::vector<std::thread> pool;
-    for (int t = 0; t < T; ++t) pool.emplace_back([&fn, rows, t, T] { fn(rows * t / T, rows * (t + 1) / T, t); });
-    for (std::thread& th : pool) th.join();
-}
-
-// indices, in increasing order, of the nodes (i, j, k) of L for which pred(n, i, j, k) holds
-template <typename P>
-std::vector<long long> scanNodes(const LevelHost& L, P pred) {
-    const int T = std::max(1, std::min(16, (int)std::thread::hardware_concurrency()));
-    std::vector<std::vector<long long>> part(T);
-    forRows((long long)L.ny * L.nz, [&](long long r0, long long r1, int t) {
-        for (long long r = r0; r < r1; ++r) {
-            const int j = (int)(r % L.ny), k = (int)(r / L.ny);
-            for (int i = 0; i < L.nx; ++i) {
-                const long long n = r * L.nx + i;
-                if (pred(n, i, j, k)) part[t].push_back(n);
-            }
-        }
-    });
-    std::vector<long long> out;
-    for (auto& v : part) out.insert(out.end(), v.begin(), v.end());
-    return out;
+    ScanPool& pool = ScanPool::get();
+    const int T = pool.threads();
+    if (T == 1) {
+        fn(0LL, rows, 0);
+        return;
+    }
+    const std::function<void(int)> job = [&fn, rows, T](int t) { fn(rows * t / T, rows * (t + 1) / T, t); };
+    pool.run(job);
 }
 
 // LODI wiring and node classes of a level whose dead / coupling nodes are
@@ -213,8 +268,7 @@ int wireLevel(acp_handle* h, LevelHost& L, int level) {
     // scanned whole, any other row holds at most its two x-face nodes
     std::vector<long long> faceNodes;
     {
-        const int T = std::max(1, std::min(16, (int)std::thread::hardware_concurrency()));
-        std::vector<std::vector<long long>> part(T);
+        std::vector<std::vector<long long>> part(ScanPool::kMax);
         forRows((long long)L.ny * L.nz, [&](long long r0, long long r1, int t) {
             for (long long r = r0; r < r1; ++r) {
                 const int j = (int)(r % L.ny), k = (int)(r / L.ny);
@@ -257,14 +311,7 @@ int wireLevel(acp_handle* h, LevelHost& L, int level) {
                 }
                 (fc[0] != 0 ? L.lodiX : L.lodiZY).push_back(b);
             }
-    std::vector<long long> live(16, 0);
-    forRows((long long)L.ny * L.nz, [&](long long r0, long long r1, int t) {
-        long long c = 0;
-        for (long long n = r0 * L.nx; n < r1 * L.nx; ++n) c += L.code[n] != CODE_DEAD;
-        live[t] = c;
-    });
-    L.active = 0;
-    for (long long c : live) L.active += c;
+    L.active = L.N - L.dead;
     L.spacing = d.spacing / std::pow(2.0, (double)level);
     L.dt = d.spacing / (d.speed_of_sound * std::sqrt(3.0)) / std::pow(2.0, (double)level);
     const double cs2 = d.speed_of_sound * d.speed_of_sound;
@@ -315,10 +362,14 @@ struct CouplingGeom {
 // segment instead of testing every node.
 void markLevel(LevelHost& L, const CouplingGeom& g) {
     L.code.assign(L.N, CODE_FLUID);
-    auto setCoupling = [&](long long n, const int* c) {
+    // coupling nodes and dead-node counts per pool thread, in node order
+    std::vector<std::vector<long long>> part(ScanPool::kMax);
+    std::vector<long long> dead(ScanPool::kMax, 0);
+    auto setCoupling = [&](long long n, const int* c, int t) {
         int f[3];
         g.normal(c, f);
         L.code[n] = (uint8_t)(CODE_IFACE0 + (g.inside ? faceCode(f[0], f[1], f[2]) : CODE_FLUID));
+        part[t].push_back(n);
     };
     // strictly-inside range of an axis (the covered nodes of a level outside its box)
     int dlo[3], dhi[3];
@@ -326,7 +377,7 @@ void markLevel(LevelHost& L, const CouplingGeom& g) {
         dlo[a] = g.loIf[a] ? g.cl[a] + 1 : g.cl[a];
         dhi[a] = g.hiIf[a] ? g.ch[a] - 1 : g.ch[a];
     }
-    forRows((long long)L.ny * L.nz, [&](long long r0, long long r1, int) {
+    forRows((long long)L.ny * L.nz, [&](long long r0, long long r1, int t) {
         for (long long r = r0; r < r1; ++r) {
             const int j = (int)(r % L.ny), k = (int)(r / L.ny);
             if (j < g.cl[1] || j > g.ch[1] || k < g.cl[2] || k > g.ch[2]) continue;  // row misses the box
@@ -338,22 +389,33 @@ void markLevel(LevelHost& L, const CouplingGeom& g) {
                 // a face coordinate lies outside the strictly-inside range: nothing dead
                 for (int i = std::max(0, g.cl[0]); i <= std::min(L.nx - 1, g.ch[0]); ++i) {
                     const int c[3] = {i, j, k};
-                    setCoupling(row + i, c);
+                    setCoupling(row + i, c, t);
                 }
                 continue;
             }
-            if (!g.inside && innerRow && dlo[0] <= dhi[0])
-                std::fill(L.code.begin() + row + std::max(0, dlo[0]), L.code.begin() + row + std::min(L.nx - 1, dhi[0]) + 1,
-                          CODE_DEAD);
+            if (!g.inside && innerRow && dlo[0] <= dhi[0]) {
+                const int i0 = std::max(0, dlo[0]), i1 = std::min(L.nx - 1, dhi[0]);
+                if (i0 <= i1) {
+                    std::fill(L.code.begin() + row + i0, L.code.begin() + row + i1 + 1, CODE_DEAD);
+                    dead[t] += i1 - i0 + 1;
+                }
+            }
+            // the x-face coupling nodes lie outside the dead segment, lower face first
             const int xs[2] = {g.loIf[0] ? g.cl[0] : -1, g.hiIf[0] ? g.ch[0] : -1};
             for (int e = 0; e < 2; ++e) {
                 const int i = xs[e];
                 if (i < 0 || i >= L.nx || (e == 1 && i == xs[0])) continue;
                 const int c[3] = {i, j, k};
-                setCoupling(row + i, c);
+                setCoupling(row + i, c, t);
             }
         }
     });
+    L.coupling.clear();
+    L.dead = 0;
+    for (int t = 0; t < ScanPool::kMax; ++t) {
+        L.coupling.insert(L.coupling.end(), part[t].begin(), part[t].end());
+        L.dead += dead[t];
+    }
 }
 
 // Two levels.  Box layout: the fine level covers the box [box_lo, box_hi]
@@ -436,10 +498,7 @@ int buildTwoLevel(acp_handle* h) {
         return true;
     };
     std::vector<C2FDev> coinc, mid, cen;
-    auto isCoupling = [](const LevelHost& L) {
-        return [&L](long long n, int, int, int) { return L.code[n] >= CODE_IFACE0 && L.code[n] != CODE_DEAD; };
-    };
-    for (const long long n : scanNodes(F, isCoupling(F))) {
+    for (const long long n : F.coupling) {
                 const int c[3] = {(int)(n % F.nx), (int)((n / F.nx) % F.ny), (int)(n / ((long long)F.nx * F.ny))};
                 int g[3], f[3], odd[3], nodd = 0;
                 gf.normal(c, f);
@@ -558,7 +617,7 @@ int buildTwoLevel(acp_handle* h) {
             h->dcHost.push_back(dn);
         }
     }
-    for (const long long n : direct ? std::vector<long long>() : scanNodes(C, isCoupling(C))) {
+    for (const long long n : direct ? std::vector<long long>() : C.coupling) {
                 const int c[3] = {(int)(n % C.nx), (int)((n / C.nx) % C.ny), (int)(n / ((long long)C.nx * C.ny))};
                 int g[3], f[3];
                 gc.normal(c, f);

@@ -25,6 +25,8 @@ struct LevelHost {
     int off[3] = {0, 0, 0};  // box origin in this level's global node index
     int per[3] = {0, 0, 0};  // periodic axes of this level
     std::vector<uint8_t> code;
+    std::vector<long long> coupling;  // coupling nodes in node order (two levels)
+    long long dead = 0;               // nodes covered by the other level
     std::vector<BNodeDev> lodiX, lodiZY;
     int nSlots = 0;  // partner-strain records kept (the device map LevelDev::slot; 0: none)
     long long active = 0;
@@ -126,6 +128,10 @@ LevelArgs<S> levelArgs(const acp_handle* h, int l, int src) {
     for (int ax = 0; ax < 3; ++ax) a.per[ax] = L.per[ax];
     a.A = (const S*)D.f[src];
     a.B = (S*)D.f[1 - src];
+    for (int q = 0; q < Q; ++q) {
+        a.Aq[q] = a.A + (size_t)q * (size_t)L.N;
+        a.Bq[q] = a.B + (size_t)q * (size_t)L.N;
+    }
     a.code = D.code;
     a.shift = h->shift;
     a.omega = L.omega;

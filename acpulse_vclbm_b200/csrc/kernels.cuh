@@ -60,6 +60,8 @@ struct LevelArgs {
     int per[3];  // periodic axes
     const S* A;  // array read this step
     S* B;        // array written this step
+    const S* Aq[Q];  // population q's part of A (A + q N): one address operand per load
+    S* Bq[Q];        // population q's part of B
     const uint8_t* code;
     double shift;   // w_q * shift is subtracted in storage (0 for the FP64 form)
     double omega;   // collision frequency of the level
@@ -226,7 +228,7 @@ __device__ __forceinline__ void regularisedEmit(R drho, const R* u, const R* s2,
 #pragma unroll
         for (int c = 0; c < 3; ++c) mc.a4[c] = rho * ec.a4[c] + om1 * nc.a4[c];
     }
-    forEachDirection<R, ORDER>(mc, kappa, [&](int q, R poly) { emit(q, R(wq(q)) * (drho + poly)); });
+    forEachWeighted<R, ORDER>(mc, drho, kappa, [&](int q, R v) { emit(q, v); });
 }
 
 // acc + Minv_RM[q][m] * d[m - 5], the term left out when the coefficient is zero
@@ -401,10 +403,10 @@ struct Pusher {
     template <typename V>
     __device__ __forceinline__ void operator()(int q, V v) const {
         if (q == 18) {
-            Store<S>::store(a.B + (18 * a.Ni + n), v, scaleOf(a, 18));
+            Store<S>::store(a.Bq[18] + n, v, scaleOf(a, 18));
         } else if (mask >> q & 1u) {
             const int t = n + o.dx[ex(q) + 1] + o.dy[ey(q) + 1] + o.dz[ez(q) + 1];
-            Store<S>::store(a.B + (q * a.Ni + t), v, scaleOf(a, q));
+            Store<S>::store(a.Bq[q] + t, v, scaleOf(a, q));
         }
     }
 };
@@ -421,7 +423,7 @@ __device__ __forceinline__ void collidePushBody(const LevelArgs<S>& a, int bx, i
     if (code == CODE_DEAD) return;
     R g[Q];
 #pragma unroll
-    for (int q = 0; q < Q; ++q) g[q] = R(Store<S>::load(a.A + (q * a.Ni + n), scaleOf(a, q)));
+    for (int q = 0; q < Q; ++q) g[q] = R(Store<S>::load(a.Aq[q] + n, scaleOf(a, q)));
     if (collides(code)) {
         Pusher<S> emit{a, n, c_pushMask[code], nbOffsets(a, i, j, k)};
         Collider<R, OP, ORDER, CUBIC, MRTWB>::run(g, a, (const R*)nullptr, emit);
@@ -459,7 +461,7 @@ template <typename S, typename R>
 __device__ __forceinline__ MomR<R> nodeMoments(const LevelArgs<S>& a, int n) {
     R g[Q];
 #pragma unroll
-    for (int q = 0; q < Q; ++q) g[q] = R(Store<S>::load(a.A + (q * a.Ni + n), scaleOf(a, q)));
+    for (int q = 0; q < Q; ++q) g[q] = R(Store<S>::load(a.Aq[q] + n, scaleOf(a, q)));
     R d, jj[3];
     pairMoments<R>(g, d, jj, (R*)nullptr);
     MomR<R> m;
@@ -485,7 +487,7 @@ __device__ __forceinline__ void planePass(const LevelArgs<S>& a, MomR<R> (*slot)
             if (a.code[n] != CODE_DEAD) {
                 R g[Q];
 #pragma unroll
-                for (int q = 0; q < Q; ++q) g[q] = R(Store<S>::load(a.A + (q * a.Ni + n), scaleOf(a, q)));
+                for (int q = 0; q < Q; ++q) g[q] = R(Store<S>::load(a.Aq[q] + n, scaleOf(a, q)));
                 R d, jj[3];
                 pairMoments<R>(g, d, jj, s2);
                 MomR<R> m;
@@ -610,7 +612,7 @@ __device__ __forceinline__ void tiledCollide(const LevelArgs<S>& a, int n, int i
         // LODI boundary node: pushes its uncollided populations inward
         Pusher<S> emit{a, n, c_pushMask[code], nbOffsets(a, i, j, z)};
 #pragma unroll
-        for (int q = 0; q < Q; ++q) emit(q, R(Store<S>::load(a.A + (q * a.Ni + n), scaleOf(a, q))));
+        for (int q = 0; q < Q; ++q) emit(q, R(Store<S>::load(a.Aq[q] + n, scaleOf(a, q))));
     }
 }
 
@@ -629,7 +631,7 @@ __device__ __forceinline__ void tiledNode(const LevelArgs<S>& a, MomR<R> (*sm)[T
     if (!s2 && collides(code)) {
         R g[Q];
 #pragma unroll
-        for (int q = 0; q < Q; ++q) g[q] = R(Store<S>::load(a.A + (q * a.Ni + n), scaleOf(a, q)));
+        for (int q = 0; q < Q; ++q) g[q] = R(Store<S>::load(a.Aq[q] + n, scaleOf(a, q)));
         secondSums<R>(g, s2buf);
         s2 = s2buf;
     }
@@ -708,12 +710,13 @@ __device__ __forceinline__ void tiledBody(const LevelArgs<S>& a, int zChunk, int
     auto key = [&](int u) { return (u - zBeg + 1) & 3; };
     {
         const int zm = wrapc(zBeg - 1, a.nz, a.per[2]);
-        if (zm >= 0) planePass<S, R>(a, sm[key(zBeg - 1)], x0, y0, zm, nxt);  // ring and moments only
+        if (zm >= 0) planePass<S, R>(a, sm[key(zBeg - 1)], x0, y0, zm, (R*)nullptr);  // ring and moments only
         planePass<S, R>(a, sm[key(zBeg)], x0, y0, zBeg, cur);
     }
     for (int z = zBeg; z < zEnd; ++z) {
         const int zp = wrapc(z + 1, a.nz, a.per[2]);
-        if (zp >= 0) planePass<S, R>(a, sm[key(z + 1)], x0, y0, zp, nxt);
+        // the plane past the chunk's end gives moments only
+        if (zp >= 0) planePass<S, R>(a, sm[key(z + 1)], x0, y0, zp, z + 1 < zEnd ? nxt : (R*)nullptr);
         __syncthreads();
         if (mine) tiledNode<S, R, OP, ORDER, CUBIC>(a, sm, i, j, z, key(z), key(z + 1), key(z - 1), cur);
 #pragma unroll
@@ -771,7 +774,7 @@ __device__ __forceinline__ void marchBody(const LevelArgs<S>& a, int yChunk, int
         if (a.code[n] == CODE_DEAD) return;
         R g[Q];
 #pragma unroll
-        for (int q = 0; q < Q; ++q) g[q] = R(Store<S>::load(a.A + (q * a.Ni + n), scaleOf(a, q)));
+        for (int q = 0; q < Q; ++q) g[q] = R(Store<S>::load(a.Aq[q] + n, scaleOf(a, q)));
         R d, jj[3];
         pairMoments<R>(g, d, jj, s2);
         MomR<R> m;
@@ -794,13 +797,14 @@ __device__ __forceinline__ void marchBody(const LevelArgs<S>& a, int yChunk, int
     R cur[6], nxt[6];
     {
         const int ym = wrapc(rowAt(-1), a.ny, a.per[1]);
-        if (ym >= 0) rowPass(key(-1), ym, nxt);  // moments only
+        if (ym >= 0) rowPass(key(-1), ym, (R*)nullptr);  // moments only
         rowPass(key(0), rowAt(0), cur);
     }
     for (int st = 0; st < len; ++st) {
         const int y = rowAt(st);
         const int yn = wrapc(rowAt(st + 1), a.ny, a.per[1]);
-        if (yn >= 0) rowPass(key(st + 1), yn, nxt);
+        // the row past the chunk's end gives moments only
+        if (yn >= 0) rowPass(key(st + 1), yn, st + 1 < len ? nxt : (R*)nullptr);
         __syncthreads();
         if (collider) {
             const int n = (tz * a.ny + y) * a.nx + xu;
@@ -848,7 +852,7 @@ __device__ __forceinline__ void marchBodyPrefetch(const LevelArgs<S>& a, int yCh
     auto loadRow = [&](int n, uint8_t c, R* g) {
         if (c == CODE_DEAD) return;
 #pragma unroll
-        for (int q = 0; q < Q; ++q) g[q] = R(Store<S>::load(a.A + (q * a.Ni + n), scaleOf(a, q)));
+        for (int q = 0; q < Q; ++q) g[q] = R(Store<S>::load(a.Aq[q] + n, scaleOf(a, q)));
     };
     auto reduceRow = [&](int s, uint8_t c, const R* g, R* s2) {
         if (c == CODE_DEAD) return;

@@ -187,3 +187,35 @@ def test_tiled_neighbour_kernels_match_oracle(name, dims, per, op, cubic):
     fo = run_oracle(d, 40)
     err = np.abs(f - fo).max() / d.ic_eps
     assert err < 1e-9, err
+
+
+# FP32 storage on the y-marching blocks (FP32 compute at its own register
+# cap): y chunks of one row, three rows (partial last chunk, odd chunks
+# marching downwards) and longer than the lattice; LODI and periodic y ends,
+# periodic x.
+MARCH_F32_CASES = [
+    ("six-planes-periodic-y", (70, 21, 6), (False, True, True), 0),
+    ("three-planes-lodi-y", (65, 19, 3), (False, False, True), 0),
+    ("periodic-x", (61, 17, 4), (True, True, True), 0),
+    ("lodi-y-chunk-1", (65, 19, 3), (False, False, True), 1),
+    ("periodic-y-chunk-3", (70, 22, 6), (False, True, True), 3),
+    ("lodi-y-chunk-past-end", (40, 13, 2), (False, False, True), 64),
+]
+
+
+@pytest.mark.parametrize("name,dims,per,chunk", MARCH_F32_CASES, ids=[c[0] for c in MARCH_F32_CASES])
+@pytest.mark.parametrize("op,cubic", [("HRR", 0), ("HRR", 1), ("RR", 1)])
+def test_fp32_march_matches_oracle(name, dims, per, chunk, op, cubic, monkeypatch):
+    if chunk:
+        monkeypatch.setenv("ACP_MARCH_YCHUNK", str(chunk))
+    nx, ny, nz = dims
+    kw = dict(op=op, nu_lu=1e-3, order=3, periodic=per, eps=2e-2, b=3.0,
+              center=(nx / 2.0 - 0.3, ny / 2.0 + 0.2, nz / 2.0 - 0.1), ic_dims=3)
+    d64 = lattice_units_case(nx, ny, nz, **kw)
+    d32 = lattice_units_case(nx, ny, nz, storage="FP32-DEV", **kw)
+    d64.cubic_mach = d32.cubic_mach = cubic
+    cs2 = d64.speed_of_sound ** 2
+    p32 = run_gpu(d32, 40).sum(axis=0) * cs2
+    p64 = run_oracle(d64, 40).sum(axis=0) * cs2
+    err = np.abs(p32 - p64).max() / (d64.ic_eps * d64.density * cs2)
+    assert err < 1e-5, err
