@@ -140,7 +140,7 @@ __global__ void __maxnreg__(ACP_MARCH_REGS_F32)
 template <typename S, int ORDER>
 __global__ void __launch_bounds__(128) kb_lodi(const BatchCase<S>* __restrict__ cases,
                                                const WorkItem* __restrict__ items, int n, int level, int fineSrc,
-                                               int flip, int zy) {
+                                               int flip, int zy, int tpn) {
     __shared__ LevelArgs<S> sa;
     __shared__ LodiArgs sp;
     for (int w = blockIdx.x; w < n; w += gridDim.x) {
@@ -150,7 +150,7 @@ __global__ void __launch_bounds__(128) kb_lodi(const BatchCase<S>* __restrict__ 
         stage(&sa, &L.a[srcOf(bc, level, fineSrc, flip)]);
         stage(&sp, &L.lodi);
         __syncthreads();
-        lodiBody<S, ORDER>(sa.A, sa.B, zy ? L.lodiZY : L.lodiX, zy ? L.nLodiZY : L.nLodiX, sp, sa, it.bx);
+        lodiBody<S, ORDER>(sa.A, sa.B, zy ? L.lodiZY : L.lodiX, zy ? L.nLodiZY : L.nLodiX, sp, sa, it.bx, tpn);
         __syncthreads();
     }
 }
@@ -232,7 +232,7 @@ __global__ void __launch_bounds__(128) kb_f2c(const BatchCase<S>* __restrict__ c
 template <typename S>
 using KbCollide = void (*)(const BatchCase<S>*, const WorkItem*, int, int, int, int);
 template <typename S>
-using KbLodi = void (*)(const BatchCase<S>*, const WorkItem*, int, int, int, int, int);
+using KbLodi = void (*)(const BatchCase<S>*, const WorkItem*, int, int, int, int, int, int);
 template <typename S>
 using KbSave = void (*)(const BatchCase<S>*, const WorkItem*, int, int);
 template <typename S, typename R>
@@ -347,6 +347,7 @@ struct Group {
     bool direct = false;
     bool tiled = false;
     int marchNz[2] = {0, 0};  // per level: z planes of the y-marching collide (0: not marching)
+    int lodiTpn = LODI_TPN_CLASSICAL;  // lanes per LODI node: lodiLanes of the members (any with transverse terms: 8)
     void* dCases = nullptr;
     WorkItem* dItems = nullptr;
     // item ranges per phase
@@ -375,6 +376,7 @@ struct acp_batch {
     TuneConfig cfg;
     std::string err;
     std::string report;
+    std::vector<const void*> bulk;  // collide kernels of the captured step (instantiateWithPriorities)
 };
 
 namespace acp {
@@ -517,8 +519,8 @@ int buildGroup(acp_batch* b, Group& g) {
         phase(g.collide[l], [&](int c, const acp_handle* h) {
             collideItems(h->host[l], c, g.tiled, g.marchNz[l] > 0, recs[c].lv[l].zChunk, items);
         });
-        phase(g.lodiX[l], [&](int c, const acp_handle* h) { blockItems(c, h->dev[l].nLodiX * LODI_TPN, 128, items); });
-        phase(g.lodiZY[l], [&](int c, const acp_handle* h) { blockItems(c, h->dev[l].nLodiZY * LODI_TPN, 128, items); });
+        phase(g.lodiX[l], [&](int c, const acp_handle* h) { blockItems(c, h->dev[l].nLodiX * g.lodiTpn, 128, items); });
+        phase(g.lodiZY[l], [&](int c, const acp_handle* h) { blockItems(c, h->dev[l].nLodiZY * g.lodiTpn, 128, items); });
     }
     if (g.levels == 2) {
         phase(g.save, [&](int c, const acp_handle* h) {
@@ -588,6 +590,9 @@ void enqueueGroup(acp_batch* b, Group& g, int flip) {
     cudaStream_t st = g.stream;
     const int o = d.eq_order;
     KbCollide<S> collide = pickBatchCollide<S, R>(d);
+    noteBulk(b->bulk, (const void*)collide);
+    for (int l = 0; l < g.levels; ++l)
+        if (g.marchNz[l]) noteBulk(b->bulk, (const void*)pickBatchMarch<S, R>(d));
     KbLodi<S> lodi = pickBatchLodi<S>(o);
     const dim3 cblock = g.tiled ? dim3(TX, TY) : dim3(128);
     auto levelStep = [&](int l, int fineSrc, cudaStream_t ls) {
@@ -601,10 +606,12 @@ void enqueueGroup(acp_batch* b, Group& g, int flip) {
                                                                                      flip);
         if (g.lodiX[l].count)
             lodi<<<gridFor(b, g.lodiX[l].count, g.resident[1]), 128, 0, ls>>>(cs, it + g.lodiX[l].off,
-                                                                             g.lodiX[l].count, l, fineSrc, flip, 0);
+                                                                             g.lodiX[l].count, l, fineSrc, flip, 0,
+                                                                             g.lodiTpn);
         if (g.lodiZY[l].count)
             lodi<<<gridFor(b, g.lodiZY[l].count, g.resident[1]), 128, 0, ls>>>(cs, it + g.lodiZY[l].off,
-                                                                              g.lodiZY[l].count, l, fineSrc, flip, 1);
+                                                                              g.lodiZY[l].count, l, fineSrc, flip, 1,
+                                                                              g.lodiTpn);
     };
     if (g.levels == 1) {
         levelStep(0, 0, st);
@@ -690,12 +697,13 @@ int buildAll(acp_batch* b) {
     // one graph per parity of the batch's step counter
     for (int p = 0; p < 2; ++p) {
         cudaGraph_t graph;
+        b->bulk.clear();
         BCU(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
         int s = enqueueBatchStep(b, p);
         cudaError_t e = cudaStreamEndCapture(b->stream, &graph);
         if (s) return s;
         if (e != cudaSuccess) return bfail(b, ACP_ERR_CUDA, "batch graph capture: %s", cudaGetErrorString(e));
-        e = cudaGraphInstantiate(&b->graph[p], graph, 0);
+        e = instantiateWithPriorities(&b->graph[p], graph, b->bulk);
         cudaGraphDestroy(graph);
         if (e != cudaSuccess) return bfail(b, ACP_ERR_CUDA, "batch graph instantiate: %s", cudaGetErrorString(e));
     }
@@ -780,6 +788,7 @@ int acp_batch_create(acp_handle* const* cases, int n, acp_batch** out) {
             f = index.find(key);
         }
         b->groups[f->second].members.push_back(i);
+        b->groups[f->second].lodiTpn = std::max(b->groups[f->second].lodiTpn, lodiLanes(h->d.transverse));
     }
     for (Group& g : b->groups) {
         BCU(b, cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));

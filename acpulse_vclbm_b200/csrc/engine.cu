@@ -361,7 +361,7 @@ struct CouplingGeom {
 // is coupling over the whole x extent of the box; classes are then set per
 // segment instead of testing every node.
 void markLevel(LevelHost& L, const CouplingGeom& g) {
-    L.code.assign(L.N, CODE_FLUID);
+    L.code.resize(L.N);  // every row is filled with CODE_FLUID below before it is marked
     // coupling nodes and dead-node counts per pool thread, in node order
     std::vector<std::vector<long long>> part(ScanPool::kMax);
     std::vector<long long> dead(ScanPool::kMax, 0);
@@ -378,6 +378,7 @@ void markLevel(LevelHost& L, const CouplingGeom& g) {
         dhi[a] = g.hiIf[a] ? g.ch[a] - 1 : g.ch[a];
     }
     forRows((long long)L.ny * L.nz, [&](long long r0, long long r1, int t) {
+        std::fill(L.code.begin() + r0 * L.nx, L.code.begin() + r1 * L.nx, CODE_FLUID);
         for (long long r = r0; r < r1; ++r) {
             const int j = (int)(r % L.ny), k = (int)(r / L.ny);
             if (j < g.cl[1] || j > g.ch[1] || k < g.cl[2] || k > g.ch[2]) continue;  // row misses the box
@@ -485,8 +486,10 @@ int buildTwoLevel(acp_handle* h) {
         const int dd[3] = {L.nx, L.ny, L.nz};
         for (int a = 0; a < 3; ++a) {
             c[a] = g[a] - L.off[a];
-            if (L.per[a]) c[a] = (c[a] % dd[a] + dd[a]) % dd[a];
-            if (c[a] < 0 || c[a] >= dd[a]) return false;
+            if (c[a] < 0 || c[a] >= dd[a]) {
+                if (!L.per[a]) return false;
+                c[a] = (c[a] % dd[a] + dd[a]) % dd[a];
+            }
         }
         out = ((long long)c[2] * L.ny + c[1]) * L.nx + c[0];
         return true;
@@ -497,8 +500,15 @@ int buildTwoLevel(acp_handle* h) {
         out = (int)n;
         return true;
     };
-    std::vector<C2FDev> coinc, mid, cen;
-    for (const long long n : F.coupling) {
+    // C2F records of the fine coupling nodes on the pool threads (contiguous
+    // ranges of the node list; per-thread lists joined in thread order keep the
+    // node order, and the first failing node's message is the one reported)
+    const int T = ScanPool::kMax;
+    std::vector<std::vector<C2FDev>> coincT(T), midT(T), cenT(T);
+    std::vector<const char*> errT(T, nullptr);
+    forRows((long long)F.coupling.size(), [&](long long i0, long long i1, int t) {
+        for (long long i = i0; i < i1 && !errT[t]; ++i) {
+                const long long n = F.coupling[i];
                 const int c[3] = {(int)(n % F.nx), (int)((n / F.nx) % F.ny), (int)(n / ((long long)F.nx * F.ny))};
                 int g[3], f[3], odd[3], nodd = 0;
                 gf.normal(c, f);
@@ -517,10 +527,12 @@ int buildTwoLevel(acp_handle* h) {
                     int gc2[3];
                     for (int a = 0; a < 3; ++a) gc2[a] = g[a] / 2;
                     long long src;
-                    if (!local(C, gc2, src) || C.code[src] == CODE_DEAD)
-                        return fail(h, ACP_ERR_INVALID, "coarse source of a fine coupling node missing");
+                    if (!local(C, gc2, src) || C.code[src] == CODE_DEAD) {
+                        errT[t] = "coarse source of a fine coupling node missing";
+                        break;
+                    }
                     cn.src = (int)src;
-                    coinc.push_back(cn);
+                    coincT[t].push_back(cn);
                     continue;
                 }
                 int ax = 0;
@@ -534,7 +546,10 @@ int buildTwoLevel(acp_handle* h) {
                     gg[ax] += off[m];
                     ok[m] = fineLocal(gg, pts[m]) && F.code[pts[m]] >= CODE_IFACE0 && F.code[pts[m]] != CODE_DEAD;
                 }
-                if (!ok[1] || !ok[2]) return fail(h, ACP_ERR_INVALID, "interpolation stencil missing on the interface");
+                if (!ok[1] || !ok[2]) {
+                    errT[t] = "interpolation stencil missing on the interface";
+                    break;
+                }
                 if (ok[0] && ok[3]) {
                     const float w[4] = {-1.f / 16.f, 9.f / 16.f, 9.f / 16.f, -1.f / 16.f};
                     for (int m = 0; m < 4; ++m) { cn.st[m] = pts[m]; cn.w[m] = w[m]; }
@@ -542,8 +557,17 @@ int buildTwoLevel(acp_handle* h) {
                     cn.st[0] = pts[1]; cn.w[0] = 0.5f;
                     cn.st[1] = pts[2]; cn.w[1] = 0.5f;
                 }
-                (nodd == 1 ? mid : cen).push_back(cn);
-            }
+                (nodd == 1 ? midT : cenT)[t].push_back(cn);
+        }
+    });
+    for (int t = 0; t < T; ++t)
+        if (errT[t]) return fail(h, ACP_ERR_INVALID, "%s", errT[t]);
+    std::vector<C2FDev> coinc, mid, cen;
+    for (int t = 0; t < T; ++t) {
+        coinc.insert(coinc.end(), coincT[t].begin(), coincT[t].end());
+        mid.insert(mid.end(), midT[t].begin(), midT[t].end());
+        cen.insert(cen.end(), cenT[t].begin(), cenT[t].end());
+    }
     h->nCoinc = (int)coinc.size();
     h->nMid = (int)mid.size();
     h->nCen = (int)cen.size();
@@ -617,7 +641,12 @@ int buildTwoLevel(acp_handle* h) {
             h->dcHost.push_back(dn);
         }
     }
-    for (const long long n : direct ? std::vector<long long>() : C.coupling) {
+    // F2C records of the coarse coupling nodes (STD), on the pool threads as above
+    std::vector<std::vector<F2CDev>> f2cT(T);
+    std::fill(errT.begin(), errT.end(), nullptr);
+    forRows(direct ? 0LL : (long long)C.coupling.size(), [&](long long i0, long long i1, int t) {
+        for (long long i = i0; i < i1 && !errT[t]; ++i) {
+                const long long n = C.coupling[i];
                 const int c[3] = {(int)(n % C.nx), (int)((n / C.nx) % C.ny), (int)(n / ((long long)C.nx * C.ny))};
                 int g[3], f[3];
                 gc.normal(c, f);
@@ -625,16 +654,28 @@ int buildTwoLevel(acp_handle* h) {
                 F2CDev fn;
                 fn.n = (int)n;
                 fn.mask = replaceMask(d.f2c_replace, f);
-                if (!fineLocal(g, fn.partner)) return fail(h, ACP_ERR_INVALID, "fine partner outside the box");
+                if (!fineLocal(g, fn.partner)) {
+                    errT[t] = "fine partner outside the box";
+                    break;
+                }
                 int m = 0;
-                for (int dz = -1; dz <= 1; ++dz)
-                    for (int dy = -1; dy <= 1; ++dy)
-                        for (int dx = -1; dx <= 1; ++dx) {
+                bool inside = true;
+                for (int dz = -1; dz <= 1 && inside; ++dz)
+                    for (int dy = -1; dy <= 1 && inside; ++dy)
+                        for (int dx = -1; dx <= 1 && inside; ++dx) {
                             int gg[3] = {g[0] + dx, g[1] + dy, g[2] + dz};
-                            if (!fineLocal(gg, fn.cube[m++])) return fail(h, ACP_ERR_INVALID, "F2C neighbourhood outside the box");
+                            inside = fineLocal(gg, fn.cube[m++]);
                         }
-                h->f2cHost.push_back(fn);
-            }
+                if (!inside) {
+                    errT[t] = "F2C neighbourhood outside the box";
+                    break;
+                }
+                f2cT[t].push_back(fn);
+        }
+    });
+    for (int t = 0; t < T; ++t)
+        if (errT[t]) return fail(h, ACP_ERR_INVALID, "%s", errT[t]);
+    for (int t = 0; t < T; ++t) h->f2cHost.insert(h->f2cHost.end(), f2cT[t].begin(), f2cT[t].end());
     // partner strain of the coupling nodes (STD scheme, HRR or RR with cubic-Mach)
     h->partner = !direct && (d.op == OP_HRR || (d.op == OP_RR && d.cubic_mach));
     h->nbHost.clear();
@@ -780,15 +821,18 @@ TiledFn<S> pickTiled(const acp_case_desc& d) {
     }
 }
 
+template <typename S>
+using MarchFn = void (*)(LevelArgs<S>, int, const int*);
+
 // the march kernel of a case: FP64 compute with its launch bound, FP32
 // compute (FP32 and FP16 storage) with its direct register cap
 template <typename S, typename R, int OP, int ORDER, bool CUBIC>
-TiledFn<S> marchKernel() {
+MarchFn<S> marchKernel() {
     if constexpr (sizeof(R) == 8) return k_collide_push_march<S, R, OP, ORDER, CUBIC>;
     else return k_collide_push_march_f32<S, R, OP, ORDER, CUBIC>;
 }
 template <typename S, typename R>
-TiledFn<S> pickMarch(const acp_case_desc& d) {
+MarchFn<S> pickMarch(const acp_case_desc& d) {
     const bool cubic = d.cubic_mach != 0;
     if (d.op == OP_RR) {
         switch (d.eq_order) {
@@ -805,7 +849,7 @@ TiledFn<S> pickMarch(const acp_case_desc& d) {
 }
 
 template <typename S>
-using LodiFn = void (*)(const S*, S*, const BNodeDev*, int, LodiArgs, LevelArgs<S>);
+using LodiFn = void (*)(const S*, S*, const BNodeDev*, int, LodiArgs, LevelArgs<S>, int);
 
 template <typename S>
 LodiFn<S> pickLodi(int order) {
@@ -834,24 +878,41 @@ dim3 gridOf(const LevelHost& L, int bx) { return dim3((L.nx + bx - 1) / bx, L.ny
 template <typename S, typename R>
 int enqueueLevelLodi(acp_handle* h, int l, int src, PhaseTimer* tm, cudaStream_t st);
 
+// part of a level's collide: every x tile, or (y-marching levels with an
+// interior / boundary split of their tiles, LevelDev::cols) the tiles that
+// touch no coupling or LODI node, or the others
+enum { PART_ALL = 0, PART_INTERIOR = 1, PART_BOUNDARY = 2 };
+
 template <typename S, typename R>
 int enqueueLevelStep(acp_handle* h, int l, int src, PhaseTimer* tm = nullptr, cudaStream_t st = nullptr,
-                     bool lodi = true) {
+                     bool lodi = true, int part = PART_ALL) {
     if (!st) st = h->stream;
     const LevelHost& L = h->host[l];
+    const LevelDev& D = h->dev[l];
     LevelArgs<S> a = levelArgs<S>(h, l, src);
     const int bx = 128;
     if (tm) tm->mark(-1);
     if (needsMoments(h->d) && marchesY(L)) {
         const int chunk = marchChunkFor(L, sizeof(R));
         dim3 grid((L.nx + MARCH_STEP - 1) / MARCH_STEP, (L.ny + chunk - 1) / chunk);
-        pickMarch<S, R>(h->d)<<<grid, dim3(MARCH_TX, L.nz), marchSmemBytes<R>(L.nz), st>>>(a, chunk);
+        const int* cols = nullptr;
+        if (part != PART_ALL && D.nInner) {
+            grid.x = part == PART_INTERIOR ? D.nInner : D.nOuter;
+            cols = part == PART_INTERIOR ? D.cols : D.cols + D.nInner;
+        }
+        const MarchFn<S> k = pickMarch<S, R>(h->d);
+        if (grid.x) k<<<grid, dim3(MARCH_TX, L.nz), marchSmemBytes<R>(L.nz), st>>>(a, chunk, cols);
+        noteBulk(h->bulk, (const void*)k);
     } else if (needsMoments(h->d)) {
         const int chunk = tiledChunkFor(L, TiledMinBlocks<R>::value);
         dim3 grid((L.nx + TX - 1) / TX, (L.ny + TY - 1) / TY, (L.nz + chunk - 1) / chunk);
-        pickTiled<S, R>(h->d)<<<grid, dim3(TX, TY), 0, st>>>(a, chunk);
+        const TiledFn<S> k = pickTiled<S, R>(h->d);
+        k<<<grid, dim3(TX, TY), 0, st>>>(a, chunk);
+        noteBulk(h->bulk, (const void*)k);
     } else {
-        pickCollide<S, R>(h->d)<<<gridOf(L, bx), bx, 0, st>>>(a);
+        const auto k = pickCollide<S, R>(h->d);
+        k<<<gridOf(L, bx), bx, 0, st>>>(a);
+        noteBulk(h->bulk, (const void*)k);
     }
     if (tm) tm->mark(ACP_K_COLLIDE);
     return lodi ? enqueueLevelLodi<S, R>(h, l, src, tm, st) : ACP_OK;
@@ -867,8 +928,9 @@ int enqueueLevelLodi(acp_handle* h, int l, int src, PhaseTimer* tm, cudaStream_t
     LodiFn<S> lf = pickLodi<S>(h->d.eq_order);
     // eight lanes per boundary node (one per stencil member) and small blocks
     // spread the few thousand nodes of a face over every SM
-    if (D.nLodiX) lf<<<(D.nLodiX * LODI_TPN + 63) / 64, 64, 0, st>>>(a.A, a.B, D.lodiX, D.nLodiX, p, a);
-    if (D.nLodiZY) lf<<<(D.nLodiZY * LODI_TPN + 63) / 64, 64, 0, st>>>(a.A, a.B, D.lodiZY, D.nLodiZY, p, a);
+    const int tpn = lodiLanes(h->d.transverse);
+    if (D.nLodiX) lf<<<(D.nLodiX * tpn + 63) / 64, 64, 0, st>>>(a.A, a.B, D.lodiX, D.nLodiX, p, a, tpn);
+    if (D.nLodiZY) lf<<<(D.nLodiZY * tpn + 63) / 64, 64, 0, st>>>(a.A, a.B, D.lodiZY, D.nLodiZY, p, a, tpn);
     if (tm && (D.nLodiX || D.nLodiZY)) tm->mark(ACP_K_LODI);
     return ACP_OK;
 }
@@ -946,6 +1008,12 @@ int enqueueStepT(acp_handle* h, int src, PhaseTimer* tm) {
         if (tm) tm->mark(ACP_K_COUPLING);
         enqueueLevelStep<S, R>(h, 0, src, tm, cs);  // coarse t -> t+1
         enqueueLevelStep<S, R>(h, 1, 0, tm, h->stream, false);  // fine t -> t+1/2
+        // the interior tiles of the next fine sub-step need only this one
+        const bool split = fork && h->dev[1].nInner > 0;
+        if (split) {
+            branch(h->side3, h->splitEv[0]);
+            enqueueLevelStep<S, R>(h, 1, 1, tm, h->side3, false, PART_INTERIOR);  // fine t+1/2 -> t+1, inside
+        }
         if (fork) branch(ls, h->branchEv[0]);
         enqueueLevelLodi<S, R>(h, 1, 0, tm, ls);
         if (fork) join(h->side, h->joinEv);
@@ -953,7 +1021,12 @@ int enqueueStepT(acp_handle* h, int src, PhaseTimer* tm) {
         enqueueC2F<S, R>(h, 1 - src, 1, R(0.5));  // C2F at t+1/2
         if (tm) tm->mark(ACP_K_COUPLING);
         if (fork) join(ls, h->branchEv[1]);
-        enqueueLevelStep<S, R>(h, 1, 1, tm, h->stream, false);  // fine t+1/2 -> t+1
+        if (split) {
+            enqueueLevelStep<S, R>(h, 1, 1, tm, h->stream, false, PART_BOUNDARY);  // the tiles at the faces
+            join(h->side3, h->splitEv[1]);
+        } else {
+            enqueueLevelStep<S, R>(h, 1, 1, tm, h->stream, false);  // fine t+1/2 -> t+1
+        }
         if (fork) branch(ls, h->branchEv[2]);
         enqueueLevelLodi<S, R>(h, 1, 1, tm, ls);
         if (tm) tm->mark(-1);
@@ -1000,6 +1073,7 @@ int launchesPerStep(const acp_handle* h) {
     if (h->host.size() == 2) {
         const int c2f = (h->nCoinc ? 1 : 0) + (h->nMid ? 1 : 0) + (h->nCen ? 1 : 0);
         n += (h->nCoinc ? 1 : 0) + 2 * c2f + (h->f2cHost.empty() ? 0 : 1);
+        if (h->dev[1].nInner) ++n;  // the second fine collide as interior and boundary tiles
     }
     if (h->nProbes) ++n;
     return n;
@@ -1017,11 +1091,12 @@ int captureGraphs(acp_handle* h) {
     destroyGraphs(h);
     for (int p = 0; p < 2; ++p) {
         cudaGraph_t g;
+        h->bulk.clear();
         CU(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
         enqueueStep(h, p);
         cudaError_t e = cudaStreamEndCapture(h->stream, &g);
         if (e != cudaSuccess) return fail(h, ACP_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
-        e = cudaGraphInstantiate(&h->graph[p], g, 0);
+        e = instantiateWithPriorities(&h->graph[p], g, h->bulk);
         cudaGraphDestroy(g);
         if (e != cudaSuccess) return fail(h, ACP_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
     }
@@ -1170,6 +1245,42 @@ int acp_estimate_bytes(const acp_case_desc* d, size_t* bytes) {
     return ACP_OK;
 }
 
+// The x tiles of the fine level's y-marching collide (STD coupling, x not
+// periodic) split into those that touch no coupling or LODI node and the
+// others (LevelDev::cols).  A tile reads and pushes within x0 - 1 .. x0 + 30;
+// one more node each side is kept clear.  The second fine sub-step runs the
+// first kind beside the first C2F and the fine LODI passes: those write only
+// coupling and LODI nodes of the array the tiles read, and read only LODI
+// nodes of the array the tiles write.
+int splitFineTiles(acp_handle* h) {
+    const LevelHost& F = h->host[1];
+    if (!h->dcHost.empty() || !needsMoments(h->d) || !marchesY(F) || F.per[0]) return ACP_OK;
+    const int ntx = (F.nx + MARCH_STEP - 1) / MARCH_STEP;
+    std::vector<char> hit(ntx, 0);
+    auto mark = [&](long long n) {
+        const int x = (int)(n % F.nx);
+        for (int bx = std::max(0, (x - 31) / MARCH_STEP - 1); bx <= std::min(ntx - 1, (x + 2) / MARCH_STEP + 1); ++bx)
+            if (x >= bx * MARCH_STEP - 2 && x <= bx * MARCH_STEP + 31) hit[bx] = 1;
+    };
+    for (const long long n : F.coupling) mark(n);
+    for (const BNodeDev& b : F.lodiX) mark(b.n);
+    for (const BNodeDev& b : F.lodiZY) mark(b.n);
+    std::vector<int> cols;
+    for (int bx = 0; bx < ntx; ++bx)
+        if (!hit[bx]) cols.push_back(bx);
+    const int inner = (int)cols.size();
+    if (inner == 0 || inner == ntx) return ACP_OK;
+    for (int bx = 0; bx < ntx; ++bx)
+        if (hit[bx]) cols.push_back(bx);
+    LevelDev& D = h->dev[1];
+    int s = devAlloc(h, (void**)&D.cols, cols.size() * sizeof(int));
+    if (s) return s;
+    CU(h, cudaMemcpyAsync(D.cols, cols.data(), cols.size() * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    D.nInner = inner;
+    D.nOuter = ntx - inner;
+    return ACP_OK;
+}
+
 int acp_create(const acp_case_desc* d, int device, acp_handle** out) {
     if (!out) return ACP_ERR_INVALID;
     *out = nullptr;
@@ -1226,6 +1337,8 @@ int acp_create(const acp_case_desc* d, int device, acp_handle** out) {
     CU(h, cudaEventCreateWithFlags(&h->joinEv, cudaEventDisableTiming));
     CU(h, cudaStreamCreateWithFlags(&h->side2, cudaStreamNonBlocking));
     for (cudaEvent_t& e : h->branchEv) CU(h, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    CU(h, cudaStreamCreateWithFlags(&h->side3, cudaStreamNonBlocking));
+    for (cudaEvent_t& e : h->splitEv) CU(h, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     if ((s = devAlloc(h, (void**)&h->dErr, sizeof(int)))) return s;
     CU(h, cudaMemsetAsync(h->dErr, 0, sizeof(int), h->stream));
     h->dev.resize(h->host.size());
@@ -1290,6 +1403,7 @@ int acp_create(const acp_case_desc* d, int device, acp_handle** out) {
             if (nc) k_scatter_slots<F2CDev><<<(nc + 255) / 256, 256, 0, h->stream>>>(h->dev[0].slot, h->dF2C, nc);
             CU(h, cudaGetLastError());
         }
+        if ((s = splitFineTiles(h))) return s;
     }
     CU(h, cudaStreamSynchronize(h->stream));
     return ACP_OK;
@@ -1942,6 +2056,7 @@ int acp_destroy(acp_handle* h) {
         cudaFree(D.lodiZY);
         cudaFree(D.slot);
         cudaFree(D.sg);
+        cudaFree(D.cols);
     }
     cudaFree(h->dNb);
     cudaFree(h->dPreNb);
@@ -1960,6 +2075,9 @@ int acp_destroy(acp_handle* h) {
     if (h->joinEv) cudaEventDestroy(h->joinEv);
     if (h->side2) cudaStreamDestroy(h->side2);
     for (cudaEvent_t e : h->branchEv)
+        if (e) cudaEventDestroy(e);
+    if (h->side3) cudaStreamDestroy(h->side3);
+    for (cudaEvent_t e : h->splitEv)
         if (e) cudaEventDestroy(e);
     delete h;
     return ACP_OK;

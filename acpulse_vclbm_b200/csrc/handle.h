@@ -19,12 +19,32 @@ struct acp_batch;
 
 namespace acp {
 
+// allocator whose resize leaves new elements uninitialised: the node-class
+// arrays are written in full by the set-up scans, row ranges on several
+// threads, so a zero fill first would be a second serial pass over them
+template <typename T>
+struct NoInitAlloc : std::allocator<T> {
+    template <typename U>
+    struct rebind {
+        using other = NoInitAlloc<U>;
+    };
+    NoInitAlloc() = default;
+    template <typename U>
+    NoInitAlloc(const NoInitAlloc<U>&) noexcept {}
+    template <typename U>
+    void construct(U*) noexcept {}
+    template <typename U, typename... A>
+    void construct(U* p, A&&... a) {
+        ::new ((void*)p) U(std::forward<A>(a)...);
+    }
+};
+
 struct LevelHost {
     int nx = 0, ny = 0, nz = 0;
     long long N = 0;
     int off[3] = {0, 0, 0};  // box origin in this level's global node index
     int per[3] = {0, 0, 0};  // periodic axes of this level
-    std::vector<uint8_t> code;
+    std::vector<uint8_t, NoInitAlloc<uint8_t>> code;
     std::vector<long long> coupling;  // coupling nodes in node order (two levels)
     long long dead = 0;               // nodes covered by the other level
     std::vector<BNodeDev> lodiX, lodiZY;
@@ -39,6 +59,12 @@ struct LevelDev {
     BNodeDev* lodiX = nullptr;
     BNodeDev* lodiZY = nullptr;
     int nLodiX = 0, nLodiZY = 0;
+    // x tiles of the y-marching collide split for the second fine sub-step:
+    // cols[0, nInner) touch no coupling or LODI node (they may run while the
+    // coupling kernels do), cols[nInner, nInner + nOuter) the others; nInner
+    // = 0: no split
+    int* cols = nullptr;
+    int nInner = 0, nOuter = 0;
     int* slot = nullptr;    // see LevelHost::slot
     double* sg = nullptr;   // [12][nSlots] partner strain S and cubic-Mach gradient G
 };
@@ -65,6 +91,10 @@ struct acp_handle {
     // coupling kernels, F2C beside the last C2F (disjoint node sets)
     cudaStream_t side2 = nullptr;
     cudaEvent_t branchEv[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    // fourth branch: the interior tiles of the second fine sub-step beside the
+    // first C2F and the fine LODI passes (LevelDev::cols)
+    cudaStream_t side3 = nullptr;
+    cudaEvent_t splitEv[2] = {nullptr, nullptr};
     cudaGraphExec_t graph[2] = {nullptr, nullptr};  // one step starting from cur == 0 / cur == 1
     // two-level coupling (fine state always in array 0 between coarse steps)
     std::vector<acp::C2FDev> c2fHost;
@@ -94,6 +124,7 @@ struct acp_handle {
     float hscale[acp::Q];
     double m4[18] = {0};  // sum_q w_q H2_q (x) H4_q(kappa) (fourth-order equilibria)
     acp_batch* batch = nullptr;  // the batch this case belongs to (stepped only through it)
+    std::vector<const void*> bulk;  // collide kernels launched while capturing the step graphs
 };
 
 namespace acp {
@@ -108,6 +139,42 @@ inline int fail(acp_handle* h, int code, const char* fmt, ...) {
         h->err = buf;
     }
     return code;
+}
+
+// adds a collide kernel to the set kept for instantiateWithPriorities
+inline void noteBulk(std::vector<const void*>& bulk, const void* f) {
+    if (std::find(bulk.begin(), bulk.end(), f) == bulk.end()) bulk.push_back(f);
+}
+
+// Instantiates a captured step graph with every kernel but the collide
+// launches (`bulk`: the kernels that fill the SMs) at the device's greatest
+// stream priority.  The small latency-bound phases (LODI, coupling, probes)
+// of one branch then take the block slots that free up while another
+// branch's collide runs, instead of waiting behind its remaining waves.
+// Priorities change no dependency of the graph.
+inline cudaError_t instantiateWithPriorities(cudaGraphExec_t* exec, cudaGraph_t g, const std::vector<const void*>& bulk) {
+    int least = 0, greatest = 0;
+    if (cudaDeviceGetStreamPriorityRange(&least, &greatest) == cudaSuccess && greatest != least) {
+        size_t n = 0;
+        if (cudaGraphGetNodes(g, nullptr, &n) == cudaSuccess && n) {
+            std::vector<cudaGraphNode_t> nodes(n);
+            if (cudaGraphGetNodes(g, nodes.data(), &n) == cudaSuccess)
+                for (cudaGraphNode_t nd : nodes) {
+                    cudaGraphNodeType t;
+                    cudaKernelNodeParams kp;
+                    if (cudaGraphNodeGetType(nd, &t) != cudaSuccess || t != cudaGraphNodeTypeKernel ||
+                        cudaGraphKernelNodeGetParams(nd, &kp) != cudaSuccess)
+                        continue;
+                    bool isBulk = false;
+                    for (const void* f : bulk) isBulk = isBulk || f == (const void*)kp.func;
+                    cudaKernelNodeAttrValue v = {};
+                    v.priority = isBulk ? least : greatest;
+                    cudaGraphKernelNodeSetAttribute(nd, cudaKernelNodeAttributePriority, &v);
+                }
+        }
+        cudaGetLastError();  // a node left at the default priority is not an error
+    }
+    return cudaGraphInstantiateWithFlags(exec, g, cudaGraphInstantiateFlagUseNodePriority);
 }
 
 #define CU(h, call)                                                                                       \

@@ -927,15 +927,17 @@ struct MarchPrefetch {
     static constexpr bool value = sizeof(R) == 8 && ACP_MARCH_PREFETCH_F64;
 };
 
+// cols: x tiles of the launch (blockIdx.x indexes this list), or null for
+// every tile (blockIdx.x is the tile)
 template <typename S, typename R, int OP, int ORDER, bool CUBIC>
 __global__ void __launch_bounds__(MARCH_TX * MARCH_MAX_NZ, TiledMinBlocks<R>::value)
-    k_collide_push_march(LevelArgs<S> a, int yChunk) {
+    k_collide_push_march(LevelArgs<S> a, int yChunk, const int* __restrict__ cols) {
     extern __shared__ __align__(16) unsigned char marchSmem[];
+    const int bx = cols ? cols[blockIdx.x] : (int)blockIdx.x;
     if (MarchPrefetch<R>::value)
-        marchBodyPrefetch<S, R, OP, ORDER, CUBIC>(a, yChunk, blockIdx.x, blockIdx.y,
-                                                  reinterpret_cast<MomR<R>*>(marchSmem));
+        marchBodyPrefetch<S, R, OP, ORDER, CUBIC>(a, yChunk, bx, blockIdx.y, reinterpret_cast<MomR<R>*>(marchSmem));
     else
-        marchBody<S, R, OP, ORDER, CUBIC>(a, yChunk, blockIdx.x, blockIdx.y, reinterpret_cast<MomR<R>*>(marchSmem));
+        marchBody<S, R, OP, ORDER, CUBIC>(a, yChunk, bx, blockIdx.y, reinterpret_cast<MomR<R>*>(marchSmem));
 }
 
 // FP32 compute: the register cap set directly, so that blocks of 32 x 6
@@ -946,9 +948,11 @@ __global__ void __launch_bounds__(MARCH_TX * MARCH_MAX_NZ, TiledMinBlocks<R>::va
 #define ACP_MARCH_REGS_F32 56
 #endif
 template <typename S, typename R, int OP, int ORDER, bool CUBIC>
-__global__ void __maxnreg__(ACP_MARCH_REGS_F32) k_collide_push_march_f32(LevelArgs<S> a, int yChunk) {
+__global__ void __maxnreg__(ACP_MARCH_REGS_F32)
+    k_collide_push_march_f32(LevelArgs<S> a, int yChunk, const int* __restrict__ cols) {
     extern __shared__ __align__(16) unsigned char marchSmem[];
-    marchBody<S, R, OP, ORDER, CUBIC>(a, yChunk, blockIdx.x, blockIdx.y, reinterpret_cast<MomR<R>*>(marchSmem));
+    const int bx = cols ? cols[blockIdx.x] : (int)blockIdx.x;
+    marchBody<S, R, OP, ORDER, CUBIC>(a, yChunk, bx, blockIdx.y, reinterpret_cast<MomR<R>*>(marchSmem));
 }
 
 
@@ -991,14 +995,20 @@ __device__ __forceinline__ void absMoments(const S* arr, long long N, long long 
 
 // threads per LODI boundary node: lane m of a node's group forms the moments
 // of its stencil member m (0 the node, 1-2 the normal neighbours, 3-6 the
-// tangent neighbours), lane 0 then the characteristic update
+// tangent neighbours), lane 0 then the characteristic update.  Without
+// transverse terms (the classical LODI) no node reads its tangents, so the
+// three members fit groups of four lanes and a warp serves eight nodes.
 constexpr int LODI_TPN = 8;
+constexpr int LODI_TPN_CLASSICAL = 4;
+__host__ __device__ inline int lodiLanes(int transverse) { return transverse ? LODI_TPN : LODI_TPN_CLASSICAL; }
 
+// tpn: lodiLanes of the case (every node of the launch without transverse
+// terms when tpn is LODI_TPN_CLASSICAL)
 template <typename S, int ORDER>
 __device__ __forceinline__ void lodiBody(const S* __restrict__ A, S* B, const BNodeDev* __restrict__ nodes, int count,
-                                         const LodiArgs& p, const LevelArgs<S>& la, int bx) {
+                                         const LodiArgs& p, const LevelArgs<S>& la, int bx, int tpn) {
     const int tg = bx * blockDim.x + threadIdx.x;
-    const int t = tg / LODI_TPN, lane = tg % LODI_TPN;
+    const int t = tpn == LODI_TPN ? tg >> 3 : tg >> 2, lane = tg & (tpn - 1);
     const bool valid = t < count;
     const float* hs = la.hscale;
     // every lane of the warp reaches the shuffles below
@@ -1017,9 +1027,9 @@ __device__ __forceinline__ void lodiBody(const S* __restrict__ A, S* B, const BN
     double sr[7], su[7][3];
 #pragma unroll
     for (int m = 0; m < 7; ++m) {
-        sr[m] = __shfl_sync(0xffffffffu, mr, m, LODI_TPN);
+        sr[m] = __shfl_sync(0xffffffffu, mr, m, tpn);  // members past the group: read only with transverse terms
 #pragma unroll
-        for (int c = 0; c < 3; ++c) su[m][c] = __shfl_sync(0xffffffffu, mu[c], m, LODI_TPN);
+        for (int c = 0; c < 3; ++c) su[m][c] = __shfl_sync(0xffffffffu, mu[c], m, tpn);
     }
     if (!valid || lane != 0) return;
     const double densB = sr[0], dN = sr[1], d2N = sr[2];
@@ -1101,8 +1111,8 @@ __device__ __forceinline__ void lodiBody(const S* __restrict__ A, S* B, const BN
 }
 template <typename S, int ORDER>
 __global__ void k_lodi(const S* __restrict__ A, S* B, const BNodeDev* __restrict__ nodes, int count, LodiArgs p,
-                       LevelArgs<S> la) {
-    lodiBody<S, ORDER>(A, B, nodes, count, p, la, blockIdx.x);
+                       LevelArgs<S> la, int tpn) {
+    lodiBody<S, ORDER>(A, B, nodes, count, p, la, blockIdx.x, tpn);
 }
 
 
