@@ -1021,12 +1021,12 @@ int enqueueStepT(acp_handle* h, int src, PhaseTimer* tm) {
         enqueueC2F<S, R>(h, 1 - src, 1, R(0.5));  // C2F at t+1/2
         if (tm) tm->mark(ACP_K_COUPLING);
         if (fork) join(ls, h->branchEv[1]);
-        if (split) {
-            enqueueLevelStep<S, R>(h, 1, 1, tm, h->stream, false, PART_BOUNDARY);  // the tiles at the faces
-            join(h->side3, h->splitEv[1]);
-        } else {
-            enqueueLevelStep<S, R>(h, 1, 1, tm, h->stream, false);  // fine t+1/2 -> t+1
-        }
+        // the LODI passes at t+1, F2C and the last C2F read and write only
+        // nodes within four of a LODI or coupling face: with the tiles split
+        // they follow the face tiles and run beside the interior tiles' last
+        // waves
+        if (split) enqueueLevelStep<S, R>(h, 1, 1, tm, h->stream, false, PART_BOUNDARY);  // the face tiles
+        else enqueueLevelStep<S, R>(h, 1, 1, tm, h->stream, false);                       // fine t+1/2 -> t+1
         if (fork) branch(ls, h->branchEv[2]);
         enqueueLevelLodi<S, R>(h, 1, 1, tm, ls);
         if (tm) tm->mark(-1);
@@ -1047,6 +1047,7 @@ int enqueueStepT(acp_handle* h, int src, PhaseTimer* tm) {
         if (fork) {
             if (!h->f2cHost.empty()) join(fs, h->branchEv[4]);
             join(ls, h->branchEv[5]);
+            if (split) join(h->side3, h->splitEv[1]);
         }
     }
     if (h->nProbes) {
@@ -1246,12 +1247,14 @@ int acp_estimate_bytes(const acp_case_desc* d, size_t* bytes) {
 }
 
 // The x tiles of the fine level's y-marching collide (STD coupling, x not
-// periodic) split into those that touch no coupling or LODI node and the
-// others (LevelDev::cols).  A tile reads and pushes within x0 - 1 .. x0 + 30;
-// one more node each side is kept clear.  The second fine sub-step runs the
-// first kind beside the first C2F and the fine LODI passes: those write only
-// coupling and LODI nodes of the array the tiles read, and read only LODI
-// nodes of the array the tiles write.
+// periodic) split into those with no coupling or LODI node within reach and
+// the others (LevelDev::cols).  A tile reads and pushes within x0 - 1 ..
+// x0 + 30; four more nodes each side are kept clear, the depth of the fine
+// nodes F2C and the partner strain read behind a coupling face.  The second
+// fine sub-step runs the first kind beside the first C2F and the fine LODI
+// passes (those write only coupling and LODI nodes of the array the tiles
+// read, and read only LODI nodes of the array the tiles write), and F2C and
+// the last C2F beside its last waves.
 int splitFineTiles(acp_handle* h) {
     const LevelHost& F = h->host[1];
     if (!h->dcHost.empty() || !needsMoments(h->d) || !marchesY(F) || F.per[0]) return ACP_OK;
@@ -1259,8 +1262,8 @@ int splitFineTiles(acp_handle* h) {
     std::vector<char> hit(ntx, 0);
     auto mark = [&](long long n) {
         const int x = (int)(n % F.nx);
-        for (int bx = std::max(0, (x - 31) / MARCH_STEP - 1); bx <= std::min(ntx - 1, (x + 2) / MARCH_STEP + 1); ++bx)
-            if (x >= bx * MARCH_STEP - 2 && x <= bx * MARCH_STEP + 31) hit[bx] = 1;
+        for (int bx = std::max(0, (x - 34) / MARCH_STEP - 1); bx <= std::min(ntx - 1, (x + 5) / MARCH_STEP + 1); ++bx)
+            if (x >= bx * MARCH_STEP - 5 && x <= bx * MARCH_STEP + 34) hit[bx] = 1;
     };
     for (const long long n : F.coupling) mark(n);
     for (const BNodeDev& b : F.lodiX) mark(b.n);

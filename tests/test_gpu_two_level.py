@@ -263,30 +263,43 @@ def test_reference_default_case_two_levels():
 # coupling or LODI node within reach) beside the first C2F and the fine LODI
 # passes, and the tiles at the faces after them; the pulse starts close to the
 # interface so its waves cross both kinds of tile.
-@pytest.mark.parametrize("op,cubic,storage", [("HRR", 0, "FP64"), ("RR", 1, "FP64"), ("HRR", 0, "FP32-DEV")])
-def test_wide_fine_level_tile_split(op, cubic, storage):
-    d64 = half_box(op, "LAG", nx=160, ny=24, cubic=cubic)
-    d64.ic_center[0] = 72.0
+# A second layout puts the fine box in the middle of x (coupling faces on both
+# x sides, F2C at both), the pulse beside its upper face.
+@pytest.mark.parametrize("op,cubic,storage,layout", [("HRR", 0, "FP64", "right"), ("RR", 1, "FP64", "right"),
+                                                     ("HRR", 0, "FP32-DEV", "right"), ("HRR", 0, "FP64", "middle")])
+def test_wide_fine_level_tile_split(op, cubic, storage, layout):
+    def case(st):
+        if layout == "right":
+            d = half_box(op, "LAG", nx=160, ny=24, cubic=cubic, storage=st)
+            d.ic_center[0] = 72.0
+        else:
+            d = half_box(op, "LAG", nx=200, ny=24, cubic=cubic, storage=st)
+            d.box_lo[0], d.box_hi[0] = 50, 150
+            d.ic_center[0] = 158.0
+        return d
+    d64 = case("FP64")
     steps = 40
     from oracle.pyoracle import OracleLattice
     o = OracleLattice(d64, threads=8)
     o.init()
     o.step(steps)
     r = [o.populations(0), o.populations(1)]
-    d = half_box(op, "LAG", nx=160, ny=24, cubic=cubic, storage=storage)
-    d.ic_center[0] = 72.0
+    d = case(storage)
     L = engine.Lattice(d).init()
     L.step(steps)
     L.sync()
     g = [L.populations(0), L.populations(1)]
     L.close()
-    live_x = slice(0, d.nx // 2 + 2)
+    # coarse nodes covered by the fine box carry no state: from lo+2 to hi-2 with
+    # an interface at both x faces, from lo+2 to the LODI face otherwise
+    live = np.ones(d.nx, dtype=bool)
+    live[d.box_lo[0] + 2:(d.box_hi[0] - 1 if layout == "middle" else d.nx)] = False
     if storage == "FP64":
-        assert np.abs(g[0][..., live_x] - r[0][..., live_x]).max() / d.ic_eps < 1e-9
+        assert np.abs(g[0][..., live] - r[0][..., live]).max() / d.ic_eps < 1e-9
         assert np.abs(g[1] - r[1]).max() / d.ic_eps < 1e-9
     else:
         cs2 = d64.speed_of_sound ** 2
         amp = d64.ic_eps * d64.density * cs2
-        pc = np.abs(g[0].sum(0)[..., live_x] - r[0].sum(0)[..., live_x]).max() * cs2 / amp
+        pc = np.abs(g[0].sum(0)[..., live] - r[0].sum(0)[..., live]).max() * cs2 / amp
         pf = np.abs(g[1].sum(0) - r[1].sum(0)).max() * cs2 / amp
         assert pc < 1e-5 and pf < 1e-5, (pc, pf)
