@@ -11,13 +11,17 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <utility>
 #include <algorithm>
 #include <condition_variable>
 #include <functional>
+#include <map>
 #include <mutex>
+#include <new>
 #include <thread>
+#include <unordered_map>
 
 #include <pthread.h>
 #include <string>
@@ -46,6 +50,70 @@ int uploadConstants(int device) {
 }  // namespace
 
 namespace acp {
+
+// Page-locked host blocks of the node-class arrays, kept for reuse once a
+// lattice is destroyed: blocks of the same rounded size are handed out again
+// (at most 1 GiB kept).  Without a usable device the blocks are ordinary heap
+// memory.
+struct HostBlocks {
+    std::mutex m;
+    std::map<size_t, std::vector<void*>> free;  // rounded size -> page-locked blocks
+    std::unordered_map<void*, bool> pinned;     // live block -> page-locked
+    size_t kept = 0;
+};
+static HostBlocks& hostBlocks() {
+    static HostBlocks* b = new HostBlocks();  // kept until the process exits
+    return *b;
+}
+static size_t roundHostBlock(size_t bytes) { return (bytes + (1u << 16) - 1) & ~(size_t)((1u << 16) - 1); }
+
+void* hostBlockAlloc(size_t bytes) {
+    HostBlocks& hb = hostBlocks();
+    const size_t r = roundHostBlock(std::max<size_t>(bytes, 1));
+    {
+        std::lock_guard<std::mutex> g(hb.m);
+        auto it = hb.free.find(r);
+        if (it != hb.free.end() && !it->second.empty()) {
+            void* p = it->second.back();
+            it->second.pop_back();
+            hb.kept -= r;
+            hb.pinned[p] = true;
+            return p;
+        }
+    }
+    void* p = nullptr;
+    bool pin = cudaMallocHost(&p, r) == cudaSuccess;
+    if (!pin) {
+        cudaGetLastError();
+        p = std::malloc(r);
+        if (!p) throw std::bad_alloc();
+    }
+    std::lock_guard<std::mutex> g(hb.m);
+    hb.pinned[p] = pin;
+    return p;
+}
+
+void hostBlockFree(void* p, size_t bytes) {
+    if (!p) return;
+    HostBlocks& hb = hostBlocks();
+    const size_t r = roundHostBlock(std::max<size_t>(bytes, 1));
+    bool pin = false;
+    {
+        std::lock_guard<std::mutex> g(hb.m);
+        auto it = hb.pinned.find(p);
+        if (it != hb.pinned.end()) {
+            pin = it->second;
+            hb.pinned.erase(it);
+        }
+        if (pin && hb.kept + r <= ((size_t)1 << 30)) {
+            hb.free[r].push_back(p);
+            hb.kept += r;
+            return;
+        }
+    }
+    if (pin) cudaFreeHost(p);
+    else std::free(p);
+}
 
 // the lattice constant table (push masks)
 int makeConstTables(ConstTables& t) {
@@ -1147,11 +1215,95 @@ __global__ void k_scatter_slots(int* slot, const Rec* recs, int n) {
     if (t < n) slot[recs[t].n] = t;
 }
 
+// Device memory of the lattices.  Blocks that a destroyed lattice (or a
+// replaced probe set) frees are kept per device and rounded size and handed
+// to the next allocation of that size, so a process that creates lattices
+// one after another (a serving loop, repeated solves) skips cudaMalloc and
+// cudaFree.  Sizes round up to 64 KiB below 1 MiB and to 2 MiB above; a
+// device keeps at most a quarter of its memory this way; an allocation that
+// cudaMalloc refuses first returns the kept blocks of its device and retries.
+// Freeing synchronises the device first, as cudaFree does.
+struct DeviceBlocks {
+    std::mutex m;
+    std::map<std::pair<int, size_t>, std::vector<void*>> free;  // (device, rounded size) -> blocks
+    std::unordered_map<void*, std::pair<int, size_t>> live;     // block -> (device, rounded size)
+    std::map<int, size_t> kept, limit;                            // per device: bytes kept, most kept
+};
+DeviceBlocks& deviceBlocks() {
+    static DeviceBlocks* b = new DeviceBlocks();  // kept until the process exits
+    return *b;
+}
+size_t roundDeviceBlock(size_t bytes) {
+    const size_t g = bytes <= ((size_t)1 << 20) ? ((size_t)1 << 16) : ((size_t)2 << 20);
+    return (std::max<size_t>(bytes, 1) + g - 1) / g * g;
+}
+void releaseDeviceBlocks(int device) {
+    DeviceBlocks& db = deviceBlocks();
+    std::vector<void*> out;
+    {
+        std::lock_guard<std::mutex> g(db.m);
+        for (auto& kv : db.free)
+            if (kv.first.first == device) {
+                out.insert(out.end(), kv.second.begin(), kv.second.end());
+                kv.second.clear();
+            }
+        db.kept[device] = 0;
+    }
+    for (void* p : out) cudaFree(p);
+}
+
 int devAlloc(acp_handle* h, void** p, size_t bytes) {
-    cudaError_t e = cudaMalloc(p, bytes);
+    DeviceBlocks& db = deviceBlocks();
+    const size_t r = roundDeviceBlock(bytes);
+    {
+        std::lock_guard<std::mutex> g(db.m);
+        auto it = db.free.find({h->device, r});
+        if (it != db.free.end() && !it->second.empty()) {
+            *p = it->second.back();
+            it->second.pop_back();
+            db.kept[h->device] -= r;
+            db.live[*p] = {h->device, r};
+            h->devBytes += bytes;
+            return ACP_OK;
+        }
+    }
+    cudaError_t e = cudaMalloc(p, r);
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        releaseDeviceBlocks(h->device);
+        e = cudaMalloc(p, r);
+    }
     if (e != cudaSuccess) return fail(h, ACP_ERR_NOMEM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+    std::lock_guard<std::mutex> g(db.m);
+    db.live[*p] = {h->device, r};
+    if (!db.limit.count(h->device)) {
+        size_t fr = 0, total = 0;
+        db.limit[h->device] = cudaMemGetInfo(&fr, &total) == cudaSuccess ? total / 4 : 0;
+    }
     h->devBytes += bytes;
     return ACP_OK;
+}
+
+// returns a block of devAlloc (kept for reuse) or frees any other device pointer
+void devFree(void* p) {
+    if (!p) return;
+    cudaDeviceSynchronize();  // no kernel may still use the block when it is handed out again
+    DeviceBlocks& db = deviceBlocks();
+    {
+        std::lock_guard<std::mutex> g(db.m);
+        auto it = db.live.find(p);
+        if (it != db.live.end()) {
+            const int dev = it->second.first;
+            const size_t r = it->second.second;
+            db.live.erase(it);
+            if (db.kept[dev] + r <= db.limit[dev]) {
+                db.free[{dev, r}].push_back(p);
+                db.kept[dev] += r;
+                return;
+            }
+        }
+    }
+    cudaFree(p);
 }
 
 size_t estimateBytes(const acp_case_desc& d) {
@@ -1911,9 +2063,9 @@ int acp_set_probes(acp_handle* h, int n, const int* lijk) {
         if (L.code[nodes[m]] == CODE_DEAD) return fail(h, ACP_ERR_INVALID, "probe %d on a node covered by the fine level", m);
         levels[m] = l;
     }
-    if (h->dProbeNodes) { cudaFree(h->dProbeNodes); h->dProbeNodes = nullptr; }
-    if (h->dProbeLevels) { cudaFree(h->dProbeLevels); h->dProbeLevels = nullptr; }
-    if (h->dSeries) { cudaFree(h->dSeries); h->dSeries = nullptr; }
+    if (h->dProbeNodes) { devFree(h->dProbeNodes); h->dProbeNodes = nullptr; }
+    if (h->dProbeLevels) { devFree(h->dProbeLevels); h->dProbeLevels = nullptr; }
+    if (h->dSeries) { devFree(h->dSeries); h->dSeries = nullptr; }
     if (!h->dCounter) {
         int s = devAlloc(h, (void**)&h->dCounter, sizeof(int));
         if (s) return s;
@@ -2052,26 +2204,26 @@ int acp_destroy(acp_handle* h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     destroyGraphs(h);
     for (LevelDev& D : h->dev) {
-        cudaFree(D.f[0]);
-        cudaFree(D.f[1]);
-        cudaFree(D.code);
-        cudaFree(D.lodiX);
-        cudaFree(D.lodiZY);
-        cudaFree(D.slot);
-        cudaFree(D.sg);
-        cudaFree(D.cols);
+        devFree(D.f[0]);
+        devFree(D.f[1]);
+        devFree(D.code);
+        devFree(D.lodiX);
+        devFree(D.lodiZY);
+        devFree(D.slot);
+        devFree(D.sg);
+        devFree(D.cols);
     }
-    cudaFree(h->dNb);
-    cudaFree(h->dPreNb);
-    cudaFree(h->dErr);
-    cudaFree(h->dC2F);
-    cudaFree(h->dF2C);
-    cudaFree(h->dDC);
-    cudaFree(h->dPre);
-    cudaFree(h->dProbeNodes);
-    cudaFree(h->dProbeLevels);
-    cudaFree(h->dSeries);
-    cudaFree(h->dCounter);
+    devFree(h->dNb);
+    devFree(h->dPreNb);
+    devFree(h->dErr);
+    devFree(h->dC2F);
+    devFree(h->dF2C);
+    devFree(h->dDC);
+    devFree(h->dPre);
+    devFree(h->dProbeNodes);
+    devFree(h->dProbeLevels);
+    devFree(h->dSeries);
+    devFree(h->dCounter);
     if (h->ownStream && h->stream) cudaStreamDestroy(h->stream);
     if (h->side) cudaStreamDestroy(h->side);
     if (h->forkEv) cudaEventDestroy(h->forkEv);

@@ -19,11 +19,19 @@ struct acp_batch;
 
 namespace acp {
 
-// allocator whose resize leaves new elements uninitialised: the node-class
-// arrays are written in full by the set-up scans, row ranges on several
-// threads, so a zero fill first would be a second serial pass over them
+// page-locked host blocks kept for reuse (engine.cu): the node-class arrays
+// live in them, so their upload is a direct DMA instead of a staged copy of
+// pageable memory; without a device they are ordinary heap blocks
+void* hostBlockAlloc(size_t bytes);
+void hostBlockFree(void* p, size_t bytes);
+
+// allocator of the node-class arrays: page-locked host blocks (above), and a
+// resize that leaves new elements uninitialised (the set-up scans write the
+// arrays in full, row ranges on several threads, so a zero fill first would
+// be a second serial pass over them)
 template <typename T>
-struct NoInitAlloc : std::allocator<T> {
+struct NoInitAlloc {
+    using value_type = T;
     template <typename U>
     struct rebind {
         using other = NoInitAlloc<U>;
@@ -31,12 +39,18 @@ struct NoInitAlloc : std::allocator<T> {
     NoInitAlloc() = default;
     template <typename U>
     NoInitAlloc(const NoInitAlloc<U>&) noexcept {}
+    T* allocate(size_t n) { return static_cast<T*>(hostBlockAlloc(n * sizeof(T))); }
+    void deallocate(T* p, size_t n) noexcept { hostBlockFree(p, n * sizeof(T)); }
     template <typename U>
     void construct(U*) noexcept {}
     template <typename U, typename... A>
     void construct(U* p, A&&... a) {
         ::new ((void*)p) U(std::forward<A>(a)...);
     }
+    template <typename U>
+    bool operator==(const NoInitAlloc<U>&) const noexcept { return true; }
+    template <typename U>
+    bool operator!=(const NoInitAlloc<U>&) const noexcept { return false; }
 };
 
 struct LevelHost {

@@ -309,6 +309,10 @@ int acp_batch_info(acp_batch* b, int* groups, int* launches_per_step, long long*
 int acp_batch_destroy(acp_batch* b);
 const char* acp_batch_last_error(const acp_batch* b);
 
+/* Releases a case (Lattice::~Lattice).  Its device blocks are kept, per
+ * device and up to a quarter of the device's memory, for the next case the
+ * process creates (an allocation the driver refuses first gives them back);
+ * its page-locked host blocks likewise (up to 1 GiB). */
 int acp_destroy(acp_handle* h);
 const char* acp_last_error(const acp_handle* h);
 const char* acp_status_string(int status);
