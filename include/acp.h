@@ -311,7 +311,7 @@ const char* acp_batch_last_error(const acp_batch* b);
 
 /* Releases a case (Lattice::~Lattice).  Its device blocks are kept, per
  * device and up to a quarter of the device's memory, for the next case the
- * process creates (an allocation the driver refuses first gives them back);
+ * process creates (an allocation the CUDA driver refuses first gives them back);
  * its page-locked host blocks likewise (up to 1 GiB). */
 int acp_destroy(acp_handle* h);
 const char* acp_last_error(const acp_handle* h);

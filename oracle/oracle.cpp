@@ -1,8 +1,8 @@
 // FP64 CPU oracle for the acPulse_vcLBM hot path.
 //
 // TEST INFRASTRUCTURE ONLY.  This is a restatement of the reference's
-// algorithm used as the checker: tests/, __graft_entry__.smoke() and the CPU
-// baseline of bench.py call it; the engine never does.
+// algorithm that checks the engine's results: tests/, __graft_entry__.smoke()
+// and the CPU baseline of bench.py call it; the engine never does.
 //
 // Single level (MaxLevel 0): Lattice::timeStepping{SRT,MRT_GS,MRT_RM,RR,HRR}
 // (Lattice.cpp:1496-2156) with the per-node operators of Node.cpp, restated

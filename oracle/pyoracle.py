@@ -1,7 +1,8 @@
 """ctypes wrapper of the FP64 CPU oracle (oracle/liboracle.so).
 
 TEST INFRASTRUCTURE: imported only by tests/, __graft_entry__.smoke() and the
-CPU-baseline leg of bench.py, as the checker.  The engine never calls it.
+CPU-baseline leg of bench.py, to check the engine's results.  The engine never
+calls it.
 """
 import ctypes as C
 import os
